@@ -1,0 +1,179 @@
+/*
+ * rbs.h -- C ABI of the B200 recursive-block sparse triangular solver.
+ *
+ * Drop-in boundary for recblock-sptrsv's analysis ("preprocess") and solve
+ * entry points.  Every function is extern "C", takes plain pointers and
+ * sizes, and returns an int status (RBS_OK == 0) where the reference returns
+ * void.  Paths in citations are relative to the reference project directory
+ * recblock-sptrsv/.
+ *
+ *   reference                                          replacement
+ *   -------------------------------------------------  -----------------------------
+ *   recblocking_solver_cuda(...)  recblocking_solver_cuda.h:21-32   recblocking_solver_cuda (same
+ *                                                      signature, below) or
+ *                                                      rbs_analyse_device + rbs_solve
+ *   recblocking_solver(...)       recblocking_solver.h:16-28        recblocking_solver (same
+ *                                                      signature) or rbs_analyse + rbs_solve_host
+ *   levelset_reordering_colrow_csc[_cuda] + mat_preprocessing[_cuda]
+ *   + per-block loop  (recblocking_solver_cuda.h:73-584,
+ *     recblocking_preprocess.h:298-967)                 rbs_analyse / rbs_analyse_device
+ *   L_calculate / U_calculate (recblocking_calculate.h:15,170)      rbs_solve
+ *   device_memfree (recblocking_calculate.h:327)        rbs_plan_free
+ *
+ * Conventions: the caller owns inputs and outputs; a plan owns its device
+ * state; each plan runs on one CUDA stream (rbs_plan_set_stream); distinct
+ * plans may be used from distinct host threads.  Errors never hang: every
+ * device wait is bounded and reports RBS_ERR_TIMEOUT.
+ */
+#ifndef RBS_H
+#define RBS_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define RBS_OK 0
+#define RBS_ERR_ARG 1          /* null pointer, bad size or flag, plan without device state */
+#define RBS_ERR_STRUCTURE 2    /* not triangular, diagonal missing/misplaced, index out of range */
+#define RBS_ERR_CUDA 3         /* CUDA runtime error (message in rbs_last_error) */
+#define RBS_ERR_NOMEM 4        /* host or device allocation failed */
+#define RBS_ERR_TIMEOUT 5      /* a bounded device wait expired (dependency never produced) */
+#define RBS_ERR_NOCONV 6       /* mixed-precision refinement missed its tolerance */
+#define RBS_ERR_BUDGET 7       /* serving: request does not fit the HBM budget */
+#define RBS_ERR_UNSUPPORTED 8  /* option combination not built */
+
+/* ---- flags ------------------------------------------------------------ */
+#define RBS_FORWARD 0          /* common.h:25 SUBSTITUTION_FORWARD  (lower, L x = b) */
+#define RBS_BACKWARD 1         /* common.h:26 SUBSTITUTION_BACKWARD (upper, U x = b) */
+
+#define RBS_FMT_CSC 0          /* the reference's input format (diagonal first/last per column) */
+#define RBS_FMT_CSR 1
+
+#define RBS_PREC_FP64 0        /* plain FP64 solve */
+#define RBS_PREC_MIXED 1       /* FP32 sweeps + FP64 residual/update refinement to ir_tol */
+#define RBS_PREC_FP32 2        /* one FP32 sweep, no refinement */
+
+#define RBS_SELECT_REFERENCE 0 /* the reference's thresholds pick the method per block
+                                  (recblocking_preprocess.h:472-709, 835-922); each reference
+                                  method maps to this library's kernel of the same kind */
+#define RBS_SELECT_AUTO 1      /* cost model over this library's kernels */
+#define RBS_SELECT_TUNE 2      /* time the candidate kernels per block at analysis, keep the fastest */
+
+typedef struct rbs_options {
+    int select;             /* RBS_SELECT_* (default AUTO) */
+    int device;             /* CUDA device ordinal, -1 = current (default -1) */
+    int lv_device_id;       /* device id used by the automatic-lv rule main.cu:245-254 (default 0) */
+    int host_only;          /* 1: analysis only, no device state (for host-side inspection) */
+    int max_rhs;            /* widest k a solve will use (default 1; grows on demand) */
+    int mixed;              /* 1: also build FP32 factor copies for RBS_PREC_MIXED/FP32 (default 1) */
+    double ir_tol;          /* refinement stop: ||dx||/||x|| <= ir_tol (default 1e-13) */
+    int ir_max_iter;        /* default 8 */
+    long long spin_limit;   /* polls before a device wait gives up (default 1<<22 with backoff) */
+} rbs_options;
+
+typedef struct rbs_stats {
+    double ms;              /* device time of the solve, CUDA events on the plan's stream */
+    int iterations;         /* refinement corrections applied (0 for FP64/FP32) */
+    double correction;      /* last ||dx||/||x|| (mixed) */
+    double useful_bytes;    /* nnz*(8+4) + 4*(n+1) + 16*n*k */
+    double moved_bytes;     /* algorithmic bytes of all passes actually run */
+} rbs_stats;
+
+typedef struct rbs_plan_info {
+    int n, nnz, lv, substitution;
+    int nlevel;             /* global level count */
+    int sum_block;          /* 2^(lv+1)-1 */
+    int kernels[8];         /* blocks per kernel kind (RBS_K_*) */
+    long long device_bytes; /* device memory held by the plan */
+    double analyse_ms;      /* wall time of the analysis */
+} rbs_plan_info;
+
+/* kernel kinds reported in rbs_plan_info.kernels / rbs_plan_export("kernel") */
+#define RBS_K_DIAG 0        /* diagonal-only triangle (reference method 0) */
+#define RBS_K_SYNCFREE 1    /* multi-CTA sync-free triangle (reference method 3) */
+#define RBS_K_LEVEL 2       /* single-CTA level-synchronous triangle (reference method 2) */
+#define RBS_K_SEQ 3         /* single-CTA sequential triangle (replaces cuSPARSE, method 1) */
+#define RBS_K_BANDSCAN 4    /* parallel affine scan for deep narrow-band triangles (method 1) */
+#define RBS_K_SPMV 5        /* square block SpMV, fused b -= S x (methods 0..3) */
+#define RBS_K_EMPTY 6       /* empty square block */
+
+typedef struct rbs_plan rbs_plan;
+
+void rbs_options_default(rbs_options *opt);
+
+/* Analysis on HOST arrays.  fmt RBS_FMT_CSC: ptr = column pointer (n+1),
+ * idx = row indices, diagonal first in each column for RBS_FORWARD and last
+ * for RBS_BACKWARD (the layout main.cu:157-238 produces).  RBS_FMT_CSR:
+ * ptr = row pointer, any order inside a row.  lv >= 0, or -1 for the
+ * reference's automatic rule.  opt may be NULL. */
+int rbs_analyse(const int *ptr, const int *idx, const double *val, int n, int nnz, int fmt,
+                int substitution, int lv, const rbs_options *opt, rbs_plan **plan);
+
+/* Analysis on DEVICE arrays (the inputs of recblocking_solver_cuda). */
+int rbs_analyse_device(const int *d_ptr, const int *d_idx, const double *d_val, int n, int nnz,
+                       int fmt, int substitution, int lv, const rbs_options *opt, rbs_plan **plan);
+
+/* Solve with k right-hand sides, DEVICE arrays, column-major with leading
+ * dimension ld (>= n).  b is read only (the reference overwrites d_b;
+ * recblocking_calculate.h:39).  Returns when the solve is complete.
+ * stats may be NULL. */
+int rbs_solve(rbs_plan *plan, const double *d_b, double *d_x, int k, int ld, int prec,
+              rbs_stats *stats);
+
+/* Same with HOST arrays: copies in, solves, copies out. */
+int rbs_solve_host(rbs_plan *plan, const double *b, double *x, int k, int ld, int prec,
+                   rbs_stats *stats);
+
+/* Asynchronous variant: enqueue on the plan's stream and return.  Status of
+ * the device-side checks is collected by rbs_plan_sync. */
+int rbs_solve_async(rbs_plan *plan, const double *d_b, double *d_x, int k, int ld, int prec);
+int rbs_plan_sync(rbs_plan *plan);
+
+/* cudaStream_t passed as void* (NULL = the plan's own stream). */
+int rbs_plan_set_stream(rbs_plan *plan, void *stream);
+int rbs_plan_info_get(const rbs_plan *plan, rbs_plan_info *info);
+
+/* Copy a named integer (or, for "recblock_Val", double) output of the
+ * analysis into dst.  Names follow the reference's variables: "levelItem",
+ * "loc_off", "tmp_off", "blk_m", "blk_n", "blk_nnz", "subtri_up",
+ * "subtri_down", "subrec_up", "subrec_down", "subrec_right", "subrec_left",
+ * "ptr_offset", "index_offset", "dcsrindex_offset", "recblock_Ptr",
+ * "recblock_Index", "recblock_Val", "recblock_dcsr_rowidx", "method", "nlv",
+ * "longrow", "m_new_dcsr", "lvl_ptr", "lvl_item", "m_lv", "offset_lv",
+ * "nnz_lv", "sizes", plus this library's "kernel" (RBS_K_* per block).
+ * With dst == NULL only *count is set.  Returns RBS_ERR_ARG for an unknown
+ * name or cap < count. */
+int rbs_plan_export(const rbs_plan *plan, const char *name, void *dst, long long cap,
+                    long long *count);
+
+int rbs_plan_free(rbs_plan *plan);
+
+/* Message of the last error on the calling thread ("" if none). */
+const char *rbs_last_error(void);
+
+/* main.cu:245-254: lv for the -lv -1 option. */
+int rbs_auto_lv(int m, int device_id);
+
+/* ---- reference-signature shims ---------------------------------------- */
+
+/* recblocking_solver_cuda.h:21-32.  Same arguments and meaning: device CSC
+ * input, solution in d_x, cal_time = mean solve ms over 200 repetitions is
+ * ADDED to *cal_time (the reference accumulates), *preprocess_time = analysis
+ * ms (the reference sets it for forward only; this sets it for both).
+ * Difference: d_b is left as the caller passed it.  Errors are reported
+ * through rbs_last_error(). */
+void recblocking_solver_cuda(int *d_cscColPtrTR, int *d_cscRowIdxTR, double *d_cscValTR, int m, int n,
+                             int nnzTR, double *d_x, double *d_b, int substitution, int lv,
+                             double *cal_time, double *preprocess_time);
+
+/* recblocking_solver.h:16-28.  Host CSC input, host b and x; x_ref unused
+ * (as in the reference); rhs columns of b/x stored column-major with
+ * leading dimension m (the reference hard-codes rhs = 1 in the GPU path). */
+void recblocking_solver(int *cscColPtr, int *cscRowIdx, double *cscVal, int m, int n, int nnz, double *b,
+                        double *x, double *x_ref, int rhs, int lv, int substitution, double *cal_time);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,554 @@
+/*
+ * oracle.c -- TEST INFRASTRUCTURE ONLY (see oracle.h).
+ *
+ * CPU restatement of recblock-sptrsv's analysis (level sets, level-set
+ * reordering, recursive-block geometry, per-block extraction, method choice
+ * and packing) and of serial substitution.  Each function names the
+ * reference lines it follows.  Paths are relative to the reference project
+ * directory recblock-sptrsv/.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* utils.h:98-113 exclusive_scan, in place over `len` entries */
+static void excl_scan(int *a, int len) {
+    if (len <= 1) return;
+    int carry = a[0];
+    a[0] = 0;
+    for (int i = 1; i < len; ++i) {
+        int cur = a[i];
+        a[i] = a[i - 1] + carry;
+        carry = cur;
+    }
+}
+
+void orc_transpose(int m, int n, int nnz, const int *ptr, const int *idx, const double *val,
+                   int *tptr, int *tidx, double *tval) {
+    /* tranpose.h:17-25: column histogram + exclusive scan */
+    memset(tptr, 0, sizeof(int) * (size_t)(n + 1));
+    for (int k = 0; k < nnz; ++k) tptr[idx[k]]++;
+    excl_scan(tptr, n + 1);
+    if (!tidx) return; /* tranpose.h:92-108 (_litelite) */
+    /* tranpose.h:31-51: scatter rows in ascending order -> stable */
+    int *fill = (int *)malloc(sizeof(int) * (size_t)(n + 1));
+    memcpy(fill, tptr, sizeof(int) * (size_t)(n + 1));
+    for (int r = 0; r < m; ++r) {
+        for (int k = ptr[r]; k < ptr[r + 1]; ++k) {
+            int c = idx[k];
+            int dst = fill[c]++;
+            tidx[dst] = r;
+            if (val && tval) tval[dst] = val[k];
+        }
+    }
+    free(fill);
+}
+
+int orc_findlevel(const int *cscColPtr, const int *cscRowIdx, const int *csrRowPtr, int m,
+                  int *nlevel, int *levelPtr, int *levelItem) {
+    /* findlevel.h:16-22: in-degree = row length, diagonal included */
+    int *deg = (int *)malloc(sizeof(int) * (size_t)(m > 0 ? m : 1));
+    for (int i = 0; i < m; ++i) deg[i] = csrRowPtr[i + 1] - csrRowPtr[i];
+    /* findlevel.h:31-50: roots are rows whose only entry is the diagonal */
+    int tail = 0;
+    levelPtr[0] = 0;
+    for (int i = 0; i < m; ++i)
+        if (deg[i] == 1) levelItem[tail++] = i;
+    levelPtr[1] = tail;
+    /* findlevel.h:53-72: walk each level in discovery order; a row joins the
+     * next level when its in-degree drops to exactly 1 */
+    int lvl = 1;
+    while (levelPtr[lvl] != m) {
+        for (int p = levelPtr[lvl - 1]; p < levelPtr[lvl]; ++p) {
+            int node = levelItem[p];
+            for (int k = cscColPtr[node]; k < cscColPtr[node + 1]; ++k) {
+                int r = cscRowIdx[k];
+                if (--deg[r] == 1) levelItem[tail++] = r;
+            }
+        }
+        ++lvl;
+        levelPtr[lvl] = tail;
+        if (levelPtr[lvl] == levelPtr[lvl - 1]) { /* the reference spins here forever */
+            free(deg);
+            return -1;
+        }
+    }
+    *nlevel = lvl;
+    free(deg);
+    return 0;
+}
+
+int orc_reorder_colrow(const int *colptr, const int *rowidx, const double *val, int m, int nnz,
+                       int substitution, int *colptr_new, int *rowidx_new, double *val_new,
+                       int *levelItem) {
+    /* utils_reordering.h:114-128: row counts, then level sets */
+    int *rowptr = (int *)malloc(sizeof(int) * (size_t)(m + 1));
+    int *levelPtr = (int *)malloc(sizeof(int) * (size_t)(m + 1));
+    orc_transpose(m, m, nnz, colptr, rowidx, NULL, rowptr, NULL, NULL);
+    int nlv = 0;
+    if (orc_findlevel(colptr, rowidx, rowptr, m, &nlv, levelPtr, levelItem) != 0) {
+        free(rowptr);
+        free(levelPtr);
+        return -1;
+    }
+    /* utils_reordering.h:130-159: new label of every row.  Forward: the
+     * inverse of levelItem (the key/value quicksort on unique keys).
+     * Backward: levelItem[i] gets label m-1-i. */
+    int *perm = (int *)malloc(sizeof(int) * (size_t)(m > 0 ? m : 1));
+    for (int i = 0; i < m; ++i)
+        perm[levelItem[i]] = substitution == ORC_FORWARD ? i : m - 1 - i;
+    /* utils_reordering.h:166-181: columns in level order (reversed for
+     * backward), entries of a column keep their order */
+    colptr_new[0] = 0;
+    for (int i = 0; i < m; ++i) {
+        int src = substitution == ORC_FORWARD ? levelItem[i] : levelItem[m - 1 - i];
+        int len = colptr[src + 1] - colptr[src];
+        colptr_new[i + 1] = colptr_new[i] + len;
+        for (int j = 0; j < len; ++j) {
+            rowidx_new[colptr_new[i] + j] = rowidx[colptr[src] + j];
+            val_new[colptr_new[i] + j] = val ? val[colptr[src] + j] : 0.0;
+        }
+    }
+    /* utils_reordering.h:184-187: relabel rows */
+    for (int k = 0; k < nnz; ++k) rowidx_new[k] = perm[rowidx_new[k]];
+    /* utils_reordering.h:189-197: backward keeps levelItem in new-label order */
+    if (substitution == ORC_BACKWARD) {
+        for (int i = 0; i < m / 2; ++i) {
+            int t = levelItem[i];
+            levelItem[i] = levelItem[m - 1 - i];
+            levelItem[m - 1 - i] = t;
+        }
+    }
+    free(perm);
+    free(rowptr);
+    free(levelPtr);
+    return 0;
+}
+
+/* lowest set bit: the reference reaches it with the figure[] loop
+ * (recblocking_preprocess.h:109-134 / 223-248) */
+static int lowbit(int t) { return t & (-t); }
+
+/* recblocking_preprocess.h:45-55: judge[j] = sum_{i=lv-1-j}^{lv-1} 2^i; a
+ * square whose preceding triangle count equals one of them reaches the
+ * matrix edge */
+static int reaches_edge(int t, int lv) {
+    for (int j = 0; j < lv; ++j) {
+        int s = 0;
+        for (int i = lv - 1 - j; i <= lv - 1; ++i) s += 1 << i;
+        if (s == t) return 1;
+    }
+    return 0;
+}
+
+void orc_geometry(const int *colptr, const int *rowidx, int m, int lv, int substitution,
+                  int *loc_off, int *tmp_off, int *blk_m, int *blk_n, int *blk_nnz,
+                  int *subtri_up, int *subtri_down, int *subrec_up, int *subrec_down,
+                  int *subrec_right, int *subrec_left) {
+    int tri = 1 << lv, sum = 2 * tri - 1;
+    int step = m / tri; /* recblocking_preprocess.h:37 */
+    for (int i = 0; i < sum; ++i) {
+        loc_off[i] = tmp_off[i] = 0; /* zeroed by the solver entry (recblocking_solver.h:42-45) */
+        subtri_up[i] = subtri_down[i] = subrec_up[i] = subrec_down[i] = -1;
+        subrec_right[i] = subrec_left[i] = -1;
+    }
+    int t = 0;
+    if (substitution == ORC_FORWARD) { /* recblocking_preprocess.h:57-178 */
+        int tu = 0, td = step;
+        for (int i = 0; i < sum; ++i) {
+            if ((i & 1) == 0) {
+                blk_m[i] = blk_n[i] = td - tu;
+                subtri_up[i] = tu;
+                subtri_down[i] = td;
+                int c = 0;
+                for (int j = tu; j < td; ++j)
+                    for (int k = colptr[j]; k < colptr[j + 1]; ++k)
+                        if (rowidx[k] < td) ++c;
+                blk_nnz[i] = c;
+                loc_off[i] = tu;
+                tu += step;
+                td += step;
+                ++t;
+            } else {
+                int up = td - step;
+                int down = up + lowbit(t) * step;
+                int right = up;
+                int left = right - (down - up);
+                if (reaches_edge(t, lv)) down = m;
+                blk_m[i] = down - up;
+                blk_n[i] = right - left;
+                int c = 0;
+                for (int j = left; j < right; ++j)
+                    for (int k = colptr[j]; k < colptr[j + 1]; ++k)
+                        if (rowidx[k] >= up && rowidx[k] < down) ++c;
+                blk_nnz[i] = c;
+                tmp_off[i] = up;
+                loc_off[i] = left;
+                if (i == sum - 2) td = m;
+                subrec_up[i] = up;
+                subrec_down[i] = down;
+                subrec_right[i] = right;
+                subrec_left[i] = left;
+            }
+        }
+    } else { /* recblocking_preprocess.h:179-292 */
+        int tu = m - step, td = m;
+        for (int i = 0; i < sum; ++i) {
+            if ((i & 1) == 0) {
+                blk_m[i] = blk_n[i] = td - tu;
+                subtri_up[i] = tu;
+                subtri_down[i] = td;
+                int c = 0;
+                for (int j = tu; j < td; ++j)
+                    for (int k = colptr[j]; k < colptr[j + 1]; ++k)
+                        if (rowidx[k] >= tu) ++c;
+                blk_nnz[i] = c;
+                loc_off[i] = tu;
+                tu -= step;
+                td -= step;
+                ++t;
+            } else {
+                int down = tu + step;
+                int up = down - lowbit(t) * step;
+                int left = down;
+                int right = left + (down - up);
+                if (reaches_edge(t, lv)) up = 0;
+                blk_m[i] = down - up;
+                blk_n[i] = right - left;
+                int c = 0;
+                for (int j = left; j < right; ++j)
+                    for (int k = colptr[j]; k < colptr[j + 1]; ++k)
+                        if (rowidx[k] >= up && rowidx[k] < down) ++c;
+                blk_nnz[i] = c;
+                tmp_off[i] = up;
+                loc_off[i] = left;
+                if (i == sum - 2) tu = 0;
+                subrec_up[i] = up;
+                subrec_down[i] = down;
+                subrec_right[i] = right;
+                subrec_left[i] = left;
+            }
+        }
+    }
+}
+
+#define ALLOC_I(n) ((int *)calloc((size_t)((n) > 0 ? (n) : 1), sizeof(int)))
+#define ALLOC_D(n) ((double *)calloc((size_t)((n) > 0 ? (n) : 1), sizeof(double)))
+
+int orc_analyse(const int *colptr, const int *rowidx, const double *val, int m, int nnz,
+                int substitution, int lv, orc_blocks *o) {
+    memset(o, 0, sizeof(*o));
+    int tri = 1 << lv, sum = 2 * tri - 1;
+    o->lv = lv;
+    o->sum_block = sum;
+    o->m = m;
+    o->nnz = nnz;
+    int *cp = ALLOC_I(m + 1), *ri = ALLOC_I(nnz);
+    double *va = ALLOC_D(nnz);
+    o->levelItem = ALLOC_I(m);
+    /* recblocking_preprocess.h:335-337 */
+    if (orc_reorder_colrow(colptr, rowidx, val, m, nnz, substitution, cp, ri, va, o->levelItem) != 0) {
+        free(cp); free(ri); free(va);
+        return -1;
+    }
+#define A(f) o->f = ALLOC_I(sum)
+    A(method); A(nlv); A(m_new); A(longrow); A(lenmax);
+    A(loc_off); A(tmp_off); A(blk_m); A(blk_n); A(blk_nnz);
+    A(subtri_up); A(subtri_down); A(subrec_up); A(subrec_down); A(subrec_right); A(subrec_left);
+#undef A
+    /* recblocking_preprocess.h:346-348 */
+    orc_geometry(cp, ri, m, lv, substitution, o->loc_off, o->tmp_off, o->blk_m, o->blk_n, o->blk_nnz,
+                 o->subtri_up, o->subtri_down, o->subrec_up, o->subrec_down, o->subrec_right,
+                 o->subrec_left);
+    /* recblocking_preprocess.h:370-384 and recblocking_solver.h:65-67 */
+    o->ptr_size = 1;
+    o->idx_size = 0;
+    o->dcsr_size = 0;
+    for (int i = 0; i < sum; ++i) {
+        if ((i & 1) == 0) {
+            o->ptr_size += o->blk_n[i] + 1;
+            o->idx_size += o->blk_nnz[i];
+        } else {
+            o->ptr_size += o->blk_m[i];
+            o->idx_size += o->blk_nnz[i];
+            o->dcsr_size += o->blk_m[i];
+        }
+    }
+    o->recblock_Ptr = ALLOC_I(o->ptr_size);
+    o->recblock_Index = ALLOC_I(o->idx_size);
+    o->recblock_Val = ALLOC_D(o->idx_size);
+    o->recblock_dcsr_rowidx = ALLOC_I(o->dcsr_size);
+    o->ptr_offset = ALLOC_I(sum + 1);
+    o->index_offset = ALLOC_I(sum + 1);
+    o->dcsrindex_offset = ALLOC_I(sum + 1);
+    o->loc_item_off = ALLOC_I(sum);
+    o->loc_ptr_off = ALLOC_I(sum);
+    o->lvl_item = ALLOC_I(m);
+    o->lvl_ptr = ALLOC_I(m + tri);
+    o->m_lv = ALLOC_I(m + tri);
+    o->offset_lv = ALLOC_I(m + tri);
+    o->nnz_lv = ALLOC_I(m + tri);
+    o->recblock_Ptr[0] = 0;     /* recblocking_solver.h:85 */
+    o->ptr_offset[0] = 1;       /* recblocking_solver.h:92-94 */
+    o->index_offset[0] = 0;
+    o->dcsrindex_offset[0] = 0;
+
+    int *P = o->recblock_Ptr;
+    int nz = 0;          /* recblock_nnz_ptr */
+    int item_off = 0, lptr_off = 0;
+    for (int b = 0; b < sum; ++b) {
+        int bm = o->blk_m[b], bn = o->blk_n[b], bnnz = o->blk_nnz[b];
+        if ((b & 1) == 0) {
+            /* recblocking_preprocess.h:432-451: extract the triangle as CSC */
+            int up = o->subtri_up[b], down = o->subtri_down[b];
+            int *scp = ALLOC_I(bn + 1), *sri = ALLOC_I(bnnz);
+            double *sva = ALLOC_D(bnnz);
+            int q = 0;
+            for (int c = up; c < down; ++c) {
+                for (int k = cp[c]; k < cp[c + 1]; ++k) {
+                    int r = ri[k];
+                    int keep = substitution == ORC_FORWARD ? r < down : r >= up;
+                    if (keep) {
+                        sri[q] = r - up;
+                        sva[q] = va[k];
+                        ++q;
+                    }
+                }
+                scp[c - up + 1] = q;
+            }
+            /* :457-463 CSR copy of the triangle */
+            int *rrp = ALLOC_I(bm + 1), *rci = ALLOC_I(bnnz);
+            double *rva = ALLOC_D(bnnz);
+            orc_transpose(bn, bm, bnnz, scp, sri, sva, rrp, rci, rva);
+            /* :469-484 local level sets unless diagonal-only */
+            int fast = bm == bnnz;
+            int nlv = 1;
+            int *lp = o->lvl_ptr + lptr_off, *li = o->lvl_item + item_off;
+            if (fast) {
+                lp[0] = 0;
+                lp[1] = bm;
+                for (int i = 0; i < bm; ++i) li[i] = i;
+            } else if (orc_findlevel(scp, sri, rrp, bm, &nlv, lp, li) != 0) {
+                free(scp); free(sri); free(sva); free(rrp); free(rci); free(rva);
+                free(cp); free(ri); free(va);
+                return -1;
+            }
+            o->nlv[b] = nlv;
+            o->loc_item_off[b] = item_off;
+            o->loc_ptr_off[b] = lptr_off;
+            int method;
+            if (fast) {
+                method = 0; /* :487-513 */
+            } else {
+                int nnzr = bnnz / bm; /* :516 */
+                if (nlv > 20000) method = 1;                                            /* :518 */
+                else if ((nnzr <= 15 && nlv <= 20) || (nnzr == 1 && nlv <= 100)) method = 2; /* :624 */
+                else method = 3;                                                       /* :664 */
+            }
+            o->method[b] = method;
+            int po = o->ptr_offset[b];
+            if (method == 0 || method == 3) { /* CSC packing :498-508, :698-708 */
+                for (int i = 0; i < bn; ++i) {
+                    for (int k = scp[i]; k < scp[i + 1]; ++k) {
+                        o->recblock_Index[nz] = sri[k];
+                        o->recblock_Val[nz] = sva[k];
+                        ++nz;
+                    }
+                    P[po + i] = P[po + i - 1] + scp[i + 1] - scp[i];
+                }
+            } else if (method == 2) { /* CSR packing :652-662, level arrays :632-645 */
+                for (int l = 0; l < nlv; ++l) {
+                    o->m_lv[lptr_off + l] = lp[l + 1] - lp[l];
+                    o->offset_lv[lptr_off + l] = lp[l];
+                    int s = 0;
+                    for (int p = lp[l]; p < lp[l + 1]; ++p) s += rrp[p + 1] - rrp[p];
+                    o->nnz_lv[lptr_off + l] = s;
+                }
+                for (int i = 0; i < bm; ++i) {
+                    for (int k = rrp[i]; k < rrp[i + 1]; ++k) {
+                        o->recblock_Index[nz] = rci[k];
+                        o->recblock_Val[nz] = rva[k];
+                        ++nz;
+                    }
+                    P[po + i] = P[po + i - 1] + rrp[i + 1] - rrp[i];
+                }
+            } else { /* method 1: private zero-based CSR pointer :603-616 */
+                P[po] = 0;
+                int c = 0;
+                for (int i = 0; i < bm; ++i) {
+                    for (int k = rrp[i]; k < rrp[i + 1]; ++k) {
+                        o->recblock_Index[nz] = rci[k];
+                        o->recblock_Val[nz] = rva[k];
+                        ++nz;
+                        ++c;
+                    }
+                    P[po + i + 1] = c;
+                }
+            }
+            /* :726-731 */
+            o->ptr_offset[b + 1] = po + bm + (method == 1 ? 1 : 0);
+            o->index_offset[b + 1] = nz;
+            o->dcsrindex_offset[b + 1] = o->dcsrindex_offset[b];
+            item_off += bm;
+            lptr_off += nlv + 1;
+            free(scp); free(sri); free(sva); free(rrp); free(rci); free(rva);
+        } else {
+            /* :749-776 extract the square as CSC, transpose to CSR */
+            int up = o->subrec_up[b], down = o->subrec_down[b];
+            int left = o->subrec_left[b], right = o->subrec_right[b];
+            int *scp = ALLOC_I(bn + 1), *sri = ALLOC_I(bnnz);
+            double *sva = ALLOC_D(bnnz);
+            int q = 0;
+            for (int c = left; c < right; ++c) {
+                for (int k = cp[c]; k < cp[c + 1]; ++k) {
+                    int r = ri[k];
+                    if (r >= up && r < down) {
+                        sri[q] = r - up;
+                        sva[q] = va[k];
+                        ++q;
+                    }
+                }
+                scp[c - left + 1] = q;
+            }
+            int *rrp = ALLOC_I(bm + 1), *rci = ALLOC_I(bnnz);
+            double *rva = ALLOC_D(bnnz);
+            orc_transpose(bn, bm, bnnz, scp, sri, sva, rrp, rci, rva);
+            /* :783-793 entries in CSR order */
+            for (int i = 0; i < bm; ++i)
+                for (int k = rrp[i]; k < rrp[i + 1]; ++k) {
+                    o->recblock_Index[nz] = rci[k];
+                    o->recblock_Val[nz] = rva[k];
+                    ++nz;
+                }
+            /* :800-826 row statistics */
+            int nonempty = 0, lenmax = bm > 0 ? rrp[1] - rrp[0] : 0, longrow = 0, longlen = 0;
+            for (int i = 1; i <= bm; ++i) {
+                int len = rrp[i] - rrp[i - 1];
+                if (len > lenmax) lenmax = len;
+                if (len != 0) {
+                    if (len > ORC_LONGROW_THRESHOLD) {
+                        ++longrow;
+                        longlen += len;
+                    }
+                    ++nonempty;
+                }
+            }
+            o->m_new[b] = nonempty;
+            o->longrow[b] = longrow;
+            o->lenmax[b] = lenmax;
+            int po = o->ptr_offset[b];
+            int real_i = 0, dcsr_i = 0, method = -1;
+            if (bnnz != 0) { /* an empty square divides by zero at :825 in the reference */
+                int nnzr = (bnnz - longlen) / nonempty;
+                double empty_ratio = 100 * (double)(bm - nonempty) / (double)bm;
+                if (nnzr <= 12 && empty_ratio <= 50) method = 0;       /* :835 */
+                else if (nnzr <= 12 && empty_ratio > 50) method = 1;   /* :856 */
+                else if (nnzr > 12 && empty_ratio <= 15) method = 2;   /* :880 */
+                else method = 3;                                       /* :898 */
+                if (method == 0 || method == 2) {
+                    for (int i = 0; i < bm; ++i) P[po + i] = P[po + i - 1] + rrp[i + 1] - rrp[i];
+                    real_i = bm;
+                } else {
+                    int dbase = o->dcsrindex_offset[b];
+                    for (int i = 0; i < bm; ++i) {
+                        if (rrp[i + 1] != rrp[i]) {
+                            P[po + dcsr_i] = P[po + dcsr_i - 1] + rrp[i + 1] - rrp[i];
+                            o->recblock_dcsr_rowidx[dbase + dcsr_i] = i;
+                            ++dcsr_i;
+                        }
+                    }
+                    real_i = dcsr_i;
+                }
+            }
+            o->method[b] = method;
+            o->nlv[b] = 0;
+            /* :952-954 */
+            o->ptr_offset[b + 1] = po + real_i;
+            o->index_offset[b + 1] = nz;
+            o->dcsrindex_offset[b + 1] = o->dcsrindex_offset[b] + dcsr_i;
+            free(scp); free(sri); free(sva); free(rrp); free(rci); free(rva);
+        }
+    }
+    free(cp); free(ri); free(va);
+    return 0;
+}
+
+void orc_blocks_free(orc_blocks *o) {
+    void *ps[] = {o->method, o->nlv, o->m_new, o->longrow, o->lenmax, o->loc_off, o->tmp_off,
+                  o->blk_m, o->blk_n, o->blk_nnz, o->subtri_up, o->subtri_down, o->subrec_up,
+                  o->subrec_down, o->subrec_right, o->subrec_left, o->ptr_offset, o->index_offset,
+                  o->dcsrindex_offset, o->recblock_Ptr, o->recblock_Index, o->recblock_Val,
+                  o->recblock_dcsr_rowidx, o->levelItem, o->loc_item_off, o->loc_ptr_off,
+                  o->lvl_item, o->lvl_ptr, o->m_lv, o->offset_lv, o->nnz_lv};
+    for (size_t i = 0; i < sizeof(ps) / sizeof(ps[0]); ++i) free(ps[i]);
+    memset(o, 0, sizeof(*o));
+}
+
+int orc_auto_lv(int m, int device_id) {
+    /* main.cu:245-254 */
+    int li;
+    for (li = 1; li <= 100; ++li)
+        if (m / pow(2, li + 1) < (device_id == 0 ? 92160 : 58880)) break;
+    return li;
+}
+
+static int find_diag(const int *rowptr, const int *colidx, int i) {
+    for (int k = rowptr[i]; k < rowptr[i + 1]; ++k)
+        if (colidx[k] == i) return k;
+    return -1;
+}
+
+int orc_sptrsv_csr(int n, const int *rowptr, const int *colidx, const double *val,
+                   int substitution, const double *b, double *x) {
+    for (int s = 0; s < n; ++s) {
+        int i = substitution == ORC_FORWARD ? s : n - 1 - s;
+        int d = find_diag(rowptr, colidx, i);
+        if (d < 0 || val[d] == 0.0) return -1;
+        double acc = 0.0;
+        for (int k = rowptr[i]; k < rowptr[i + 1]; ++k)
+            if (k != d) acc += val[k] * x[colidx[k]];
+        x[i] = (b[i] - acc) / val[d];
+    }
+    return 0;
+}
+
+int orc_sptrsv_csr_compensated(int n, const int *rowptr, const int *colidx, const double *val,
+                               int substitution, const double *b, double *x) {
+    /* Neumaier's improved Kahan summation of b_i - sum_j a_ij x_j */
+    for (int s = 0; s < n; ++s) {
+        int i = substitution == ORC_FORWARD ? s : n - 1 - s;
+        int d = find_diag(rowptr, colidx, i);
+        if (d < 0 || val[d] == 0.0) return -1;
+        double sum = b[i], comp = 0.0;
+        for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+            if (k == d) continue;
+            double term = -(val[k] * x[colidx[k]]);
+            double t = sum + term;
+            if (fabs(sum) >= fabs(term)) comp += (sum - t) + term;
+            else comp += (term - t) + sum;
+            sum = t;
+        }
+        x[i] = (sum + comp) / val[d];
+    }
+    return 0;
+}
+
+int orc_sptrsv_csr_multi(int n, const int *rowptr, const int *colidx, const double *val,
+                         int substitution, int k, const double *b, int ldb, double *x, int ldx) {
+    for (int c = 0; c < k; ++c)
+        if (orc_sptrsv_csr(n, rowptr, colidx, val, substitution, b + (size_t)c * ldb,
+                           x + (size_t)c * ldx) != 0)
+            return -1;
+    return 0;
+}
+
+void orc_spmv_csr(int n, const int *rowptr, const int *colidx, const double *val,
+                  const double *x, double *y) {
+    for (int i = 0; i < n; ++i) {
+        double acc = 0.0;
+        for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) acc += val[k] * x[colidx[k]];
+        y[i] = acc;
+    }
+}

@@ -1,0 +1,102 @@
+/*
+ * oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C restatement of recblock-sptrsv's CPU analysis and a serial FP64
+ * substitution, used as the checker for the B200 library.  Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it; the
+ * product never links or calls it.
+ *
+ * Parity pin: the integer outputs of this restatement are checked against
+ * golden vectors produced by the reference's own analysis code
+ * (recblocking_preprocess.h get_recblock_size + L_/U_preprocessing), compiled
+ * from the reference sources by oracle/Makefile into oracle/_ref/.
+ *
+ * The value oracle (orc_sptrsv_csr) is a restatement of textbook serial
+ * substitution: the reference has no CPU triangular solve; its only value
+ * check is main.cu:296-317 against x_ref.
+ */
+#ifndef RBS_ORACLE_H
+#define RBS_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_FORWARD 0  /* common.h:25 SUBSTITUTION_FORWARD */
+#define ORC_BACKWARD 1 /* common.h:26 SUBSTITUTION_BACKWARD */
+#define ORC_LONGROW_THRESHOLD 2048 /* utils_spmv_cuda.h:9 */
+
+/* tranpose.h:7-54 -- CSR(m x n) -> CSC, stable by rows.  val/tval may be NULL. */
+void orc_transpose(int m, int n, int nnz, const int *ptr, const int *idx, const double *val,
+                   int *tptr, int *tidx, double *tval);
+
+/* findlevel.h:7-83 -- Kahn BFS level sets in discovery order.
+ * Returns 0, or -1 when a level makes no progress (the reference loops forever there). */
+int orc_findlevel(const int *cscColPtr, const int *cscRowIdx, const int *csrRowPtr, int m,
+                  int *nlevel, int *levelPtr, int *levelItem);
+
+/* utils_reordering.h:102-210 -- symmetric level-set permutation of a CSC. */
+int orc_reorder_colrow(const int *colptr, const int *rowidx, const double *val, int m, int nnz,
+                       int substitution, int *colptr_new, int *rowidx_new, double *val_new,
+                       int *levelItem);
+
+/* recblocking_preprocess.h:15-296 -- recursive-block geometry.  All arrays
+ * have 2^(lv+1)-1 entries; entries that the reference leaves unset are
+ * written as -1 here. */
+void orc_geometry(const int *colptr, const int *rowidx, int m, int lv, int substitution,
+                  int *loc_off, int *tmp_off, int *blk_m, int *blk_n, int *blk_nnz,
+                  int *subtri_up, int *subtri_down, int *subrec_up, int *subrec_down,
+                  int *subrec_right, int *subrec_left);
+
+/* Outputs of L_preprocessing / U_preprocessing (recblocking_preprocess.h:387-967, 969-1474). */
+typedef struct orc_blocks {
+    int lv, sum_block, m, nnz;
+    int ptr_size, idx_size, dcsr_size;   /* get_recblock_size :370-384 */
+    int *method;        /* [sum_block] tri: 0..3, square: 0..3, -1 empty square */
+    int *nlv;           /* [sum_block] local levels of tri blocks (1 for fasttrack), 0 for squares */
+    int *m_new;         /* [sum_block] nonempty rows of square blocks */
+    int *longrow;       /* [sum_block] rows longer than 2048 in square blocks */
+    int *lenmax;        /* [sum_block] longest row of square blocks */
+    int *loc_off, *tmp_off, *blk_m, *blk_n, *blk_nnz;
+    int *subtri_up, *subtri_down, *subrec_up, *subrec_down, *subrec_right, *subrec_left;
+    int *ptr_offset, *index_offset, *dcsrindex_offset;  /* [sum_block+1] */
+    int *recblock_Ptr;     /* [ptr_size] (unwritten tail entries are 0) */
+    int *recblock_Index;   /* [idx_size] */
+    double *recblock_Val;  /* [idx_size] */
+    int *recblock_dcsr_rowidx; /* [dcsr_size] (unwritten tail entries are 0) */
+    int *levelItem;        /* [m] global level order (reversed for backward) */
+    /* local level sets of tri blocks, concatenated: block b occupies
+     * lvl_item[loc_item_off[b] .. +blk_m[b]) and lvl_ptr[loc_ptr_off[b] .. +nlv[b]+1) */
+    int *loc_item_off, *loc_ptr_off, *lvl_item, *lvl_ptr;
+    /* method-2 per-level arrays, concatenated like lvl_ptr (nlv entries each) */
+    int *m_lv, *offset_lv, *nnz_lv;
+} orc_blocks;
+
+/* Full CPU analysis: reorder + geometry + per-block extraction, method choice
+ * and packing, on a CSC triangular input.  Returns 0, or -1 on a structure the
+ * reference cannot handle (level search stuck). */
+int orc_analyse(const int *colptr, const int *rowidx, const double *val, int m, int nnz,
+                int substitution, int lv, orc_blocks *out);
+void orc_blocks_free(orc_blocks *b);
+
+/* main.cu:245-254 -- automatic recursion depth for lv == -1. */
+int orc_auto_lv(int m, int device_id);
+
+/* Serial FP64 substitution on CSR.  lower: x_i = (b_i - sum_{j<i} L_ij x_j)/L_ii
+ * for i ascending; upper: descending.  Returns -1 on a zero/missing diagonal. */
+int orc_sptrsv_csr(int n, const int *rowptr, const int *colidx, const double *val,
+                   int substitution, const double *b, double *x);
+/* Same with Neumaier-compensated row sums (bounds the oracle's own rounding). */
+int orc_sptrsv_csr_compensated(int n, const int *rowptr, const int *colidx, const double *val,
+                               int substitution, const double *b, double *x);
+/* k right-hand sides, column-major with leading dimension ld. */
+int orc_sptrsv_csr_multi(int n, const int *rowptr, const int *colidx, const double *val,
+                         int substitution, int k, const double *b, int ldb, double *x, int ldx);
+/* y = A x  (CSR) */
+void orc_spmv_csr(int n, const int *rowptr, const int *colidx, const double *val,
+                  const double *x, double *y);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

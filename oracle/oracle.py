@@ -1,0 +1,183 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of liboracle.so (oracle.c).
+
+Loaded by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
+the checker; the library under test never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+REF_DUMP = os.path.join(_HERE, "_ref", "ref_dump")
+
+FORWARD, BACKWARD = 0, 1
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE, "oracle"], check=True)
+
+
+if not os.path.exists(_LIB):
+    build()
+
+lib = ctypes.CDLL(_LIB)
+_ip = ctypes.POINTER(ctypes.c_int)
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class Blocks(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_int) for f in ("lv", "sum_block", "m", "nnz", "ptr_size", "idx_size", "dcsr_size")] + [
+        (f, _ip) for f in ("method", "nlv", "m_new", "longrow", "lenmax", "loc_off", "tmp_off", "blk_m", "blk_n",
+                           "blk_nnz", "subtri_up", "subtri_down", "subrec_up", "subrec_down", "subrec_right",
+                           "subrec_left", "ptr_offset", "index_offset", "dcsrindex_offset", "recblock_Ptr",
+                           "recblock_Index")
+    ] + [("recblock_Val", _dp)] + [
+        (f, _ip) for f in ("recblock_dcsr_rowidx", "levelItem", "loc_item_off", "loc_ptr_off", "lvl_item", "lvl_ptr",
+                           "m_lv", "offset_lv", "nnz_lv")
+    ]
+
+
+lib.orc_analyse.argtypes = [_ip, _ip, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                            ctypes.POINTER(Blocks)]
+lib.orc_blocks_free.argtypes = [ctypes.POINTER(Blocks)]
+lib.orc_sptrsv_csr.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, _dp, _dp]
+lib.orc_sptrsv_csr_compensated.argtypes = lib.orc_sptrsv_csr.argtypes
+lib.orc_spmv_csr.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp, _dp]
+lib.orc_spmv_csr.restype = None
+lib.orc_transpose.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _ip, _ip, _dp]
+lib.orc_transpose.restype = None
+lib.orc_auto_lv.argtypes = [ctypes.c_int, ctypes.c_int]
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def transpose(ptr, idx, val, ncols=None):
+    """CSR(rows) -> CSC, stable (tranpose.h:7-54)."""
+    ptr, idx, val = _i(ptr), _i(idx), _d(val)
+    m = len(ptr) - 1
+    n = m if ncols is None else ncols
+    tp = np.zeros(n + 1, np.int32)
+    ti = np.zeros(max(len(idx), 1), np.int32)
+    tv = np.zeros(max(len(idx), 1), np.float64)
+    lib.orc_transpose(m, n, len(idx), ptr.ctypes.data_as(_ip), idx.ctypes.data_as(_ip), val.ctypes.data_as(_dp),
+                      tp.ctypes.data_as(_ip), ti.ctypes.data_as(_ip), tv.ctypes.data_as(_dp))
+    return tp, ti[: len(idx)], tv[: len(idx)]
+
+
+def auto_lv(m, device_id=0):
+    return lib.orc_auto_lv(m, device_id)
+
+
+def analyse(colptr, rowidx, val, substitution, lv):
+    """Restated reference analysis; returns a dict of numpy arrays named like the reference's variables."""
+    cp, ri, va = _i(colptr), _i(rowidx), _d(val)
+    m = len(cp) - 1
+    b = Blocks()
+    rc = lib.orc_analyse(cp.ctypes.data_as(_ip), ri.ctypes.data_as(_ip), va.ctypes.data_as(_dp), m, len(ri),
+                         substitution, lv, ctypes.byref(b))
+    if rc != 0:
+        raise RuntimeError("oracle analysis: level search stuck")
+    s = b.sum_block
+
+    def arr(p, n, dt=np.int32):
+        return np.ctypeslib.as_array(p, shape=(max(n, 1),))[:n].astype(dt).copy()
+
+    out = {}
+    for f in ("method", "nlv", "m_new", "longrow", "lenmax", "loc_off", "tmp_off", "blk_m", "blk_n", "blk_nnz",
+              "subtri_up", "subtri_down", "subrec_up", "subrec_down", "subrec_right", "subrec_left"):
+        out[f] = arr(getattr(b, f), s)
+    for f in ("ptr_offset", "index_offset", "dcsrindex_offset"):
+        out[f] = arr(getattr(b, f), s + 1)
+    out["sizes"] = np.array([b.ptr_size, b.idx_size, b.dcsr_size], np.int32)
+    out["recblock_Ptr"] = arr(b.recblock_Ptr, int(out["ptr_offset"][s]))
+    out["recblock_Index"] = arr(b.recblock_Index, int(out["index_offset"][s]))
+    out["recblock_Val"] = arr(b.recblock_Val, int(out["index_offset"][s]), np.float64)
+    out["recblock_dcsr_rowidx"] = arr(b.recblock_dcsr_rowidx, int(out["dcsrindex_offset"][s]))
+    out["levelItem"] = arr(b.levelItem, m)
+    # local level sets of the triangles, concatenated in block order
+    lp, li, mlv, olv, nlvv = [], [], [], [], []
+    lvl_ptr_all = np.ctypeslib.as_array(b.lvl_ptr, shape=(m + (1 << lv),))
+    lvl_item_all = np.ctypeslib.as_array(b.lvl_item, shape=(m,))
+    mlv_all = np.ctypeslib.as_array(b.m_lv, shape=(m + (1 << lv),))
+    olv_all = np.ctypeslib.as_array(b.offset_lv, shape=(m + (1 << lv),))
+    nnzlv_all = np.ctypeslib.as_array(b.nnz_lv, shape=(m + (1 << lv),))
+    ptr_off = np.ctypeslib.as_array(b.loc_ptr_off, shape=(s,))
+    item_off = np.ctypeslib.as_array(b.loc_item_off, shape=(s,))
+    for blk in range(0, s, 2):
+        nl = int(out["nlv"][blk])
+        po, io, bm = int(ptr_off[blk]), int(item_off[blk]), int(out["blk_m"][blk])
+        lp.append(lvl_ptr_all[po:po + nl + 1])
+        li.append(lvl_item_all[io:io + bm])
+        if out["method"][blk] == 2:
+            mlv.append(mlv_all[po:po + nl])
+            olv.append(olv_all[po:po + nl])
+            nlvv.append(nnzlv_all[po:po + nl])
+    cat = lambda xs: np.concatenate(xs).astype(np.int32) if xs else np.zeros(0, np.int32)
+    out["lvl_ptr"], out["lvl_item"] = cat(lp), cat(li)
+    out["m_lv"], out["offset_lv"], out["nnz_lv"] = cat(mlv), cat(olv), cat(nlvv)
+    lib.orc_blocks_free(ctypes.byref(b))
+    return out
+
+
+def sptrsv_csr(rowptr, colidx, val, substitution, b, compensated=False):
+    """Serial FP64 substitution; b may be (n,) or (k, n)."""
+    rp, ci, va = _i(rowptr), _i(colidx), _d(val)
+    b = _d(b)
+    n = len(rp) - 1
+    f = lib.orc_sptrsv_csr_compensated if compensated else lib.orc_sptrsv_csr
+    bs = b.reshape(-1, n)
+    xs = np.zeros_like(bs)
+    for c in range(bs.shape[0]):
+        bc = np.ascontiguousarray(bs[c])
+        xc = np.zeros(n)
+        if f(n, rp.ctypes.data_as(_ip), ci.ctypes.data_as(_ip), va.ctypes.data_as(_dp), substitution,
+             bc.ctypes.data_as(_dp), xc.ctypes.data_as(_dp)) != 0:
+            raise RuntimeError("oracle substitution: zero or missing diagonal")
+        xs[c] = xc
+    return xs.reshape(b.shape)
+
+
+def spmv_csr(rowptr, colidx, val, x):
+    rp, ci, va, x = _i(rowptr), _i(colidx), _d(val), _d(x)
+    y = np.zeros(len(rp) - 1)
+    lib.orc_spmv_csr(len(rp) - 1, rp.ctypes.data_as(_ip), ci.ctypes.data_as(_ip), va.ctypes.data_as(_dp),
+                     x.ctypes.data_as(_dp), y.ctypes.data_as(_dp))
+    return y
+
+
+def run_reference_dump(colptr, rowidx, val, substitution, lv, workdir):
+    """Run the reference's own analysis (oracle/_ref/ref_dump) and read its outputs."""
+    cp, ri, va = _i(colptr), _i(rowidx), _d(val)
+    m = len(cp) - 1
+    inp = os.path.join(workdir, "ref_in.bin")
+    outp = os.path.join(workdir, "ref_out.bin")
+    with open(inp, "wb") as f:
+        np.array([m, len(ri), substitution, lv], np.int32).tofile(f)
+        cp.tofile(f)
+        ri.tofile(f)
+        va.tofile(f)
+    subprocess.run([REF_DUMP, inp, outp], check=True, stdout=subprocess.DEVNULL)
+    res = {}
+    with open(outp, "rb") as f:
+        data = f.read()
+    pos = 0
+    while pos < len(data):
+        name = data[pos:pos + 32].split(b"\0")[0].decode()
+        kind = int(np.frombuffer(data, np.int32, 1, pos + 32)[0])
+        cnt = int(np.frombuffer(data, np.int64, 1, pos + 36)[0])
+        pos += 44
+        dt = np.int32 if kind == 0 else np.float64
+        res[name] = np.frombuffer(data, dt, cnt, pos).copy()
+        pos += cnt * np.dtype(dt).itemsize
+    return res

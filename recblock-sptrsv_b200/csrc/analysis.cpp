@@ -1,0 +1,719 @@
+// analysis.cpp -- host analysis: validation, level sets, level-set
+// permutation, recursive-block geometry, per-block statistics, the
+// reference's per-block method codes, kernel selection and the
+// processing-order execution layout.
+//
+// Integer outputs that the reference also produces (level order, labels,
+// block bounds, nnz per block, method codes, local level counts, packed
+// arrays) are bit-identical to recblock-sptrsv's CPU analysis
+// (recblocking_preprocess.h get_recblock_size + L_/U_preprocessing); the
+// packed reference-format arrays are rebuilt on demand by export_reference.
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+#include "rbs_internal.h"
+
+namespace rbs {
+
+namespace {
+
+constexpr int kLongRow = 2048;  // utils_spmv_cuda.h:9 LONGROW_THRESHOLD
+
+int lowbit(int t) { return t & -t; }
+
+// Stable CSR(rows x cols) -> CSC transposition (tranpose.h:7-54 semantics:
+// entries of a column appear in ascending row order).
+void transpose(int rows, int cols, const int *ptr, const int *idx, const double *val, std::vector<int> &tptr,
+               std::vector<int> &tidx, std::vector<double> &tval) {
+    int nnz = ptr[rows];
+    tptr.assign((size_t)cols + 1, 0);
+    for (int k = 0; k < nnz; ++k) tptr[(size_t)idx[k] + 1]++;
+    for (int c = 0; c < cols; ++c) tptr[(size_t)c + 1] += tptr[c];
+    tidx.resize((size_t)nnz);
+    tval.resize(val ? (size_t)nnz : 0);
+    std::vector<int> fill(tptr.begin(), tptr.end() - 1);
+    for (int r = 0; r < rows; ++r)
+        for (int k = ptr[r]; k < ptr[r + 1]; ++k) {
+            int d = fill[idx[k]]++;
+            tidx[d] = r;
+            if (val) tval[d] = val[k];
+        }
+}
+
+// Kahn breadth-first level sets in the discovery order of findlevel.h:7-83:
+// in-degree = entries per row (diagonal included), a row joins the next
+// level the moment its in-degree reaches 1, levels are walked in the order
+// their rows were discovered and each column in stored order.
+// Returns the level count, or -1 if a level makes no progress.
+int bfs_levels(const int *cp, const int *ri, int m, std::vector<int> &levelPtr, std::vector<int> &item) {
+    std::vector<int> deg((size_t)m, 0);
+    for (int k = 0; k < cp[m]; ++k) deg[ri[k]]++;
+    item.resize((size_t)m);
+    levelPtr.clear();
+    levelPtr.push_back(0);
+    int tail = 0;
+    for (int i = 0; i < m; ++i)
+        if (deg[i] == 1) item[tail++] = i;
+    levelPtr.push_back(tail);
+    int head = 0;
+    while (tail != m) {
+        int end = tail;
+        if (head == end) return -1;  // no root / cycle: the reference spins forever here
+        for (; head < end; ++head) {
+            int node = item[head];
+            for (int k = cp[node]; k < cp[node + 1]; ++k) {
+                int r = ri[k];
+                if (--deg[r] == 1) item[tail++] = r;
+            }
+        }
+        if (tail == end) return -1;
+        levelPtr.push_back(tail);
+    }
+    return (int)levelPtr.size() - 1;
+}
+
+int pick_group(double avg) {
+    if (avg < 3) return 1;
+    if (avg < 6) return 2;
+    if (avg < 12) return 4;
+    if (avg < 24) return 8;
+    if (avg < 48) return 16;
+    return 32;
+}
+
+// Kernel choice.  REFERENCE maps each reference method to this library's
+// kernel of the same kind; AUTO uses a latency/bandwidth cost model of the
+// B200 (constants measured with bench.py, see DESIGN notes in the repo).
+void select_kernel(ExecBlock &b, const rbs_options &opt, const std::vector<int> &lvl_sizes) {
+    if (!b.tri) {
+        if (b.nnz == 0) {
+            b.kernel = RBS_K_EMPTY;
+            b.group = 1;
+            return;
+        }
+        b.kernel = RBS_K_SPMV;
+        double avg = (double)b.nnz / std::max(1, b.nonempty);
+        if (opt.select == RBS_SELECT_REFERENCE)
+            b.group = (b.ref_method == 0 || b.ref_method == 1) ? 1 : 32;
+        else
+            b.group = pick_group(avg);
+        return;
+    }
+    int off = b.nnz - b.m;  // strictly off-diagonal entries
+    double avg = (double)off / std::max(1, b.m);
+    b.group = pick_group(avg);
+    if (off == 0) {
+        b.kernel = RBS_K_DIAG;
+        return;
+    }
+    if (opt.select == RBS_SELECT_REFERENCE) {
+        switch (b.ref_method) {
+        case 0: b.kernel = RBS_K_DIAG; break;
+        case 1: b.kernel = b.bandwidth <= 8 ? RBS_K_BANDSCAN : RBS_K_SEQ; break;
+        case 2: b.kernel = RBS_K_LEVEL; break;
+        default: b.kernel = RBS_K_SYNCFREE; break;
+        }
+        return;
+    }
+    // AUTO cost model (microseconds).
+    double bytes = (double)off * 12.0 + (double)b.m * 24.0;
+    double passes = 0;
+    for (int w : lvl_sizes) passes += std::max(1.0, std::ceil((double)w * b.group / 1024.0));
+    double t_level = passes * 0.12 + bytes / 180e3 + 4.0;
+    double t_sync = (double)b.nlv * 0.9 + bytes / 4.0e6 + 4.0;
+    double t_seq = (double)b.m * 0.012 + bytes / 120e3 + 4.0;
+    double t_scan = b.bandwidth <= 8 ? bytes * 3.0 / 3.0e6 + 25.0 : 1e30;
+    double best = t_sync;
+    b.kernel = RBS_K_SYNCFREE;
+    if (t_level < best) { best = t_level; b.kernel = RBS_K_LEVEL; }
+    if (t_seq < best) { best = t_seq; b.kernel = RBS_K_SEQ; }
+    if (t_scan < best) { best = t_scan; b.kernel = RBS_K_BANDSCAN; }
+}
+
+}  // namespace
+
+int auto_lv(int m, int device_id) {
+    // main.cu:245-254: smallest li >= 1 with m / 2^(li+1) below the wave size
+    int li;
+    for (li = 1; li <= 100; ++li)
+        if (m / std::pow(2.0, li + 1) < (device_id == 0 ? 92160 : 58880)) break;
+    return li;
+}
+
+int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int n, int nnz, int fmt,
+                 int substitution, int lv, const rbs_options &opt, std::string &err) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (n <= 0 || nnz < n || !ptr || !idx || !val) {
+        err = "rbs_analyse: need n > 0, nnz >= n and non-null arrays";
+        return RBS_ERR_ARG;
+    }
+    if (substitution != RBS_FORWARD && substitution != RBS_BACKWARD) {
+        err = "rbs_analyse: substitution must be RBS_FORWARD or RBS_BACKWARD";
+        return RBS_ERR_ARG;
+    }
+    if (fmt != RBS_FMT_CSC && fmt != RBS_FMT_CSR) {
+        err = "rbs_analyse: fmt must be RBS_FMT_CSC or RBS_FMT_CSR";
+        return RBS_ERR_ARG;
+    }
+    if (ptr[0] != 0 || ptr[n] != nnz) {
+        err = "rbs_analyse: pointer array must start at 0 and end at nnz";
+        return RBS_ERR_STRUCTURE;
+    }
+    for (int c = 0; c < n; ++c)
+        if (ptr[c + 1] < ptr[c]) {
+            err = "rbs_analyse: pointer array decreases at " + std::to_string(c);
+            return RBS_ERR_STRUCTURE;
+        }
+    for (int k = 0; k < nnz; ++k)
+        if (idx[k] < 0 || idx[k] >= n) {
+            err = "rbs_analyse: index out of range at entry " + std::to_string(k);
+            return RBS_ERR_STRUCTURE;
+        }
+    P.opt = opt;
+    P.n = n;
+    P.nnz = nnz;
+    P.sub = substitution;
+    // 1. the reference's input layout: CSC with the diagonal first (forward)
+    //    or last (backward) in every column
+    if (fmt == RBS_FMT_CSR) {
+        transpose(n, n, ptr, idx, val, P.in_cp, P.in_ri, P.in_va);
+    } else {
+        P.in_cp.assign(ptr, ptr + n + 1);
+        P.in_ri.assign(idx, idx + nnz);
+        P.in_va.assign(val, val + nnz);
+    }
+    const int *cp = P.in_cp.data(), *ri = P.in_ri.data();
+    const double *va = P.in_va.data();
+    for (int c = 0; c < n; ++c) {
+        int b = cp[c], e = cp[c + 1];
+        if (b == e) {
+            err = "rbs_analyse: column " + std::to_string(c) + " has no diagonal";
+            return RBS_ERR_STRUCTURE;
+        }
+        int dpos = substitution == RBS_FORWARD ? b : e - 1;
+        if (ri[dpos] != c) {
+            err = "rbs_analyse: diagonal of column " + std::to_string(c) + " missing or not " +
+                  (substitution == RBS_FORWARD ? "first" : "last");
+            return RBS_ERR_STRUCTURE;
+        }
+        if (va[dpos] == 0.0) {
+            err = "rbs_analyse: zero diagonal in column " + std::to_string(c);
+            return RBS_ERR_STRUCTURE;
+        }
+        for (int k = b; k < e; ++k) {
+            int r = ri[k];
+            bool ok = substitution == RBS_FORWARD ? r >= c : r <= c;
+            if (!ok) {
+                err = "rbs_analyse: entry (" + std::to_string(r) + "," + std::to_string(c) + ") outside the " +
+                      (substitution == RBS_FORWARD ? "lower" : "upper") + " triangle";
+                return RBS_ERR_STRUCTURE;
+            }
+            if (k != dpos && r == c) {
+                err = "rbs_analyse: duplicate diagonal in column " + std::to_string(c);
+                return RBS_ERR_STRUCTURE;
+            }
+        }
+    }
+    // 2. recursion depth (main.cu:245-254 for lv == -1)
+    if (lv == -1) {
+        lv = auto_lv(n, opt.lv_device_id);
+        while (lv > 0 && (1 << lv) > n) --lv;
+    }
+    if (lv < 0 || lv > 24 || (1 << lv) > n) {
+        err = "rbs_analyse: lv must satisfy 0 <= lv and 2^lv <= n";
+        return RBS_ERR_ARG;
+    }
+    P.lv = lv;
+    const int T = 1 << lv;
+    P.sum_block = 2 * T - 1;
+    P.step = n / T;
+    const int s = P.step;
+
+    // 3. level sets in the reference's discovery order
+    int nlevel = bfs_levels(cp, ri, n, P.bfs_ptr, P.bfs_item);
+    if (nlevel < 0) {
+        err = "rbs_analyse: level search stuck (dependency cycle)";
+        return RBS_ERR_STRUCTURE;
+    }
+    P.nlevel = nlevel;
+    // labels (utils_reordering.h:130-159) and processing positions
+    P.label.resize(n);
+    P.perm.resize(n);
+    std::vector<int> pos_of((size_t)n);
+    for (int i = 0; i < n; ++i) {
+        int orig = P.bfs_item[i];
+        P.label[orig] = substitution == RBS_FORWARD ? i : n - 1 - i;
+        P.perm[i] = orig;  // processing position i is BFS position i in both directions
+        pos_of[orig] = i;
+    }
+
+    // 4. processing-order CSR with columns ascending (two stable counting
+    //    sorts: by column, then by row)
+    {
+        std::vector<int> P_of((size_t)nnz), Q_of((size_t)nnz);
+        for (int c = 0; c < n; ++c)
+            for (int k = cp[c]; k < cp[c + 1]; ++k) {
+                P_of[k] = pos_of[ri[k]];
+                Q_of[k] = pos_of[c];
+            }
+        std::vector<int> byq((size_t)n + 1, 0), order1((size_t)nnz);
+        for (int k = 0; k < nnz; ++k) byq[(size_t)Q_of[k] + 1]++;
+        for (int q = 0; q < n; ++q) byq[(size_t)q + 1] += byq[q];
+        for (int k = 0; k < nnz; ++k) order1[byq[Q_of[k]]++] = k;
+        P.full_rp.assign((size_t)n + 1, 0);
+        for (int k = 0; k < nnz; ++k) P.full_rp[(size_t)P_of[k] + 1]++;
+        for (int p = 0; p < n; ++p) P.full_rp[(size_t)p + 1] += P.full_rp[p];
+        std::vector<int> fill(P.full_rp.begin(), P.full_rp.end() - 1);
+        P.full_col.resize((size_t)nnz);
+        P.full_val.resize((size_t)nnz);
+        for (int t = 0; t < nnz; ++t) {
+            int k = order1[t];
+            int d = fill[P_of[k]]++;
+            P.full_col[d] = Q_of[k];
+            P.full_val[d] = va[k];
+        }
+    }
+    const int *frp = P.full_rp.data(), *fcol = P.full_col.data();
+    const double *fval = P.full_val.data();
+
+    // 5. blocks in processing coordinates
+    auto tri_of = [&](int p) { return std::min(p / s, T - 1); };
+    P.blocks.assign((size_t)P.sum_block, ExecBlock{});
+    for (int b = 0; b < P.sum_block; ++b) {
+        ExecBlock &B = P.blocks[b];
+        B.index = b;
+        B.tri = (b & 1) == 0;
+        B.rows_off = B.long_off = B.map_off = B.lvl_off = -1;
+        if (B.tri) {
+            int i = b / 2;
+            B.r0 = i * s;
+            B.m = (i == T - 1 ? n : (i + 1) * s) - B.r0;
+            B.c0 = B.r0;
+            B.ncols = B.m;
+        } else {
+            int t = (b + 1) / 2, lb = lowbit(t);
+            B.r0 = t * s;
+            B.m = (t + lb == T ? n : (t + lb) * s) - B.r0;
+            B.c0 = (t - lb) * s;
+            B.ncols = t * s - B.c0;
+        }
+    }
+    // per-row entry counts of every block, local levels, bandwidth
+    std::vector<std::vector<int>> rowcnt((size_t)P.sum_block);
+    for (int b = 0; b < P.sum_block; ++b) rowcnt[b].assign((size_t)P.blocks[b].m, 0);
+    std::vector<int> level((size_t)n, 0);
+    P.inv_diag.resize((size_t)n);
+    for (int p = 0; p < n; ++p) {
+        int i = tri_of(p);
+        int tb = 2 * i;
+        ExecBlock &TB = P.blocks[tb];
+        int lvmax = -1, minq = p;
+        for (int k = frp[p]; k < frp[p + 1]; ++k) {
+            int q = fcol[k];
+            if (q == p) {
+                P.inv_diag[p] = 1.0 / fval[k];
+                continue;
+            }
+            if (q >= TB.r0) {
+                rowcnt[tb][p - TB.r0]++;
+                lvmax = std::max(lvmax, level[q]);
+                minq = std::min(minq, q);
+            } else {
+                int j = tri_of(q);
+                int h = 31 - __builtin_clz((unsigned)(i ^ j));
+                int t = i & ~((1 << h) - 1);
+                int sb = 2 * t - 1;
+                rowcnt[sb][p - P.blocks[sb].r0]++;
+            }
+        }
+        level[p] = lvmax + 1;
+        TB.bandwidth = std::max(TB.bandwidth, p - minq);
+    }
+    // block statistics and the reference's method codes
+    std::vector<std::vector<int>> lvl_sizes((size_t)P.sum_block);
+    for (int b = 0; b < P.sum_block; ++b) {
+        ExecBlock &B = P.blocks[b];
+        long long tot = 0;
+        int nonempty = 0, longrows = 0, lenmax = B.m > 0 ? rowcnt[b][0] : 0;
+        long long longlen = 0;
+        for (int r = 0; r < B.m; ++r) {
+            int c = rowcnt[b][r];
+            tot += c;
+            lenmax = std::max(lenmax, c);
+            if (c) {
+                ++nonempty;
+                if (c > kLongRow) {
+                    ++longrows;
+                    longlen += c;
+                }
+            }
+        }
+        if (B.tri) {
+            B.nnz = (int)(tot + B.m);
+            int nl = 0;
+            for (int r = 0; r < B.m; ++r) nl = std::max(nl, level[B.r0 + r] + 1);
+            B.nlv = B.nnz == B.m ? 1 : nl;  // recblocking_preprocess.h:478-479
+            lvl_sizes[b].assign((size_t)B.nlv, 0);
+            int contiguous = 1;
+            for (int r = 0; r < B.m; ++r) {
+                int L = B.nnz == B.m ? 0 : level[B.r0 + r];
+                lvl_sizes[b][L]++;
+                if (r > 0 && L < (B.nnz == B.m ? 0 : level[B.r0 + r - 1])) contiguous = 0;
+            }
+            B.contiguous = contiguous;
+            B.maxwidth = *std::max_element(lvl_sizes[b].begin(), lvl_sizes[b].end());
+            // recblocking_preprocess.h:472-709
+            if (B.nnz == B.m) B.ref_method = 0;
+            else {
+                int nnzr = B.nnz / B.m;
+                if (B.nlv > 20000) B.ref_method = 1;
+                else if ((nnzr <= 15 && B.nlv <= 20) || (nnzr == 1 && B.nlv <= 100)) B.ref_method = 2;
+                else B.ref_method = 3;
+            }
+        } else {
+            B.nnz = (int)tot;
+            B.nonempty = nonempty;
+            B.longrows = longrows;
+            B.lenmax = lenmax;
+            // recblocking_preprocess.h:824-922 (an empty square divides by zero there)
+            if (B.nnz == 0) B.ref_method = -1;
+            else {
+                int nnzr = (int)((B.nnz - longlen) / nonempty);
+                double empty_ratio = 100 * (double)(B.m - nonempty) / (double)B.m;
+                if (nnzr <= 12 && empty_ratio <= 50) B.ref_method = 0;
+                else if (nnzr <= 12 && empty_ratio > 50) B.ref_method = 1;
+                else if (nnzr > 12 && empty_ratio <= 15) B.ref_method = 2;
+                else B.ref_method = 3;
+            }
+        }
+        select_kernel(B, opt, lvl_sizes[b]);
+    }
+
+    // 6. pools.  Squares use a row list (DCSR) when more than half of their
+    //    rows are empty; rows longer than 2048 go to the split kernel.
+    P.rp_pool.clear();
+    P.col_pool.clear();
+    P.val_pool.clear();
+    P.lvl_pool.clear();
+    P.map_pool.clear();
+    P.rows_pool.clear();
+    long long total_entries = 0;
+    for (int b = 0; b < P.sum_block; ++b) total_entries += P.blocks[b].tri ? P.blocks[b].nnz - P.blocks[b].m : P.blocks[b].nnz;
+    P.col_pool.reserve((size_t)total_entries);
+    P.val_pool.reserve((size_t)total_entries);
+    // entry offset of every (block, local row) so the fill is one pass over rows
+    std::vector<std::vector<int>> rowstart((size_t)P.sum_block);
+    long long ent = 0;
+    for (int b = 0; b < P.sum_block; ++b) {
+        ExecBlock &B = P.blocks[b];
+        rowstart[b].resize((size_t)B.m + 1);
+        rowstart[b][0] = (int)ent;
+        for (int r = 0; r < B.m; ++r) rowstart[b][r + 1] = rowstart[b][r] + rowcnt[b][r];
+        ent = rowstart[b][B.m];
+        bool dcsr = !B.tri && B.kernel == RBS_K_SPMV &&
+                    (opt.select == RBS_SELECT_REFERENCE ? (B.ref_method == 1 || B.ref_method == 3)
+                                                        : 2 * B.nonempty < B.m);
+        B.rp_off = (long long)P.rp_pool.size();
+        if (dcsr) {
+            B.rows_off = (long long)P.rows_pool.size();
+            int cnt = 0;
+            for (int r = 0; r < B.m; ++r)
+                if (rowcnt[b][r]) {
+                    P.rows_pool.push_back(r);
+                    P.rp_pool.push_back(rowstart[b][r]);
+                    ++cnt;
+                }
+            P.rp_pool.push_back(rowstart[b][B.m]);
+            B.nrows = cnt;
+        } else {
+            for (int r = 0; r <= B.m; ++r) P.rp_pool.push_back(rowstart[b][r]);
+            B.nrows = B.m;
+        }
+        if (!B.tri && B.longrows) {
+            // positions in the row pointer: the row for CSR, the list index for DCSR
+            B.long_off = (long long)P.rows_pool.size();
+            int pos = 0;
+            for (int r = 0; r < B.m; ++r) {
+                if (dcsr && rowcnt[b][r] == 0) continue;
+                if (rowcnt[b][r] > kLongRow) P.rows_pool.push_back(pos);
+                ++pos;
+            }
+        }
+        if (B.tri && B.kernel == RBS_K_LEVEL) {
+            B.lvl_off = (long long)P.lvl_pool.size();
+            P.lvl_pool.push_back(0);
+            for (int L = 0; L < B.nlv; ++L) P.lvl_pool.push_back(P.lvl_pool.back() + lvl_sizes[b][L]);
+            if (!B.contiguous) {
+                B.map_off = (long long)P.map_pool.size();
+                std::vector<int> fillL(P.lvl_pool.begin() + B.lvl_off, P.lvl_pool.begin() + B.lvl_off + B.nlv);
+                P.map_pool.resize(P.map_pool.size() + (size_t)B.m);
+                for (int r = 0; r < B.m; ++r) {
+                    int L = B.nnz == B.m ? 0 : level[B.r0 + r];
+                    P.map_pool[(size_t)B.map_off + fillL[L]++] = r;
+                }
+            }
+        }
+    }
+    P.col_pool.resize((size_t)ent);
+    P.val_pool.resize((size_t)ent);
+    {
+        std::vector<std::vector<int>> cur((size_t)P.sum_block);
+        for (int b = 0; b < P.sum_block; ++b) cur[b].assign(rowstart[b].begin(), rowstart[b].end() - 1);
+        for (int p = 0; p < n; ++p) {
+            int i = tri_of(p);
+            int tb = 2 * i;
+            const ExecBlock &TB = P.blocks[tb];
+            for (int k = frp[p]; k < frp[p + 1]; ++k) {
+                int q = fcol[k];
+                if (q == p) continue;
+                int b, lc;
+                if (q >= TB.r0) {
+                    b = tb;
+                    lc = q - TB.r0;
+                } else {
+                    int j = tri_of(q);
+                    int h = 31 - __builtin_clz((unsigned)(i ^ j));
+                    int t = i & ~((1 << h) - 1);
+                    b = 2 * t - 1;
+                    lc = q - P.blocks[b].c0;
+                }
+                int d = cur[b][p - P.blocks[b].r0]++;
+                P.col_pool[d] = lc;
+                P.val_pool[d] = fval[k];
+            }
+        }
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    P.analyse_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    return RBS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Reference-format outputs, rebuilt from the plan on request.  This follows
+// recblocking_preprocess.h:298-967 (get_recblock_size, L_preprocessing) and
+// its U twin (:969-1474): the level-permuted CSC keeps each column's entry
+// order, each block is cut out with the reference's bounds filter, triangles
+// get their local level sets from the BFS and are packed as CSC (methods 0,3)
+// or CSR (method 2, method 1 with a private zero-based pointer), squares as
+// CSR or DCSR, and recblock_Ptr blocks share their first entry with the
+// previous block's last entry.
+// ---------------------------------------------------------------------------
+int export_reference(const Plan &P, const std::string &name, std::vector<int> &iv, std::vector<double> &dv,
+                     bool &is_double, std::string &err) {
+    const int n = P.n, nnz = P.nnz, sum = P.sum_block;
+    const bool fwd = P.sub == RBS_FORWARD;
+    is_double = false;
+    iv.clear();
+    dv.clear();
+    auto mirror = [&](int lo, int hi, int &a, int &b) {  // processing range -> reference range
+        if (fwd) { a = lo; b = hi; } else { a = n - hi; b = n - lo; }
+    };
+    // geometry
+    std::vector<int> loc_off(sum, 0), tmp_off(sum, 0), blk_m(sum), blk_n(sum), blk_nnz(sum);
+    std::vector<int> stu(sum, -1), std_(sum, -1), sru(sum, -1), srd(sum, -1), srr(sum, -1), srl(sum, -1);
+    std::vector<int> method(sum), kernel(sum);
+    for (int b = 0; b < sum; ++b) {
+        const ExecBlock &B = P.blocks[b];
+        blk_m[b] = B.m;
+        blk_n[b] = B.ncols;
+        blk_nnz[b] = B.nnz;
+        method[b] = B.ref_method;
+        kernel[b] = B.kernel;
+        if (B.tri) {
+            mirror(B.r0, B.r0 + B.m, stu[b], std_[b]);
+            loc_off[b] = stu[b];
+        } else {
+            mirror(B.r0, B.r0 + B.m, sru[b], srd[b]);
+            mirror(B.c0, B.c0 + B.ncols, srl[b], srr[b]);
+            tmp_off[b] = sru[b];
+            loc_off[b] = srl[b];
+        }
+    }
+    auto put = [&](const std::vector<int> &v) { iv = v; return RBS_OK; };
+    if (name == "loc_off") return put(loc_off);
+    if (name == "tmp_off") return put(tmp_off);
+    if (name == "blk_m") return put(blk_m);
+    if (name == "blk_n") return put(blk_n);
+    if (name == "blk_nnz") return put(blk_nnz);
+    if (name == "subtri_up") return put(stu);
+    if (name == "subtri_down") return put(std_);
+    if (name == "subrec_up") return put(sru);
+    if (name == "subrec_down") return put(srd);
+    if (name == "subrec_right") return put(srr);
+    if (name == "subrec_left") return put(srl);
+    if (name == "method") return put(method);
+    if (name == "kernel") return put(kernel);
+    if (name == "perm") return put(P.perm);
+    if (name == "levelItem") {
+        // utils_reordering.h:189-197: reversed for backward
+        iv = P.bfs_item;
+        if (!fwd) std::reverse(iv.begin(), iv.end());
+        return RBS_OK;
+    }
+    if (name == "levelPtr") return put(P.bfs_ptr);
+    if (name == "sizes") {
+        int ps = 1, is = 0, ds = 0;  // recblocking_preprocess.h:370-384
+        for (int b = 0; b < sum; ++b) {
+            if ((b & 1) == 0) { ps += blk_n[b] + 1; is += blk_nnz[b]; }
+            else { ps += blk_m[b]; is += blk_nnz[b]; ds += blk_m[b]; }
+        }
+        iv = {ps, is, ds};
+        return RBS_OK;
+    }
+    // Everything below needs the reference-order permuted CSC and the
+    // per-block extraction.
+    std::vector<int> cp_new((size_t)n + 1), ri_new((size_t)nnz);
+    std::vector<double> va_new((size_t)nnz);
+    cp_new[0] = 0;
+    for (int i = 0; i < n; ++i) {
+        int src = fwd ? P.bfs_item[i] : P.bfs_item[n - 1 - i];
+        int len = P.in_cp[src + 1] - P.in_cp[src];
+        cp_new[i + 1] = cp_new[i] + len;
+        for (int j = 0; j < len; ++j) {
+            ri_new[cp_new[i] + j] = P.label[P.in_ri[P.in_cp[src] + j]];
+            va_new[cp_new[i] + j] = P.in_va[P.in_cp[src] + j];
+        }
+    }
+    std::vector<int> ptr_offset(sum + 1), index_offset(sum + 1), dcsr_offset(sum + 1);
+    int ps = 1, is = 0, ds = 0;
+    for (int b = 0; b < sum; ++b) {
+        if ((b & 1) == 0) { ps += blk_n[b] + 1; is += blk_nnz[b]; }
+        else { ps += blk_m[b]; is += blk_nnz[b]; ds += blk_m[b]; }
+    }
+    std::vector<int> Ptr((size_t)ps, 0), Index((size_t)std::max(is, 1)), Dcsr((size_t)std::max(ds, 1), 0);
+    std::vector<double> Val((size_t)std::max(is, 1));
+    std::vector<int> nlv(sum, 0), longrow(sum, 0), m_new_dcsr(sum, -1);
+    std::vector<int> lvl_ptr, lvl_item, m_lv, off_lv, nnz_lv;
+    ptr_offset[0] = 1;
+    index_offset[0] = 0;
+    dcsr_offset[0] = 0;
+    int nz = 0;
+    for (int b = 0; b < sum; ++b) {
+        const int bm = blk_m[b], bn = blk_n[b];
+        int po = ptr_offset[b];
+        std::vector<int> scp((size_t)bn + 1, 0), sri;
+        std::vector<double> sva;
+        if ((b & 1) == 0) {
+            int up = stu[b], down = std_[b];
+            for (int c = up; c < down; ++c) {
+                for (int k = cp_new[c]; k < cp_new[c + 1]; ++k) {
+                    int r = ri_new[k];
+                    if (fwd ? r < down : r >= up) {
+                        sri.push_back(r - up);
+                        sva.push_back(va_new[k]);
+                    }
+                }
+                scp[(size_t)(c - up) + 1] = (int)sri.size();
+            }
+            std::vector<int> rrp, rci;
+            std::vector<double> rva;
+            transpose(bn, bm, scp.data(), sri.data(), sva.data(), rrp, rci, rva);
+            std::vector<int> lp, li;
+            int nl = 1;
+            if (bm == (int)sri.size()) {
+                lp = {0, bm};
+                li.resize((size_t)bm);
+                for (int i = 0; i < bm; ++i) li[i] = i;
+            } else {
+                nl = bfs_levels(scp.data(), sri.data(), bm, lp, li);
+                if (nl < 0) { err = "export: local level search stuck"; return RBS_ERR_STRUCTURE; }
+            }
+            nlv[b] = nl;
+            lvl_ptr.insert(lvl_ptr.end(), lp.begin(), lp.end());
+            lvl_item.insert(lvl_item.end(), li.begin(), li.end());
+            int meth = method[b];
+            if (meth == 0 || meth == 3) {
+                for (int i = 0; i < bn; ++i) {
+                    for (int k = scp[i]; k < scp[i + 1]; ++k) { Index[nz] = sri[k]; Val[nz] = sva[k]; ++nz; }
+                    Ptr[po + i] = Ptr[po + i - 1] + scp[i + 1] - scp[i];
+                }
+            } else if (meth == 2) {
+                for (int l = 0; l < nl; ++l) {
+                    m_lv.push_back(lp[l + 1] - lp[l]);
+                    off_lv.push_back(lp[l]);
+                    int sacc = 0;
+                    for (int q = lp[l]; q < lp[l + 1]; ++q) sacc += rrp[q + 1] - rrp[q];
+                    nnz_lv.push_back(sacc);
+                }
+                for (int i = 0; i < bm; ++i) {
+                    for (int k = rrp[i]; k < rrp[i + 1]; ++k) { Index[nz] = rci[k]; Val[nz] = rva[k]; ++nz; }
+                    Ptr[po + i] = Ptr[po + i - 1] + rrp[i + 1] - rrp[i];
+                }
+            } else {
+                Ptr[po] = 0;
+                int c = 0;
+                for (int i = 0; i < bm; ++i) {
+                    for (int k = rrp[i]; k < rrp[i + 1]; ++k) { Index[nz] = rci[k]; Val[nz] = rva[k]; ++nz; ++c; }
+                    Ptr[po + i + 1] = c;
+                }
+            }
+            ptr_offset[b + 1] = po + bm + (meth == 1 ? 1 : 0);
+            index_offset[b + 1] = nz;
+            dcsr_offset[b + 1] = dcsr_offset[b];
+        } else {
+            int up = sru[b], down = srd[b], left = srl[b], right = srr[b];
+            for (int c = left; c < right; ++c) {
+                for (int k = cp_new[c]; k < cp_new[c + 1]; ++k) {
+                    int r = ri_new[k];
+                    if (r >= up && r < down) {
+                        sri.push_back(r - up);
+                        sva.push_back(va_new[k]);
+                    }
+                }
+                scp[(size_t)(c - left) + 1] = (int)sri.size();
+            }
+            std::vector<int> rrp, rci;
+            std::vector<double> rva;
+            transpose(bn, bm, scp.data(), sri.data(), sva.data(), rrp, rci, rva);
+            for (int i = 0; i < bm; ++i)
+                for (int k = rrp[i]; k < rrp[i + 1]; ++k) { Index[nz] = rci[k]; Val[nz] = rva[k]; ++nz; }
+            int real_i = 0, dcsr_i = 0, meth = method[b];
+            int lr = 0;
+            for (int i = 0; i < bm; ++i)
+                if (rrp[i + 1] - rrp[i] > kLongRow) ++lr;
+            longrow[b] = meth >= 0 ? lr : 0;
+            if (meth == 0 || meth == 2) {
+                for (int i = 0; i < bm; ++i) Ptr[po + i] = Ptr[po + i - 1] + rrp[i + 1] - rrp[i];
+                real_i = bm;
+            } else if (meth == 1 || meth == 3) {
+                for (int i = 0; i < bm; ++i)
+                    if (rrp[i + 1] != rrp[i]) {
+                        Ptr[po + dcsr_i] = Ptr[po + dcsr_i - 1] + rrp[i + 1] - rrp[i];
+                        Dcsr[dcsr_offset[b] + dcsr_i] = i;
+                        ++dcsr_i;
+                    }
+                real_i = dcsr_i;
+                m_new_dcsr[b] = dcsr_i;
+            }
+            ptr_offset[b + 1] = po + real_i;
+            index_offset[b + 1] = nz;
+            dcsr_offset[b + 1] = dcsr_offset[b] + dcsr_i;
+        }
+    }
+    if (name == "ptr_offset") return put(ptr_offset);
+    if (name == "index_offset") return put(index_offset);
+    if (name == "dcsrindex_offset") return put(dcsr_offset);
+    if (name == "recblock_Ptr") { iv.assign(Ptr.begin(), Ptr.begin() + ptr_offset[sum]); return RBS_OK; }
+    if (name == "recblock_Index") { iv.assign(Index.begin(), Index.begin() + index_offset[sum]); return RBS_OK; }
+    if (name == "recblock_dcsr_rowidx") { iv.assign(Dcsr.begin(), Dcsr.begin() + dcsr_offset[sum]); return RBS_OK; }
+    if (name == "recblock_Val") {
+        is_double = true;
+        dv.assign(Val.begin(), Val.begin() + index_offset[sum]);
+        return RBS_OK;
+    }
+    if (name == "nlv") return put(nlv);
+    if (name == "longrow") return put(longrow);
+    if (name == "m_new_dcsr") return put(m_new_dcsr);
+    if (name == "lvl_ptr") return put(lvl_ptr);
+    if (name == "lvl_item") return put(lvl_item);
+    if (name == "m_lv") return put(m_lv);
+    if (name == "offset_lv") return put(off_lv);
+    if (name == "nnz_lv") return put(nnz_lv);
+    err = "rbs_plan_export: unknown name '" + name + "'";
+    return RBS_ERR_ARG;
+}
+
+}  // namespace rbs

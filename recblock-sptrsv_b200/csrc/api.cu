@@ -1,0 +1,276 @@
+// api.cu -- the extern "C" boundary declared in include/rbs.h.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "rbs.h"
+#include "rbs_internal.h"
+
+struct rbs_plan {
+    rbs::Plan p;
+};
+
+namespace rbs {
+namespace {
+thread_local std::string g_error;
+}
+void set_error(const std::string &msg) { g_error = msg; }
+}  // namespace rbs
+
+using rbs::set_error;
+
+static int fail(int rc, const std::string &msg) {
+    set_error(msg);
+    return rc;
+}
+
+extern "C" {
+
+const char *rbs_last_error(void) { return rbs::g_error.c_str(); }
+
+void rbs_options_default(rbs_options *opt) {
+    if (!opt) return;
+    std::memset(opt, 0, sizeof(*opt));
+    opt->select = RBS_SELECT_AUTO;
+    opt->device = -1;
+    opt->lv_device_id = 0;
+    opt->host_only = 0;
+    opt->max_rhs = 1;
+    opt->mixed = 1;
+    opt->ir_tol = 1e-13;
+    opt->ir_max_iter = 8;
+    opt->spin_limit = 1LL << 22;
+}
+
+int rbs_auto_lv(int m, int device_id) { return rbs::auto_lv(m, device_id); }
+
+int rbs_analyse(const int *ptr, const int *idx, const double *val, int n, int nnz, int fmt, int substitution, int lv,
+                const rbs_options *opt, rbs_plan **plan) {
+    if (!plan) return fail(RBS_ERR_ARG, "rbs_analyse: plan is NULL");
+    *plan = nullptr;
+    rbs_options o;
+    rbs_options_default(&o);
+    if (opt) o = *opt;
+    if (o.max_rhs < 1) o.max_rhs = 1;
+    if (o.spin_limit <= 0) o.spin_limit = 1LL << 22;
+    if (o.ir_max_iter <= 0) o.ir_max_iter = 8;
+    if (!(o.ir_tol > 0)) o.ir_tol = 1e-13;
+    if (o.select < RBS_SELECT_REFERENCE || o.select > RBS_SELECT_TUNE)
+        return fail(RBS_ERR_ARG, "rbs_analyse: unknown select mode");
+    rbs_plan *P = new (std::nothrow) rbs_plan();
+    if (!P) return fail(RBS_ERR_NOMEM, "rbs_analyse: out of host memory");
+    std::string err;
+    int rc;
+    try {
+        rc = rbs::analyse_host(P->p, ptr, idx, val, n, nnz, fmt, substitution, lv, o, err);
+        if (rc == RBS_OK && !o.host_only) rc = rbs::device_build(P->p, err);
+    } catch (const std::bad_alloc &) {
+        rc = RBS_ERR_NOMEM;
+        err = "rbs_analyse: out of host memory";
+    }
+    if (rc != RBS_OK) {
+        rbs::device_free(P->p);
+        delete P;
+        return fail(rc, err);
+    }
+    *plan = P;
+    set_error("");
+    return RBS_OK;
+}
+
+int rbs_analyse_device(const int *d_ptr, const int *d_idx, const double *d_val, int n, int nnz, int fmt,
+                       int substitution, int lv, const rbs_options *opt, rbs_plan **plan) {
+    if (!plan || !d_ptr || !d_idx || !d_val || n <= 0 || nnz < n)
+        return fail(RBS_ERR_ARG, "rbs_analyse_device: bad arguments");
+    std::vector<int> ptr((size_t)n + 1), idx((size_t)nnz);
+    std::vector<double> val((size_t)nnz);
+    cudaError_t e = cudaMemcpy(ptr.data(), d_ptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(idx.data(), d_idx, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(val.data(), d_val, sizeof(double) * (size_t)nnz, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(RBS_ERR_CUDA, std::string("rbs_analyse_device: ") + cudaGetErrorString(e));
+    return rbs_analyse(ptr.data(), idx.data(), val.data(), n, nnz, fmt, substitution, lv, opt, plan);
+}
+
+static int check_solve_args(rbs_plan *plan, const double *b, const double *x, int k, int ld, int prec) {
+    if (!plan) return fail(RBS_ERR_ARG, "solve: plan is NULL");
+    if (!b || !x) return fail(RBS_ERR_ARG, "solve: b or x is NULL");
+    if (k < 1) return fail(RBS_ERR_ARG, "solve: k must be >= 1");
+    if (ld < plan->p.n) return fail(RBS_ERR_ARG, "solve: ld must be >= n");
+    if (prec != RBS_PREC_FP64 && prec != RBS_PREC_MIXED && prec != RBS_PREC_FP32)
+        return fail(RBS_ERR_ARG, "solve: unknown precision");
+    return RBS_OK;
+}
+
+int rbs_solve(rbs_plan *plan, const double *d_b, double *d_x, int k, int ld, int prec, rbs_stats *stats) {
+    int rc = check_solve_args(plan, d_b, d_x, k, ld, prec);
+    if (rc) return rc;
+    std::string err;
+    rc = rbs::device_solve(plan->p, d_b, d_x, k, ld, prec, true, stats, err);
+    if (rc) return fail(rc, err);
+    return RBS_OK;
+}
+
+int rbs_solve_async(rbs_plan *plan, const double *d_b, double *d_x, int k, int ld, int prec) {
+    int rc = check_solve_args(plan, d_b, d_x, k, ld, prec);
+    if (rc) return rc;
+    if (prec == RBS_PREC_MIXED) return rbs_solve(plan, d_b, d_x, k, ld, prec, nullptr);
+    std::string err;
+    rc = rbs::device_solve(plan->p, d_b, d_x, k, ld, prec, false, nullptr, err);
+    if (rc) return fail(rc, err);
+    return RBS_OK;
+}
+
+int rbs_plan_sync(rbs_plan *plan) {
+    if (!plan || !plan->p.dev) return fail(RBS_ERR_ARG, "rbs_plan_sync: no device plan");
+    std::string err;
+    int rc = rbs::device_sync(plan->p, err);
+    if (rc) return fail(rc, err);
+    return RBS_OK;
+}
+
+int rbs_solve_host(rbs_plan *plan, const double *b, double *x, int k, int ld, int prec, rbs_stats *stats) {
+    int rc = check_solve_args(plan, b, x, k, ld, prec);
+    if (rc) return rc;
+    if (!plan->p.dev) return fail(RBS_ERR_ARG, "rbs_solve_host: plan has no device state");
+    size_t bytes = sizeof(double) * (size_t)ld * (size_t)k;
+    double *db = nullptr, *dx = nullptr;
+    cudaError_t e = cudaMalloc(&db, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&dx, bytes);
+    if (e != cudaSuccess) {
+        cudaFree(db);
+        return fail(RBS_ERR_NOMEM, std::string("rbs_solve_host: ") + cudaGetErrorString(e));
+    }
+    e = cudaMemcpy(db, b, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dx, x, bytes, cudaMemcpyHostToDevice);  // keeps rows beyond n when ld > n
+    if (e != cudaSuccess) {
+        cudaFree(db);
+        cudaFree(dx);
+        return fail(RBS_ERR_CUDA, std::string("rbs_solve_host: ") + cudaGetErrorString(e));
+    }
+    std::string err;
+    rc = rbs::device_solve(plan->p, db, dx, k, ld, prec, true, stats, err);
+    if (rc == RBS_OK || rc == RBS_ERR_NOCONV) {
+        e = cudaMemcpy(x, dx, bytes, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess && rc == RBS_OK) {
+            rc = RBS_ERR_CUDA;
+            err = std::string("rbs_solve_host: ") + cudaGetErrorString(e);
+        }
+    }
+    cudaFree(db);
+    cudaFree(dx);
+    if (rc) return fail(rc, err);
+    return RBS_OK;
+}
+
+int rbs_plan_set_stream(rbs_plan *plan, void *stream) {
+    if (!plan) return fail(RBS_ERR_ARG, "rbs_plan_set_stream: plan is NULL");
+    std::string err;
+    int rc = rbs::device_set_stream(plan->p, stream, err);
+    if (rc) return fail(rc, err);
+    return RBS_OK;
+}
+
+int rbs_plan_info_get(const rbs_plan *plan, rbs_plan_info *info) {
+    if (!plan || !info) return fail(RBS_ERR_ARG, "rbs_plan_info_get: NULL argument");
+    const rbs::Plan &P = plan->p;
+    std::memset(info, 0, sizeof(*info));
+    info->n = P.n;
+    info->nnz = P.nnz;
+    info->lv = P.lv;
+    info->substitution = P.sub;
+    info->nlevel = P.nlevel;
+    info->sum_block = P.sum_block;
+    for (const rbs::ExecBlock &B : P.blocks)
+        if (B.kernel >= 0 && B.kernel < 8) info->kernels[B.kernel]++;
+    info->device_bytes = rbs::device_bytes(P);
+    info->analyse_ms = P.analyse_ms;
+    return RBS_OK;
+}
+
+int rbs_plan_export(const rbs_plan *plan, const char *name, void *dst, long long cap, long long *count) {
+    if (!plan || !name || !count) return fail(RBS_ERR_ARG, "rbs_plan_export: NULL argument");
+    std::vector<int> iv;
+    std::vector<double> dv;
+    bool is_double = false;
+    std::string err;
+    int rc;
+    try {
+        rc = rbs::export_reference(plan->p, name, iv, dv, is_double, err);
+    } catch (const std::bad_alloc &) {
+        return fail(RBS_ERR_NOMEM, "rbs_plan_export: out of host memory");
+    }
+    if (rc) return fail(rc, err);
+    *count = is_double ? (long long)dv.size() : (long long)iv.size();
+    if (!dst) return RBS_OK;
+    if (cap < *count) return fail(RBS_ERR_ARG, "rbs_plan_export: destination too small");
+    if (is_double)
+        std::memcpy(dst, dv.data(), dv.size() * sizeof(double));
+    else
+        std::memcpy(dst, iv.data(), iv.size() * sizeof(int));
+    return RBS_OK;
+}
+
+int rbs_plan_free(rbs_plan *plan) {
+    if (!plan) return RBS_OK;
+    rbs::device_free(plan->p);
+    delete plan;
+    return RBS_OK;
+}
+
+// ---- reference-signature shims ------------------------------------------
+
+static int bench_repeat() {
+    const char *s = std::getenv("RBS_BENCH_REPEAT");  // common.h:13-15 BENCH_REPEAT
+    int r = s ? std::atoi(s) : 200;
+    return r > 0 ? r : 200;
+}
+
+void recblocking_solver_cuda(int *d_cscColPtrTR, int *d_cscRowIdxTR, double *d_cscValTR, int m, int n, int nnzTR,
+                             double *d_x, double *d_b, int substitution, int lv, double *cal_time,
+                             double *preprocess_time) {
+    if (m != n) {
+        set_error("recblocking_solver_cuda: matrix must be square");
+        return;
+    }
+    auto t0 = std::chrono::steady_clock::now();
+    rbs_plan *plan = nullptr;
+    int rc = rbs_analyse_device(d_cscColPtrTR, d_cscRowIdxTR, d_cscValTR, m, nnzTR, RBS_FMT_CSC, substitution, lv,
+                                nullptr, &plan);
+    auto t1 = std::chrono::steady_clock::now();
+    if (rc) return;
+    if (preprocess_time) *preprocess_time = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    // recblocking_calculate.h:37-167: mean over BENCH_REPEAT solves
+    int reps = bench_repeat();
+    double total = 0;
+    for (int r = 0; r < reps && rc == RBS_OK; ++r) {
+        rbs_stats st;
+        rc = rbs_solve(plan, d_b, d_x, 1, m, RBS_PREC_FP64, &st);
+        total += st.ms;
+    }
+    if (rc == RBS_OK && cal_time) *cal_time += total / reps;
+    rbs_plan_free(plan);
+}
+
+void recblocking_solver(int *cscColPtr, int *cscRowIdx, double *cscVal, int m, int n, int nnz, double *b, double *x,
+                        double *x_ref, int rhs, int lv, int substitution, double *cal_time) {
+    (void)x_ref;
+    if (m != n) {
+        set_error("recblocking_solver: matrix must be square");
+        return;
+    }
+    rbs_options o;
+    rbs_options_default(&o);
+    o.max_rhs = rhs > 0 ? rhs : 1;
+    rbs_plan *plan = nullptr;
+    if (rbs_analyse(cscColPtr, cscRowIdx, cscVal, m, nnz, RBS_FMT_CSC, substitution, lv, &o, &plan)) return;
+    rbs_stats st;
+    int k = rhs > 0 ? rhs : 1;
+    if (rbs_solve_host(plan, b, x, k, m, RBS_PREC_FP64, &st) == RBS_OK && cal_time) *cal_time += st.ms;
+    rbs_plan_free(plan);
+}
+
+}  // extern "C"

@@ -1,0 +1,460 @@
+// kernels.cuh -- sm_100a kernels of the recursive-block triangular solve.
+//
+// All triangles are solved in processing order (lower triangular, see
+// rbs_internal.h).  Work vectors are row-interleaved: entry (row p, rhs c)
+// of a K-wide vector lives at v[p*K + c], so the K values one row produces
+// or consumes are contiguous.
+//
+// Readiness of x: the solution work vector is filled with a NaN sentinel
+// before a solve; a value is ready when it no longer carries the sentinel
+// bit pattern.  Arithmetic never produces that pattern (the hardware's NaN
+// is canonical and results equal to it are replaced), so one relaxed load
+// both polls and fetches the value: no separate flag array, no fence.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rbs {
+
+#define RBS_SENT64 0xFFF8DEADBEEFCAFEull
+#define RBS_SENT32 0xFFC0DEADu
+#define RBS_STATUS_TIMEOUT 1
+#define RBS_LONGROW 2048
+
+template <typename VT> struct Sent;
+template <> struct Sent<double> {
+    __device__ __forceinline__ static double value() { return __longlong_as_double((long long)RBS_SENT64); }
+    __device__ __forceinline__ static bool is(double v) {
+        return (unsigned long long)__double_as_longlong(v) == RBS_SENT64;
+    }
+    __device__ __forceinline__ static double nan() { return __longlong_as_double(0x7FF8000000000000ll); }
+};
+template <> struct Sent<float> {
+    __device__ __forceinline__ static float value() { return __uint_as_float(RBS_SENT32); }
+    __device__ __forceinline__ static bool is(float v) { return __float_as_uint(v) == RBS_SENT32; }
+    __device__ __forceinline__ static float nan() { return __uint_as_float(0x7FC00000u); }
+};
+
+__device__ __forceinline__ double ld_relaxed(const double *p) {
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ float ld_relaxed(const float *p) {
+    float v;
+    asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(double *p, double v) {
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(float *p, float v) {
+    asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+
+// Wait until x[i] is produced.  Bounded: after `limit` polls the wait gives
+// up, raises RBS_STATUS_TIMEOUT and returns NaN so dependants still finish.
+template <typename VT>
+__device__ __forceinline__ VT wait_value(const VT *p, int *status, long long limit) {
+    VT v = ld_relaxed(p);
+    if (!Sent<VT>::is(v)) return v;
+    unsigned ns = 32;
+    for (long long it = 0; it < limit; ++it) {
+        if (it > 16) {
+            __nanosleep(ns);
+            if (ns < 1024) ns <<= 1;
+        }
+        v = ld_relaxed(p);
+        if (!Sent<VT>::is(v)) return v;
+    }
+    atomicOr(status, RBS_STATUS_TIMEOUT);
+    return Sent<VT>::nan();
+}
+
+template <typename VT>
+__device__ __forceinline__ VT finalize(VT v) {
+    return Sent<VT>::is(v) ? Sent<VT>::nan() : v;
+}
+
+// ---------------------------------------------------------------------------
+// Vector permutations (utils_cuda.h:858-876 levelset_reordering_vecb/vecx,
+// fused with the RHS interleave, the precision cast and the sentinel reset).
+// ---------------------------------------------------------------------------
+template <typename VT, int K>
+__global__ void k_gather(const double *__restrict__ b, int ld, int k, const int *__restrict__ perm, int n,
+                         VT *__restrict__ out) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long total = (long long)n * K;
+    for (; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int p = (int)(t / K), c = (int)(t % K);
+        double v = c < k ? b[(long long)c * ld + perm[p]] : 0.0;
+        out[t] = (VT)v;
+    }
+}
+
+// x[perm[p] + c*ld] = xw[p*K + c]; xw reset to the sentinel for the next solve.
+template <typename VT, int K>
+__global__ void k_scatter_reset(VT *__restrict__ xw, const int *__restrict__ perm, int n, int k, double *x,
+                                int ld) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long total = (long long)n * K;
+    for (; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int p = (int)(t / K), c = (int)(t % K);
+        VT v = xw[t];
+        if (c < k) x[(long long)c * ld + perm[p]] = (double)v;
+        xw[t] = Sent<VT>::value();
+    }
+}
+
+template <typename VT>
+__global__ void k_fill(VT *__restrict__ v, long long count, VT value) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; t < count; t += (long long)gridDim.x * blockDim.x) v[t] = value;
+}
+
+// ---------------------------------------------------------------------------
+// Diagonal-only triangle (reference method 0, utils_sptrsv_cuda.h:202-216).
+// ---------------------------------------------------------------------------
+template <typename VT, int K>
+__global__ void k_tri_diag(const VT *__restrict__ inv, const VT *__restrict__ b, VT *x, int m) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long total = (long long)m * K;
+    for (; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int p = (int)(t / K);
+        st_relaxed(x + t, finalize(b[t] * inv[p]));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Sync-free triangle (replaces reference method 3, utils_sptrsv_cuda.h:53-114).
+// Pull-style over CSR: a group of lanes owns a row, gathers its dependencies
+// as they become ready and publishes x_p once.  Rows are handed out by a
+// ticket counter in processing (topological) order, so every row a waiting
+// group depends on is owned by a group that is already running: no
+// deadlock for any grid size.  No atomics on values: results are
+// deterministic.
+//   K == 1: G lanes share the entries of a row (G in {1,..,32}).
+//   K  > 1: R = min(K,32) lanes per row, each owns K/R right-hand sides.
+// ---------------------------------------------------------------------------
+template <typename VT, int K>
+__global__ void __launch_bounds__(256) k_tri_syncfree(const int *__restrict__ rp, const int *__restrict__ col,
+                                                      const VT *__restrict__ val, const VT *__restrict__ inv,
+                                                      const VT *__restrict__ b, VT *x, int m, int G,
+                                                      int *ticket, int *status, long long limit) {
+    const int lane = threadIdx.x & 31;
+    constexpr int R = K < 32 ? K : 32;
+    constexpr int RPL = K / R;
+    const int g = K == 1 ? G : R;
+    const int rows_per_warp = 32 / g;
+    const int sub = lane / g, sl = lane % g;
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(ticket, rows_per_warp);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= m) return;
+        const int row = base + sub;
+        const bool active = row < m;
+        if (K == 1) {
+            // Reduce inside the row group only: a later group of this warp may
+            // be spinning on the row this group is about to publish.
+            const unsigned gmask = g == 32 ? 0xffffffffu : (((1u << g) - 1u) << (sub * g));
+            VT sum = 0;
+            if (active) {
+                const int s = rp[row], e = rp[row + 1];
+                for (int k = s + sl; k < e; k += g) sum += val[k] * wait_value(x + col[k], status, limit);
+            }
+            for (int off = g >> 1; off > 0; off >>= 1) sum += __shfl_down_sync(gmask, sum, off, g);
+            if (active && sl == 0) st_relaxed(x + row, finalize((b[row] - sum) * inv[row]));
+            __syncwarp();
+        } else {
+            if (active) {
+                VT acc[RPL];
+#pragma unroll
+                for (int r = 0; r < RPL; ++r) acc[r] = 0;
+                const int s = rp[row], e = rp[row + 1];
+                for (int k = s; k < e; ++k) {
+                    const VT v = val[k];
+                    const VT *xs = x + (long long)col[k] * K + sl * RPL;
+#pragma unroll
+                    for (int r = 0; r < RPL; ++r) acc[r] += v * wait_value(xs + r, status, limit);
+                }
+                const VT d = inv[row];
+                const long long o = (long long)row * K + sl * RPL;
+#pragma unroll
+                for (int r = 0; r < RPL; ++r) st_relaxed(x + o + r, finalize((b[o + r] - acc[r]) * d));
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Single-CTA level-synchronous triangle (replaces reference method 2,
+// utils_sptrsv_cuda.h:116-200 + the per-level launches of
+// recblocking_calculate.h:68-94): one launch walks all local levels with a
+// CTA barrier between levels instead of a kernel boundary.  Level l is the
+// row range [lvl[l], lvl[l+1]) (or rows map[lvl[l]..lvl[l+1]) when the local
+// levels are not contiguous).  gridDim.x > 1 solves independent systems
+// described by `desc` (batched mode).
+// ---------------------------------------------------------------------------
+struct LevelDesc {
+    const int *rp, *col, *lvl, *map;
+    const void *val, *inv, *b;
+    void *x;
+    int m, nlv, G, pad;
+};
+
+template <typename VT, int K>
+__global__ void __launch_bounds__(1024) k_tri_level(const LevelDesc *__restrict__ descs) {
+    const LevelDesc d = descs[blockIdx.x];
+    const int *__restrict__ rp = d.rp;
+    const int *__restrict__ col = d.col;
+    const VT *__restrict__ val = (const VT *)d.val;
+    const VT *__restrict__ inv = (const VT *)d.inv;
+    const VT *__restrict__ b = (const VT *)d.b;
+    VT *x = (VT *)d.x;
+    constexpr int R = K < 32 ? K : 32;
+    constexpr int RPL = K / R;
+    const int g = K == 1 ? d.G : R;
+    const int lane = threadIdx.x & 31;
+    const int sl = lane % g;
+    const int slot = threadIdx.x / g, nslots = blockDim.x / g;
+    for (int l = 0; l < d.nlv; ++l) {
+        const int lo = d.lvl[l], hi = d.lvl[l + 1];
+        // all lanes of a group stay together; groups never straddle warps
+        for (int base = lo; base < hi; base += nslots) {
+            const int idx = base + slot;
+            const bool active = idx < hi;
+            const int row = active ? (d.map ? d.map[idx] : idx) : 0;
+            if (K == 1) {
+                VT sum = 0;
+                if (active) {
+                    const int s = rp[row], e = rp[row + 1];
+                    for (int k = s + sl; k < e; k += g) sum += val[k] * x[col[k]];
+                }
+                for (int off = g >> 1; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off, g);
+                if (active && sl == 0) x[row] = finalize((b[row] - sum) * inv[row]);
+            } else if (active) {
+                VT acc[RPL];
+#pragma unroll
+                for (int r = 0; r < RPL; ++r) acc[r] = 0;
+                const int s = rp[row], e = rp[row + 1];
+                for (int k = s; k < e; ++k) {
+                    const VT v = val[k];
+                    const VT *xs = x + (long long)col[k] * K + sl * RPL;
+#pragma unroll
+                    for (int r = 0; r < RPL; ++r) acc[r] += v * xs[r];
+                }
+                const VT dv = inv[row];
+                const long long o = (long long)row * K + sl * RPL;
+#pragma unroll
+                for (int r = 0; r < RPL; ++r) x[o + r] = finalize((b[o + r] - acc[r]) * dv);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Sequential triangle for deep, narrow blocks without a small bandwidth: one
+// warp walks the rows in order, lanes split a row's entries; x of recent
+// rows is kept in a shared-memory ring.
+// ---------------------------------------------------------------------------
+template <typename VT, int K>
+__global__ void __launch_bounds__(32) k_tri_seq(const int *__restrict__ rp, const int *__restrict__ col,
+                                                const VT *__restrict__ val, const VT *__restrict__ inv,
+                                                const VT *__restrict__ b, VT *x, int m) {
+    constexpr int RING = 4096 / K;
+    __shared__ VT ring[RING * K];
+    const int lane = threadIdx.x;
+    for (int row = 0; row < m; ++row) {
+        const int s = rp[row], e = rp[row + 1];
+        for (int c = 0; c < K; ++c) {
+            VT sum = 0;
+            for (int k = s + lane; k < e; k += 32) {
+                const int q = col[k];
+                const VT xv = q >= row - RING ? ring[(q % RING) * K + c] : x[(long long)q * K + c];
+                sum += val[k] * xv;
+            }
+            for (int off = 16; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off);
+            if (lane == 0) {
+                const VT v = finalize((b[(long long)row * K + c] - sum) * inv[row]);
+                ring[(row % RING) * K + c] = v;
+                x[(long long)row * K + c] = v;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Square block: b[rows] -= S * x[cols]  (reference mv methods 0..3,
+// utils_spmv_cuda.h:60-203, with subKernel :205-212 fused).  `rows` lists
+// the rows for the DCSR form, NULL for plain CSR.  Rows longer than 2048 are
+// skipped here and handled by k_spmv_long (utils_spmv_cuda.h:30-58).
+// ---------------------------------------------------------------------------
+template <typename VT, int K>
+__global__ void __launch_bounds__(256) k_spmv_sub(const int *__restrict__ rp, const int *__restrict__ col,
+                                                  const VT *__restrict__ val, const int *__restrict__ rows,
+                                                  int nrows, int G, const VT *__restrict__ x, VT *b,
+                                                  int skip_long) {
+    constexpr int R = K < 32 ? K : 32;
+    constexpr int RPL = K / R;
+    const int g = K == 1 ? G : R;
+    const int lane = threadIdx.x & 31;
+    const int sl = lane % g, rpw = 32 / g;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = warp * rpw; base < nrows; base += nwarps * rpw) {
+        const long long i = base + lane / g;
+        const bool active = i < nrows;
+        int s = 0, e = 0, row = 0;
+        if (active) {
+            s = rp[i];
+            e = rp[i + 1];
+            row = rows ? rows[i] : (int)i;
+            if (skip_long && e - s > RBS_LONGROW) e = s;
+        }
+        if (K == 1) {
+            VT sum = 0;
+            for (int k = s + sl; k < e; k += g) sum += val[k] * x[col[k]];
+            for (int off = g >> 1; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off, g);
+            if (active && sl == 0 && e > s) b[row] -= sum;
+        } else if (active && e > s) {
+            VT acc[RPL];
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) acc[r] = 0;
+            for (int k = s; k < e; ++k) {
+                const VT v = val[k];
+                const VT *xs = x + (long long)col[k] * K + sl * RPL;
+#pragma unroll
+                for (int r = 0; r < RPL; ++r) acc[r] += v * xs[r];
+            }
+            const long long o = (long long)row * K + sl * RPL;
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) b[o + r] -= acc[r];
+        }
+    }
+}
+
+// Long rows: each warp takes a 32*8-entry slice of one long row and
+// accumulates into b with atomics (the only atomics of the solve; their
+// order varies, so long-row results can differ in the last bits between
+// runs).
+template <typename VT, int K>
+__global__ void __launch_bounds__(256) k_spmv_long(const int *__restrict__ rp, const int *__restrict__ col,
+                                                   const VT *__restrict__ val, const int *__restrict__ rows,
+                                                   const int *__restrict__ longpos, int nlong,
+                                                   const VT *__restrict__ x, VT *b) {
+    constexpr int SLICE = 256;
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (int li = 0; li < nlong; ++li) {
+        const int pos = longpos[li];  // index into rp (the row itself for plain CSR)
+        const int row = rows ? rows[pos] : pos;
+        const int s = rp[pos], e = rp[pos + 1];
+        const long long nslices = (e - s + SLICE - 1) / SLICE;
+        for (long long w = warp; w < nslices; w += nwarps) {
+            const int ss = s + (int)w * SLICE, se = min(e, ss + SLICE);
+            for (int c = 0; c < K; ++c) {
+                VT sum = 0;
+                for (int k = ss + lane; k < se; k += 32) sum += val[k] * x[(long long)col[k] * K + c];
+                for (int off = 16; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off);
+                if (lane == 0) atomicAdd(b + (long long)row * K + c, -sum);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Mixed precision: r32 = (float)(b - A x) with FP64 A, x, b (full
+// processing-order CSR including the diagonal).
+// ---------------------------------------------------------------------------
+template <int K>
+__global__ void __launch_bounds__(256) k_residual(const int *__restrict__ rp, const int *__restrict__ col,
+                                                  const double *__restrict__ val, const double *__restrict__ x,
+                                                  const double *__restrict__ b, float *__restrict__ r32, int n,
+                                                  int G) {
+    constexpr int R = K < 32 ? K : 32;
+    constexpr int RPL = K / R;
+    const int g = K == 1 ? G : R;
+    const int lane = threadIdx.x & 31;
+    const int sl = lane % g, rpw = 32 / g;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = warp * rpw; base < n; base += nwarps * rpw) {
+        const long long row = base + lane / g;
+        const bool active = row < n;
+        if (K == 1) {
+            double sum = 0;
+            if (active)
+                for (int k = rp[row] + sl; k < rp[row + 1]; k += g) sum += val[k] * x[col[k]];
+            for (int off = g >> 1; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off, g);
+            if (active && sl == 0) r32[row] = (float)(b[row] - sum);
+        } else if (active) {
+            double acc[RPL];
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) acc[r] = 0;
+            for (int k = rp[row]; k < rp[row + 1]; ++k) {
+                const double v = val[k];
+                const double *xs = x + (long long)col[k] * K + sl * RPL;
+#pragma unroll
+                for (int r = 0; r < RPL; ++r) acc[r] += v * xs[r];
+            }
+            const long long o = row * K + sl * RPL;
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) r32[o + r] = (float)(b[o + r] - acc[r]);
+        }
+    }
+}
+
+// x64 (+)= d32; d32 reset to the sentinel; per-column sums of squares of the
+// correction and of the updated solution accumulated into norms[2*K].
+template <int K>
+__global__ void __launch_bounds__(256) k_update(double *__restrict__ x64, float *__restrict__ d32, int n, int first,
+                                                double *__restrict__ norms) {
+    // blockDim (256) and the grid stride are multiples of K, so a thread
+    // always works on the same right-hand side c.
+    __shared__ double sd[2 * K];
+    for (int i = threadIdx.x; i < 2 * K; i += blockDim.x) sd[i] = 0;
+    __syncthreads();
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)n * K;
+    const int c = (int)(t % K);
+    double dd = 0, xx = 0;
+    for (; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const double d = (double)d32[t];
+        const double xn = first ? d : x64[t] + d;
+        x64[t] = xn;
+        d32[t] = __uint_as_float(RBS_SENT32);
+        dd += d * d;
+        xx += xn * xn;
+    }
+    atomicAdd(&sd[c], dd);
+    atomicAdd(&sd[K + c], xx);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * K; i += blockDim.x) atomicAdd(&norms[i], sd[i]);
+}
+
+// x[perm[p] + c*ld] = x64[p*K + c]
+template <int K>
+__global__ void k_scatter64(const double *__restrict__ x64, const int *__restrict__ perm, int n, int k, double *x,
+                            int ld) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long total = (long long)n * K;
+    for (; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int p = (int)(t / K), c = (int)(t % K);
+        if (c < k) x[(long long)c * ld + perm[p]] = x64[t];
+    }
+}
+
+// Probe for the bounded wait: polls a value nothing writes.  Used by the
+// failure-detection test to show a device wait ends with a status instead
+// of hanging.
+__global__ void k_wait_probe(const double *never, int *status, long long limit, double *out) {
+    out[0] = wait_value(never, status, limit);
+}
+
+}  // namespace rbs

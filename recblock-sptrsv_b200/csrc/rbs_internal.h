@@ -1,0 +1,104 @@
+// rbs_internal.h -- plan layout shared by the host analysis and the executor.
+//
+// Orders used in this library
+//   original row i      : the caller's numbering
+//   reference label     : the reference's level-set relabelling
+//                         (utils_reordering.h:130-159): forward label =
+//                         position in the BFS level order, backward label =
+//                         m-1-position
+//   processing position : the order in which rows are solved.  Forward:
+//                         p = label.  Backward: p = m-1-label (= BFS
+//                         position).  In processing order every system is
+//                         LOWER triangular, so every kernel is written once
+//                         for forward substitution.
+//
+// In processing order the recursive-block geometry of both directions is the
+// forward geometry of recblocking_preprocess.h:57-178: triangle i covers
+// rows [i*s, (i+1)*s) (the last one runs to m), and the square after t
+// triangles covers rows [t*s, (t+lowbit(t))*s) x cols [(t-lowbit(t))*s, t*s)
+// (rows run to m when t+lowbit(t) == 2^lv).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "rbs.h"
+
+namespace rbs {
+
+// Per-block execution record (processing order).  Offsets index the pools
+// of the plan.
+struct ExecBlock {
+    int index;          // block index in the reference's order (T0, S1, T2, ...)
+    int tri;            // 1 triangle, 0 square
+    int r0, m;          // rows [r0, r0+m)
+    int c0, ncols;      // squares: columns [c0, c0+ncols); triangles: c0 = r0
+    int nnz;            // reference blk_nnz (triangles include the diagonal)
+    int ref_method;     // reference method code (recblocking_preprocess.h:472-709, 835-922)
+    int kernel;         // RBS_K_*
+    int group;          // lanes per row for k == 1
+    // triangles
+    int nlv;            // local level count
+    int contiguous;     // 1 if local levels are contiguous row ranges in processing order
+    int bandwidth;      // max over rows of (p - smallest column) inside the triangle
+    int maxwidth;       // widest local level
+    long long lvl_off;  // level pointer pool offset (nlv+1 entries)
+    long long map_off;  // row list offset (m entries) when !contiguous, else -1
+    // all blocks
+    long long rp_off;   // row pointer pool offset (m+1 entries, or nrows+1 for DCSR)
+    int nrows;          // rows listed in the row pointer (m, or nonempty rows for DCSR)
+    long long rows_off; // DCSR row list offset or -1
+    int nonempty;       // squares: nonempty rows
+    int longrows;       // squares: rows longer than 2048 (handled by the split kernel)
+    long long long_off; // long-row list offset or -1
+    int lenmax;
+};
+
+struct DeviceState;  // executor side (solve.cu)
+
+struct Plan {
+    int n = 0, nnz = 0, lv = 0, sub = 0, nlevel = 0, sum_block = 0, step = 0;
+    rbs_options opt{};
+    double analyse_ms = 0;
+
+    // inputs kept for the reference-format export (CSC, caller's entry order)
+    std::vector<int> in_cp, in_ri;
+    std::vector<double> in_va;
+    std::vector<int> bfs_item;   // BFS level order (findlevel.h:7-83)
+    std::vector<int> bfs_ptr;    // level pointers (nlevel+1)
+    std::vector<int> label;      // original row -> reference label
+
+    // processing order
+    std::vector<int> perm;       // processing position -> original row
+    std::vector<ExecBlock> blocks;
+    // pools (uploaded to the device)
+    std::vector<int> rp_pool, col_pool, lvl_pool, map_pool, rows_pool;
+    std::vector<double> val_pool;
+    std::vector<double> inv_diag;
+    // full processing-order CSR (with diagonal) for FP64 residuals
+    std::vector<int> full_rp, full_col;
+    std::vector<double> full_val;
+
+    DeviceState *dev = nullptr;
+};
+
+// analysis.cpp
+int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int n, int nnz, int fmt,
+                 int substitution, int lv, const rbs_options &opt, std::string &err);
+int export_reference(const Plan &P, const std::string &name, std::vector<int> &iv, std::vector<double> &dv,
+                     bool &is_double, std::string &err);
+int auto_lv(int m, int device_id);
+
+// solve.cu
+int device_build(Plan &P, std::string &err);
+void device_free(Plan &P);
+int device_solve(Plan &P, const double *d_b, double *d_x, int k, int ld, int prec, bool sync,
+                 rbs_stats *stats, std::string &err);
+int device_sync(Plan &P, std::string &err);
+int device_set_stream(Plan &P, void *stream, std::string &err);
+long long device_bytes(const Plan &P);
+
+void set_error(const std::string &msg);
+
+}  // namespace rbs

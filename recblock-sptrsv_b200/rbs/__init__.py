@@ -1,0 +1,299 @@
+"""Python mirror of the recblock-sptrsv solver interface over librbs.so.
+
+The product is the C ABI in include/rbs.h; this module binds it with ctypes
+for tests, the benchmark and notebooks.  Function names follow the
+reference's entry points:
+
+  recblocking_solver_cuda(...)   recblocking_solver_cuda.h:21-32 (device pointers)
+  recblocking_solver(...)        recblocking_solver.h:16-28 (host arrays)
+  analyse(...) -> Plan           preprocess (levelset_reordering_colrow_csc +
+                                 mat_preprocessing + per-block loop)
+  Plan.solve(...)                L_calculate / U_calculate
+
+Device buffers are passed as torch CUDA tensors (only their data_ptr is
+used); host buffers as numpy arrays.  The library must be built
+(`make -C recblock-sptrsv_b200`); importing this module without it raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(os.path.dirname(_HERE), "librbs.so")
+
+FORWARD, BACKWARD = 0, 1
+FMT_CSC, FMT_CSR = 0, 1
+PREC_FP64, PREC_MIXED, PREC_FP32 = 0, 1, 2
+SELECT_REFERENCE, SELECT_AUTO, SELECT_TUNE = 0, 1, 2
+(K_DIAG, K_SYNCFREE, K_LEVEL, K_SEQ, K_BANDSCAN, K_SPMV, K_EMPTY) = range(7)
+KERNEL_NAMES = ["diag", "syncfree", "level", "seq", "bandscan", "spmv", "empty"]
+
+OK = 0
+ERR_ARG, ERR_STRUCTURE, ERR_CUDA, ERR_NOMEM, ERR_TIMEOUT, ERR_NOCONV, ERR_BUDGET, ERR_UNSUPPORTED = range(1, 9)
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("select", ctypes.c_int),
+        ("device", ctypes.c_int),
+        ("lv_device_id", ctypes.c_int),
+        ("host_only", ctypes.c_int),
+        ("max_rhs", ctypes.c_int),
+        ("mixed", ctypes.c_int),
+        ("ir_tol", ctypes.c_double),
+        ("ir_max_iter", ctypes.c_int),
+        ("spin_limit", ctypes.c_longlong),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("ms", ctypes.c_double),
+        ("iterations", ctypes.c_int),
+        ("correction", ctypes.c_double),
+        ("useful_bytes", ctypes.c_double),
+        ("moved_bytes", ctypes.c_double),
+    ]
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int),
+        ("nnz", ctypes.c_int),
+        ("lv", ctypes.c_int),
+        ("substitution", ctypes.c_int),
+        ("nlevel", ctypes.c_int),
+        ("sum_block", ctypes.c_int),
+        ("kernels", ctypes.c_int * 8),
+        ("device_bytes", ctypes.c_longlong),
+        ("analyse_ms", ctypes.c_double),
+    ]
+
+
+class GenSpec(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int),
+        ("n", ctypes.c_int),
+        ("grid", ctypes.c_int),
+        ("lam", ctypes.c_double),
+        ("band", ctypes.c_int),
+        ("zipf_alpha", ctypes.c_double),
+        ("zipf_max", ctypes.c_int),
+        ("chain_bw", ctypes.c_int),
+        ("seed", ctypes.c_ulonglong),
+    ]
+
+
+# every symbol include/rbs.h and include/rbs_gen.h declare
+EXPORTS = [
+    "rbs_options_default", "rbs_analyse", "rbs_analyse_device", "rbs_solve", "rbs_solve_host",
+    "rbs_solve_async", "rbs_plan_sync", "rbs_plan_set_stream", "rbs_plan_info_get", "rbs_plan_export",
+    "rbs_plan_free", "rbs_last_error", "rbs_auto_lv", "recblocking_solver_cuda", "recblocking_solver",
+    "rbs_gen_lower_csr", "rbs_gen_uniform", "rbs_gen_free",
+]
+
+
+class RbsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"rbs error {code}: {msg}")
+        self.code = code
+
+
+def _load():
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(f"{_LIB_PATH} not built; run make -C {os.path.dirname(_HERE)}")
+    lib = ctypes.CDLL(_LIB_PATH)
+    P = ctypes.c_void_p
+    ip = ctypes.POINTER(ctypes.c_int)
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.rbs_options_default.argtypes = [ctypes.POINTER(Options)]
+    lib.rbs_analyse.argtypes = [ip, ip, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                ctypes.POINTER(Options), ctypes.POINTER(P)]
+    lib.rbs_analyse_device.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.POINTER(Options), ctypes.POINTER(P)]
+    lib.rbs_solve.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Stats)]
+    lib.rbs_solve_host.argtypes = [P, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Stats)]
+    lib.rbs_solve_async.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.rbs_plan_sync.argtypes = [P]
+    lib.rbs_plan_set_stream.argtypes = [P, P]
+    lib.rbs_plan_info_get.argtypes = [P, ctypes.POINTER(PlanInfo)]
+    lib.rbs_plan_export.argtypes = [P, ctypes.c_char_p, P, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
+    lib.rbs_plan_free.argtypes = [P]
+    lib.rbs_last_error.restype = ctypes.c_char_p
+    lib.rbs_auto_lv.argtypes = [ctypes.c_int, ctypes.c_int]
+    lib.recblocking_solver_cuda.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_int,
+                                            ctypes.c_int, dp, dp]
+    lib.recblocking_solver_cuda.restype = None
+    lib.recblocking_solver.argtypes = [ip, ip, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
+    lib.recblocking_solver.restype = None
+    lib.rbs_gen_lower_csr.argtypes = [ctypes.POINTER(GenSpec), ip, ctypes.POINTER(ctypes.c_longlong),
+                                      ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(dp)]
+    lib.rbs_gen_uniform.argtypes = [ctypes.c_ulonglong, ctypes.c_longlong, ctypes.c_double, ctypes.c_double, dp]
+    lib.rbs_gen_free.argtypes = [P]
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    return lib.rbs_last_error().decode()
+
+
+def _check(rc: int):
+    if rc != OK:
+        raise RbsError(rc, last_error())
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def options(**kw) -> Options:
+    o = Options()
+    lib.rbs_options_default(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def auto_lv(m: int, device_id: int = 0) -> int:
+    return lib.rbs_auto_lv(m, device_id)
+
+
+class Plan:
+    """A device-resident analysis (permutation, block bounds, kernel plan)."""
+
+    def __init__(self, handle: ctypes.c_void_p, n: int):
+        self._h = handle
+        self.n = n
+
+    def __del__(self):
+        self.free()
+
+    def free(self):
+        if getattr(self, "_h", None):
+            lib.rbs_plan_free(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> PlanInfo:
+        inf = PlanInfo()
+        _check(lib.rbs_plan_info_get(self._h, ctypes.byref(inf)))
+        return inf
+
+    def export(self, name: str) -> np.ndarray:
+        cnt = ctypes.c_longlong()
+        _check(lib.rbs_plan_export(self._h, name.encode(), None, 0, ctypes.byref(cnt)))
+        dt = np.float64 if name == "recblock_Val" else np.int32
+        out = np.empty(max(cnt.value, 1), dtype=dt)
+        _check(lib.rbs_plan_export(self._h, name.encode(), out.ctypes.data_as(ctypes.c_void_p), cnt.value,
+                                   ctypes.byref(cnt)))
+        return out[: cnt.value]
+
+    def solve(self, b, x, k: int = 1, ld: int | None = None, prec: int = PREC_FP64) -> Stats:
+        """Device solve: b, x are torch CUDA tensors (column-major n x k)."""
+        st = Stats()
+        ld = self.n if ld is None else ld
+        _check(lib.rbs_solve(self._h, ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(x.data_ptr()), k, ld, prec,
+                             ctypes.byref(st)))
+        return st
+
+    def solve_async(self, b, x, k: int = 1, ld: int | None = None, prec: int = PREC_FP64):
+        ld = self.n if ld is None else ld
+        _check(lib.rbs_solve_async(self._h, ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(x.data_ptr()), k, ld,
+                                   prec))
+
+    def sync(self):
+        _check(lib.rbs_plan_sync(self._h))
+
+    def solve_host(self, b: np.ndarray, k: int = 1, prec: int = PREC_FP64):
+        """Host solve: b is a numpy array (n,) or (k, n) (one row per RHS)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b)
+        st = Stats()
+        _check(lib.rbs_solve_host(self._h, _dp(b), _dp(x), k, self.n, prec, ctypes.byref(st)))
+        return x, st
+
+    def set_stream(self, stream_ptr: int | None):
+        _check(lib.rbs_plan_set_stream(self._h, ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+
+
+def analyse(ptr: np.ndarray, idx: np.ndarray, val: np.ndarray, substitution: int = FORWARD, lv: int = -1,
+            fmt: int = FMT_CSC, opts: Options | None = None) -> Plan:
+    ptr = np.ascontiguousarray(ptr, dtype=np.int32)
+    idx = np.ascontiguousarray(idx, dtype=np.int32)
+    val = np.ascontiguousarray(val, dtype=np.float64)
+    n = len(ptr) - 1
+    h = ctypes.c_void_p()
+    _check(lib.rbs_analyse(_ip(ptr), _ip(idx), _dp(val), n, len(idx), fmt, substitution, lv,
+                           ctypes.byref(opts) if opts is not None else None, ctypes.byref(h)))
+    return Plan(h, n)
+
+
+def analyse_device(ptr, idx, val, n: int, nnz: int, substitution: int = FORWARD, lv: int = -1,
+                   fmt: int = FMT_CSC, opts: Options | None = None) -> Plan:
+    h = ctypes.c_void_p()
+    _check(lib.rbs_analyse_device(ctypes.c_void_p(ptr.data_ptr()), ctypes.c_void_p(idx.data_ptr()),
+                                  ctypes.c_void_p(val.data_ptr()), n, nnz, fmt, substitution, lv,
+                                  ctypes.byref(opts) if opts is not None else None, ctypes.byref(h)))
+    return Plan(h, n)
+
+
+def recblocking_solver_cuda(d_colptr, d_rowidx, d_val, m: int, n: int, nnz: int, d_x, d_b, substitution: int,
+                            lv: int):
+    """recblocking_solver_cuda.h:21-32 with torch CUDA tensors; returns (cal_time, preprocess_time) in ms."""
+    cal = ctypes.c_double(0.0)
+    pre = ctypes.c_double(0.0)
+    lib.recblocking_solver_cuda(ctypes.c_void_p(d_colptr.data_ptr()), ctypes.c_void_p(d_rowidx.data_ptr()),
+                                ctypes.c_void_p(d_val.data_ptr()), m, n, nnz, ctypes.c_void_p(d_x.data_ptr()),
+                                ctypes.c_void_p(d_b.data_ptr()), substitution, lv, ctypes.byref(cal),
+                                ctypes.byref(pre))
+    err = last_error()
+    if err:
+        raise RbsError(-1, err)
+    return cal.value, pre.value
+
+
+# ---- synthetic inputs (include/rbs_gen.h) -------------------------------
+GEN_BAND_POISSON, GEN_LAPLACE2D, GEN_ZIPF, GEN_CHAIN, GEN_DIAG = range(5)
+
+
+def gen_lower_csr(kind: int, n: int = 0, grid: int = 0, lam: float = 0.0, band: int = 0, zipf_alpha: float = 0.0,
+                  zipf_max: int = 0, chain_bw: int = 0, seed: int = 0):
+    """Seeded lower-triangular CSR (columns ascending, diagonal last)."""
+    spec = GenSpec(kind, n, grid, lam, band, zipf_alpha, zipf_max, chain_bw, seed)
+    nn = ctypes.c_int()
+    nnz = ctypes.c_longlong()
+    rp = ctypes.POINTER(ctypes.c_int)()
+    ci = ctypes.POINTER(ctypes.c_int)()
+    va = ctypes.POINTER(ctypes.c_double)()
+    _check(lib.rbs_gen_lower_csr(ctypes.byref(spec), ctypes.byref(nn), ctypes.byref(nnz), ctypes.byref(rp),
+                                 ctypes.byref(ci), ctypes.byref(va)))
+    try:
+        n_, z = nn.value, nnz.value
+        rowptr = np.ctypeslib.as_array(rp, shape=(n_ + 1,)).copy()
+        colidx = np.ctypeslib.as_array(ci, shape=(max(z, 1),))[:z].copy()
+        val = np.ctypeslib.as_array(va, shape=(max(z, 1),))[:z].copy()
+    finally:
+        lib.rbs_gen_free(ctypes.cast(rp, ctypes.c_void_p))
+        lib.rbs_gen_free(ctypes.cast(ci, ctypes.c_void_p))
+        lib.rbs_gen_free(ctypes.cast(va, ctypes.c_void_p))
+    return rowptr, colidx, val
+
+
+def gen_uniform(seed: int, n: int, lo: float = -1.0, hi: float = 1.0) -> np.ndarray:
+    out = np.empty(n, dtype=np.float64)
+    _check(lib.rbs_gen_uniform(seed, n, lo, hi, _dp(out)))
+    return out
