@@ -149,6 +149,17 @@ int rbs_plan_export(const rbs_plan *plan, const char *name, void *dst, long long
 
 int rbs_plan_free(rbs_plan *plan);
 
+/* Per-block device timing (no counterpart in the reference, which times the
+ * whole walk with gettimeofday, recblocking_calculate.h:45,164-165).  When
+ * enabled, every FP64/FP32 solve records CUDA events around each block's
+ * kernels; rbs_plan_block_times returns, per block in the reference's block
+ * order, the accumulated milliseconds and the number of timed solves, and
+ * the algorithmic bytes one FP64 single-RHS pass of the block moves
+ * (entries x 12 + row pointers + b, x and diagonal traffic).
+ * Enabling/disabling resets the accumulators. */
+int rbs_plan_profile(rbs_plan *plan, int enable);
+int rbs_plan_block_times(const rbs_plan *plan, double *ms, double *bytes, long long *solves, int cap);
+
 /* Message of the last error on the calling thread ("" if none). */
 const char *rbs_last_error(void);
 

@@ -135,6 +135,18 @@ void select_kernel(ExecBlock &b, const rbs_options &opt, const std::vector<int> 
 
 }  // namespace
 
+// Algorithmic bytes of one FP64 single-RHS pass over a block: every stored
+// entry once (8-byte value + 4-byte index), the row pointer, and per row the
+// right-hand side read plus the result written; triangles also read the
+// inverse diagonal; squares read the x segment they multiply once.
+double block_bytes(const Plan &P, const ExecBlock &B) {
+    (void)P;
+    if (B.tri) return (double)(B.nnz - B.m) * 12.0 + 4.0 * (B.m + 1) + 24.0 * B.m;
+    if (B.nnz == 0) return 0.0;
+    return (double)B.nnz * 12.0 + 4.0 * (B.nrows + 1) + 16.0 * B.nonempty + 8.0 * B.ncols +
+           (B.rows_off >= 0 ? 4.0 * B.nrows : 0.0);
+}
+
 int auto_lv(int m, int device_id) {
     // main.cu:245-254: smallest li >= 1 with m / 2^(li+1) below the wave size
     int li;
@@ -554,6 +566,22 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
         return RBS_OK;
     }
     if (name == "levelPtr") return put(P.bfs_ptr);
+    if (name == "group") {
+        iv.resize(sum);
+        for (int b = 0; b < sum; ++b) iv[b] = P.blocks[b].group;
+        return RBS_OK;
+    }
+    if (name == "local_nlv") {
+        iv.resize(sum);
+        for (int b = 0; b < sum; ++b) iv[b] = P.blocks[b].tri ? P.blocks[b].nlv : 0;
+        return RBS_OK;
+    }
+    if (name == "block_bytes") {
+        is_double = true;
+        dv.resize(sum);
+        for (int b = 0; b < sum; ++b) dv[b] = block_bytes(P, P.blocks[b]);
+        return RBS_OK;
+    }
     if (name == "sizes") {
         int ps = 1, is = 0, ds = 0;  // recblocking_preprocess.h:370-384
         for (int b = 0; b < sum; ++b) {

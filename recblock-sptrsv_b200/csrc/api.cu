@@ -136,32 +136,33 @@ int rbs_solve_host(rbs_plan *plan, const double *b, double *x, int k, int ld, in
     int rc = check_solve_args(plan, b, x, k, ld, prec);
     if (rc) return rc;
     if (!plan->p.dev) return fail(RBS_ERR_ARG, "rbs_solve_host: plan has no device state");
+    // plan-owned staging buffers (kept between calls); the copies run on the
+    // plan's stream, so pinned host arrays overlap nothing else but avoid a
+    // bounce through pageable staging in the driver
     size_t bytes = sizeof(double) * (size_t)ld * (size_t)k;
     double *db = nullptr, *dx = nullptr;
-    cudaError_t e = cudaMalloc(&db, bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&dx, bytes);
-    if (e != cudaSuccess) {
-        cudaFree(db);
-        return fail(RBS_ERR_NOMEM, std::string("rbs_solve_host: ") + cudaGetErrorString(e));
-    }
-    e = cudaMemcpy(db, b, bytes, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(dx, x, bytes, cudaMemcpyHostToDevice);  // keeps rows beyond n when ld > n
-    if (e != cudaSuccess) {
-        cudaFree(db);
-        cudaFree(dx);
-        return fail(RBS_ERR_CUDA, std::string("rbs_solve_host: ") + cudaGetErrorString(e));
-    }
     std::string err;
-    rc = rbs::device_solve(plan->p, db, dx, k, ld, prec, true, stats, err);
+    rc = rbs::device_staging(plan->p, bytes, db, dx, err);
+    if (rc) return fail(rc, err);
+    void *st = rbs::device_stream(plan->p);
+    size_t nbytes = sizeof(double) * (size_t)plan->p.n;
+    cudaError_t e = cudaSuccess;
+    for (int c = 0; c < k && e == cudaSuccess; ++c)
+        e = cudaMemcpyAsync(db + (size_t)c * ld, b + (size_t)c * ld, nbytes, cudaMemcpyHostToDevice,
+                            (cudaStream_t)st);
+    if (e != cudaSuccess) return fail(RBS_ERR_CUDA, std::string("rbs_solve_host: ") + cudaGetErrorString(e));
+    rc = rbs::device_solve(plan->p, db, dx, k, ld, prec, false, nullptr, err);
     if (rc == RBS_OK || rc == RBS_ERR_NOCONV) {
-        e = cudaMemcpy(x, dx, bytes, cudaMemcpyDeviceToHost);
+        for (int c = 0; c < k && e == cudaSuccess; ++c)
+            e = cudaMemcpyAsync(x + (size_t)c * ld, dx + (size_t)c * ld, nbytes, cudaMemcpyDeviceToHost,
+                                (cudaStream_t)st);
         if (e != cudaSuccess && rc == RBS_OK) {
             rc = RBS_ERR_CUDA;
             err = std::string("rbs_solve_host: ") + cudaGetErrorString(e);
         }
     }
-    cudaFree(db);
-    cudaFree(dx);
+    int rc2 = rbs::device_finish(plan->p, stats, k, prec, err);
+    if (rc == RBS_OK) rc = rc2;
     if (rc) return fail(rc, err);
     return RBS_OK;
 }
@@ -211,6 +212,27 @@ int rbs_plan_export(const rbs_plan *plan, const char *name, void *dst, long long
         std::memcpy(dst, dv.data(), dv.size() * sizeof(double));
     else
         std::memcpy(dst, iv.data(), iv.size() * sizeof(int));
+    return RBS_OK;
+}
+
+int rbs_plan_profile(rbs_plan *plan, int enable) {
+    if (!plan) return fail(RBS_ERR_ARG, "rbs_plan_profile: plan is NULL");
+    std::string err;
+    int rc = rbs::device_profile(plan->p, enable, err);
+    if (rc) return fail(rc, err);
+    return RBS_OK;
+}
+
+int rbs_plan_block_times(const rbs_plan *plan, double *ms, double *bytes, long long *solves, int cap) {
+    if (!plan || cap < plan->p.sum_block) return fail(RBS_ERR_ARG, "rbs_plan_block_times: bad arguments");
+    std::vector<double> v;
+    long long s = 0;
+    if (rbs::device_block_times(plan->p, v, s)) return fail(RBS_ERR_ARG, "rbs_plan_block_times: no device state");
+    for (int b = 0; b < plan->p.sum_block; ++b) {
+        if (ms) ms[b] = v[b];
+        if (bytes) bytes[b] = rbs::block_bytes(plan->p, plan->p.blocks[b]);
+    }
+    if (solves) *solves = s;
     return RBS_OK;
 }
 

@@ -96,7 +96,13 @@ void device_free(Plan &P);
 int device_solve(Plan &P, const double *d_b, double *d_x, int k, int ld, int prec, bool sync,
                  rbs_stats *stats, std::string &err);
 int device_sync(Plan &P, std::string &err);
+int device_finish(Plan &P, rbs_stats *stats, int k, int prec, std::string &err);
+void *device_stream(Plan &P);
 int device_set_stream(Plan &P, void *stream, std::string &err);
+int device_profile(Plan &P, int enable, std::string &err);
+int device_block_times(const Plan &P, std::vector<double> &ms, long long &solves);
+int device_staging(Plan &P, size_t bytes, double *&db, double *&dx, std::string &err);
+double block_bytes(const Plan &P, const ExecBlock &B);
 long long device_bytes(const Plan &P);
 
 void set_error(const std::string &msg);

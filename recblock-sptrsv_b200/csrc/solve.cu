@@ -35,6 +35,16 @@ struct DeviceState {
     std::map<long long, LevelDesc *> desc_cache;
     long long bytes = 0, work_bytes = 0;
     bool mixed = false;
+    // per-block timing (rbs_plan_profile)
+    bool profile = false;
+    std::vector<cudaEvent_t> bev;
+    std::vector<double> bms;
+    long long bsolves = 0;
+    // staging for the host-array API
+    double *stage_b = nullptr, *stage_x = nullptr;
+    size_t stage_bytes = 0;
+    int last_iters = 0;
+    double last_corr = 0;
 };
 
 namespace {
@@ -212,6 +222,7 @@ int run_blocks(Plan &P, std::string &err) {
     const long long limit = P.opt.spin_limit;
     int ti = 0, li = 0;
     for (const ExecBlock &B : P.blocks) {
+        if (D.profile) CK(cudaEventRecord(D.bev[2 * B.index], st));
         if (B.tri) {
             const VT *bb = bw + (long long)B.r0 * K;
             VT *xx = xw + (long long)B.r0 * K;
@@ -250,6 +261,7 @@ int run_blocks(Plan &P, std::string &err) {
                                                                   D.rows + B.long_off, B.longrows,
                                                                   xw + (long long)B.c0 * K, bw + (long long)B.r0 * K);
         }
+        if (D.profile) CK(cudaEventRecord(D.bev[2 * B.index + 1], st));
     }
     CK(cudaGetLastError());
     return RBS_OK;
@@ -379,11 +391,57 @@ int device_build(Plan &P, std::string &err) {
     return RBS_OK;
 }
 
+int device_profile(Plan &P, int enable, std::string &err) {
+    if (!P.dev) {
+        err = "plan has no device state";
+        return RBS_ERR_ARG;
+    }
+    DeviceState &D = *P.dev;
+    CK(cudaStreamSynchronize(D.stream));
+    if (enable && D.bev.empty()) {
+        D.bev.resize(2 * P.blocks.size());
+        for (auto &e : D.bev) CK(cudaEventCreate(&e));
+    }
+    D.profile = enable != 0;
+    D.bms.assign(P.blocks.size(), 0.0);
+    D.bsolves = 0;
+    return RBS_OK;
+}
+
+int device_block_times(const Plan &P, std::vector<double> &ms, long long &solves) {
+    if (!P.dev) return RBS_ERR_ARG;
+    ms = P.dev->bms;
+    ms.resize(P.blocks.size(), 0.0);
+    solves = P.dev->bsolves;
+    return RBS_OK;
+}
+
+int device_staging(Plan &P, size_t bytes, double *&db, double *&dx, std::string &err) {
+    DeviceState &D = *P.dev;
+    if (bytes > D.stage_bytes) {
+        cudaFree(D.stage_b);
+        cudaFree(D.stage_x);
+        D.stage_b = D.stage_x = nullptr;
+        D.bytes -= 2 * (long long)D.stage_bytes;
+        D.stage_bytes = 0;
+        int rc;
+        if ((rc = alloc(D, D.stage_b, bytes / sizeof(double), err))) return rc;
+        if ((rc = alloc(D, D.stage_x, bytes / sizeof(double), err))) return rc;
+        D.stage_bytes = bytes;
+    }
+    db = D.stage_b;
+    dx = D.stage_x;
+    return RBS_OK;
+}
+
 void device_free(Plan &P) {
     if (!P.dev) return;
     DeviceState &D = *P.dev;
     if (D.stream) cudaStreamSynchronize(D.stream);
     free_work(D);
+    for (auto &e : D.bev) cudaEventDestroy(e);
+    cudaFree(D.stage_b);
+    cudaFree(D.stage_x);
     void *ptrs[] = {D.rp, D.col, D.lvl, D.map, D.rows, D.perm, D.val, D.inv, D.val32, D.inv32,
                     D.full_rp, D.full_col, D.full_val, D.tickets, D.status, D.norms};
     for (void *p : ptrs) cudaFree(p);
@@ -433,6 +491,8 @@ int device_sync(Plan &P, std::string &err) {
     return RBS_OK;
 }
 
+void *device_stream(Plan &P) { return P.dev ? (void *)P.dev->stream : nullptr; }
+
 int device_solve(Plan &P, const double *d_b, double *d_x, int k, int ld, int prec, bool sync, rbs_stats *stats,
                  std::string &err) {
     if (!P.dev) {
@@ -470,15 +530,30 @@ int device_solve(Plan &P, const double *d_b, double *d_x, int k, int ld, int pre
         corr = std::max(corr, cr);
     }
     CK(cudaEventRecord(D.ev1, D.stream));
+    D.last_iters = iters;
+    D.last_corr = corr;
     if (!sync) return rc;
-    int rc2 = device_sync(P, err);
-    if (rc == RBS_OK) rc = rc2;
+    int rc2 = device_finish(P, stats, k, prec, err);
+    return rc != RBS_OK ? rc : rc2;
+}
+
+int device_finish(Plan &P, rbs_stats *stats, int k, int prec, std::string &err) {
+    DeviceState &D = *P.dev;
+    int rc = device_sync(P, err);
+    if (rc == RBS_OK && D.profile && prec != RBS_PREC_MIXED && k <= 128) {
+        for (size_t b = 0; b < P.blocks.size(); ++b) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, D.bev[2 * b], D.bev[2 * b + 1]) == cudaSuccess) D.bms[b] += ms;
+        }
+        ++D.bsolves;
+    }
     if (stats) {
         float ms = 0;
         cudaEventElapsedTime(&ms, D.ev0, D.ev1);
+        const int iters = D.last_iters;
         stats->ms = ms;
         stats->iterations = iters;
-        stats->correction = corr;
+        stats->correction = D.last_corr;
         double n = P.n, nnz = P.nnz;
         stats->useful_bytes = nnz * 12.0 + 4.0 * (n + 1) + 16.0 * n * k;
         if (prec == RBS_PREC_FP64)

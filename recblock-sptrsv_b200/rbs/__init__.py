@@ -92,7 +92,7 @@ EXPORTS = [
     "rbs_options_default", "rbs_analyse", "rbs_analyse_device", "rbs_solve", "rbs_solve_host",
     "rbs_solve_async", "rbs_plan_sync", "rbs_plan_set_stream", "rbs_plan_info_get", "rbs_plan_export",
     "rbs_plan_free", "rbs_last_error", "rbs_auto_lv", "recblocking_solver_cuda", "recblocking_solver",
-    "rbs_gen_lower_csr", "rbs_gen_uniform", "rbs_gen_free",
+    "rbs_gen_lower_csr", "rbs_gen_uniform", "rbs_gen_free", "rbs_plan_profile", "rbs_plan_block_times",
 ]
 
 
@@ -134,6 +134,8 @@ def _load():
                                       ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(dp)]
     lib.rbs_gen_uniform.argtypes = [ctypes.c_ulonglong, ctypes.c_longlong, ctypes.c_double, ctypes.c_double, dp]
     lib.rbs_gen_free.argtypes = [P]
+    lib.rbs_plan_profile.argtypes = [P, ctypes.c_int]
+    lib.rbs_plan_block_times.argtypes = [P, dp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
     return lib
 
 
@@ -196,7 +198,7 @@ class Plan:
     def export(self, name: str) -> np.ndarray:
         cnt = ctypes.c_longlong()
         _check(lib.rbs_plan_export(self._h, name.encode(), None, 0, ctypes.byref(cnt)))
-        dt = np.float64 if name == "recblock_Val" else np.int32
+        dt = np.float64 if name in ("recblock_Val", "block_bytes") else np.int32
         out = np.empty(max(cnt.value, 1), dtype=dt)
         _check(lib.rbs_plan_export(self._h, name.encode(), out.ctypes.data_as(ctypes.c_void_p), cnt.value,
                                    ctypes.byref(cnt)))
@@ -218,13 +220,29 @@ class Plan:
     def sync(self):
         _check(lib.rbs_plan_sync(self._h))
 
-    def solve_host(self, b: np.ndarray, k: int = 1, prec: int = PREC_FP64):
-        """Host solve: b is a numpy array (n,) or (k, n) (one row per RHS)."""
+    def solve_host(self, b: np.ndarray, k: int = 1, prec: int = PREC_FP64, x: np.ndarray | None = None):
+        """Host solve: b is a numpy array (n,) or (k, n) (one row per RHS); x
+        (same shape, e.g. a pinned buffer) receives the solution."""
         b = np.ascontiguousarray(b, dtype=np.float64)
-        x = np.zeros_like(b)
+        if x is None:
+            x = np.zeros_like(b)
+        assert x.flags.c_contiguous and x.dtype == np.float64 and x.shape == b.shape
         st = Stats()
         _check(lib.rbs_solve_host(self._h, _dp(b), _dp(x), k, self.n, prec, ctypes.byref(st)))
         return x, st
+
+    def profile(self, enable: bool = True):
+        """Per-block CUDA-event timing of FP64/FP32 solves (resets the totals)."""
+        _check(lib.rbs_plan_profile(self._h, int(enable)))
+
+    def block_times(self):
+        """(ms per block accumulated, algorithmic bytes per block per pass, timed solves)."""
+        nb = self.info().sum_block
+        ms = np.zeros(nb)
+        by = np.zeros(nb)
+        solves = ctypes.c_longlong()
+        _check(lib.rbs_plan_block_times(self._h, _dp(ms), _dp(by), ctypes.byref(solves), nb))
+        return ms, by, solves.value
 
     def set_stream(self, stream_ptr: int | None):
         _check(lib.rbs_plan_set_stream(self._h, ctypes.c_void_p(stream_ptr) if stream_ptr else None))
