@@ -166,6 +166,31 @@ const char *rbs_last_error(void);
 /* main.cu:245-254: lv for the -lv -1 option. */
 int rbs_auto_lv(int m, int device_id);
 
+/* Solve without allocating device memory.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc/cudaFree where they need a solve:
+ * a host framework whose caching allocator already holds the device's free
+ * memory (a raw cudaMalloc fails, and cudaFree would synchronise the whole
+ * device), or a latency-critical loop that forbids allocation after
+ * start-up.  The caller passes a triangular CSR (row pointer, column
+ * indices, values with the diagonal stored in each row, any order inside a
+ * row), b and x, all device pointers; lower for RBS_FORWARD, upper for
+ * RBS_BACKWARD.  No analysis: rows are solved in index order by the
+ * sync-free kernel.  stream may be NULL (legacy default stream).  The call
+ * returns when the solve is complete.
+ *
+ * Scratch: a static device array of RBS_NOALLOC_MAX_ROWS doubles plus 256
+ * bytes (about 8 MB), held by every GPU that loads this library until the
+ * process exits.  n > RBS_NOALLOC_MAX_ROWS is rejected with RBS_ERR_ARG.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call on a device shares the one array: calls whose work overlaps on
+ * the GPU (different streams or host threads) race and corrupt each other's
+ * results; serialise them. */
+#define RBS_NOALLOC_MAX_ROWS (1 << 20)
+int rbs_sptrsv_csr_noalloc(const int *d_rowptr, const int *d_colidx, const double *d_val, int n,
+                           int substitution, const double *d_b, double *d_x, void *stream);
+
 /* ---- reference-signature shims ---------------------------------------- */
 
 /* recblocking_solver_cuda.h:21-32.  Same arguments and meaning: device CSC

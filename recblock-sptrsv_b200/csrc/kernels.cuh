@@ -450,11 +450,4 @@ __global__ void k_scatter64(const double *__restrict__ x64, const int *__restric
     }
 }
 
-// Probe for the bounded wait: polls a value nothing writes.  Used by the
-// failure-detection test to show a device wait ends with a status instead
-// of hanging.
-__global__ void k_wait_probe(const double *never, int *status, long long limit, double *out) {
-    out[0] = wait_value(never, status, limit);
-}
-
 }  // namespace rbs

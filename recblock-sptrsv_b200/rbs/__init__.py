@@ -93,6 +93,7 @@ EXPORTS = [
     "rbs_solve_async", "rbs_plan_sync", "rbs_plan_set_stream", "rbs_plan_info_get", "rbs_plan_export",
     "rbs_plan_free", "rbs_last_error", "rbs_auto_lv", "recblocking_solver_cuda", "recblocking_solver",
     "rbs_gen_lower_csr", "rbs_gen_uniform", "rbs_gen_free", "rbs_plan_profile", "rbs_plan_block_times",
+    "rbs_sptrsv_csr_noalloc",
 ]
 
 
@@ -136,6 +137,7 @@ def _load():
     lib.rbs_gen_free.argtypes = [P]
     lib.rbs_plan_profile.argtypes = [P, ctypes.c_int]
     lib.rbs_plan_block_times.argtypes = [P, dp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
+    lib.rbs_sptrsv_csr_noalloc.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, P, P, P]
     return lib
 
 
@@ -282,6 +284,18 @@ def recblocking_solver_cuda(d_colptr, d_rowidx, d_val, m: int, n: int, nnz: int,
     if err:
         raise RbsError(-1, err)
     return cal.value, pre.value
+
+
+NOALLOC_MAX_ROWS = 1 << 20  # RBS_NOALLOC_MAX_ROWS
+
+
+def sptrsv_csr_noalloc(d_rowptr, d_colidx, d_val, n: int, substitution: int, d_b, d_x, stream_ptr: int | None = None):
+    """rbs_sptrsv_csr_noalloc: solve from a device CSR (diagonal inside the
+    rows) with no device allocation; scratch is the library's static array."""
+    _check(lib.rbs_sptrsv_csr_noalloc(ctypes.c_void_p(d_rowptr.data_ptr()), ctypes.c_void_p(d_colidx.data_ptr()),
+                                      ctypes.c_void_p(d_val.data_ptr()), n, substitution,
+                                      ctypes.c_void_p(d_b.data_ptr()), ctypes.c_void_p(d_x.data_ptr()),
+                                      ctypes.c_void_p(stream_ptr) if stream_ptr else None))
 
 
 # ---- synthetic inputs (include/rbs_gen.h) -------------------------------
