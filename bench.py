@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-sweep", action="store_true", help="skip the structure/variant side measurements")
+    ap.add_argument("--no-extras", action="store_true", help="skip e2e, side measurements and the CPU baseline "
+                                                               "(short runs for profilers)")
     return ap.parse_args()
 
 
@@ -284,6 +286,14 @@ def run_ours(args):
                 "bytes_per_launch": dom_bytes_per_launch, "launch_ms": dom_launch_ms,
                 "solve_frac": useful / (ms_per_step / 1000) / 1e9 / peak}
     plan.profile(False)
+
+    if args.no_extras:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "solves/s", "ms_per_step": ms_per_step,
+                              "roofline": roofline, "note": "--no-extras run (profiling)"}))
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     # end to end through the host-array API (pinned buffers, H2D + solve + D2H per step)
     hb = torch.empty(sysm["n"], dtype=torch.float64, pin_memory=True)

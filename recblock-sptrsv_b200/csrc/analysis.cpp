@@ -299,6 +299,14 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
         B.index = b;
         B.tri = (b & 1) == 0;
         B.rows_off = B.long_off = B.map_off = B.lvl_off = -1;
+        B.band_w = B.band_c = B.band_nch = 0;
+        B.band_off = -1;
+        B.tma_ok = B.nchunks = 0;
+        B.chunk_off = -1;
+        B.ell_ok = B.ell_nchunks = 0;
+        B.ell_chunk_off = B.ell_lo = B.ell_hi = -1;
+        B.ca_ok = B.ca_w = 0;
+        B.ca_tab_off = B.ca_lo = B.ca_hi = -1;
         if (B.tri) {
             int i = b / 2;
             B.r0 = i * s;
@@ -498,6 +506,161 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
             }
         }
     }
+    // 7. band layout of band-scan triangles: row r of the block is row
+    //    i = r % C of chunk j = r / C; its coefficient of x_{r-1-d} sits at
+    //    band_coef[band_off + (i*nch + j)*W + d], its inverse diagonal at
+    //    band_inv[band_off/W + i*nch + j].
+    P.band_coef.clear();
+    P.band_inv.clear();
+    for (ExecBlock &B : P.blocks) {
+        if (!B.tri || B.kernel != RBS_K_BANDSCAN) continue;
+        int W = 1;
+        while (W < std::max(1, B.bandwidth)) W <<= 1;
+        B.band_w = W;
+        B.band_c = 16;
+        B.band_nch = (B.m + B.band_c - 1) / B.band_c;
+        B.band_off = (long long)P.band_coef.size();
+        const long long slots = (long long)B.band_nch * B.band_c;
+        P.band_coef.resize(P.band_coef.size() + (size_t)(slots * W), 0.0);
+        P.band_inv.resize(P.band_inv.size() + (size_t)slots, 0.0);
+        const long long inv_off = B.band_off / W;
+        for (int r = 0; r < B.m; ++r) {
+            const long long o = (long long)(r % B.band_c) * B.band_nch + r / B.band_c;
+            P.band_inv[(size_t)(inv_off + o)] = P.inv_diag[(size_t)B.r0 + r];
+            const int s0 = P.rp_pool[(size_t)B.rp_off + r], s1 = P.rp_pool[(size_t)B.rp_off + r + 1];
+            for (int k = s0; k < s1; ++k) {
+                const int d = r - P.col_pool[k] - 1;
+                P.band_coef[(size_t)(B.band_off + o * W + d)] += P.val_pool[k];
+            }
+        }
+    }
+    // 8. row chunks of level triangles (contiguous levels) for the staged
+    //    kernel: greedy runs of <= 512 rows and <= 2048 entries
+    P.chunk_pool.clear();
+    for (ExecBlock &B : P.blocks) {
+        if (!B.tri || B.kernel != RBS_K_LEVEL || !B.contiguous) continue;
+        std::vector<int> cuts{0};
+        bool ok = true;
+        int rows = 0;
+        long long ents = 0;
+        for (int r = 0; r < B.m; ++r) {
+            const int len = P.rp_pool[(size_t)B.rp_off + r + 1] - P.rp_pool[(size_t)B.rp_off + r];
+            if (len > 2048) { ok = false; break; }
+            if (rows == 512 || ents + len > 2048) {
+                cuts.push_back(r);
+                rows = 0;
+                ents = 0;
+            }
+            ++rows;
+            ents += len;
+        }
+        if (!ok) continue;
+        cuts.push_back(B.m);
+        B.tma_ok = 1;
+        B.nchunks = (int)cuts.size() - 1;
+        B.chunk_off = (long long)P.chunk_pool.size();
+        P.chunk_pool.insert(P.chunk_pool.end(), cuts.begin(), cuts.end());
+        for (int c : cuts) P.chunk_pool.push_back(P.rp_pool[(size_t)B.rp_off + c]);  // entry offsets
+    }
+    // 9. ELL chunks of single-CTA triangles (the CTA sync-free kernel,
+    //    cta_syncfree.cuh): chunks of <= 512 rows and <= 2048 ELL slots,
+    //    column-major inside a chunk, padding column -1
+    P.ell_col.clear();
+    P.ell_val.clear();
+    P.ell_chunks.clear();
+    constexpr int RMAX = 512, EMAX = 2048;
+    for (ExecBlock &B : P.blocks) {
+        if (!B.tri || B.kernel != RBS_K_LEVEL) continue;
+        const int *rp = P.rp_pool.data() + B.rp_off;
+        std::vector<int> cuts{0}, widths;
+        bool ok = true;
+        int w = 0, rows = 0;
+        for (int r = 0; r < B.m && ok; ++r) {
+            const int len = rp[r + 1] - rp[r];
+            if (len > EMAX) ok = false;
+            const int w2 = std::max(w, len);
+            if (rows == RMAX || (long long)(rows + 1) * w2 > EMAX) {
+                cuts.push_back(r);
+                widths.push_back(w);
+                w = len;
+                rows = 1;
+            } else {
+                w = w2;
+                ++rows;
+            }
+        }
+        if (!ok) continue;
+        cuts.push_back(B.m);
+        widths.push_back(w);
+        const int nch = (int)widths.size();
+        B.ell_ok = 1;
+        B.ell_nchunks = nch;
+        B.ell_chunk_off = (long long)P.ell_chunks.size() / 4;
+        B.ell_lo = (long long)P.ell_col.size();
+        for (int q = 0; q < nch; ++q) {
+            while (P.ell_col.size() % 4) {  // 16-byte aligned chunk starts
+                P.ell_col.push_back(-1);
+                P.ell_val.push_back(0.0);
+            }
+            const int R0 = cuts[q], R1 = cuts[q + 1], W = widths[q], R = R1 - R0;
+            const long long off = (long long)P.ell_col.size();
+            P.ell_chunks.insert(P.ell_chunks.end(), {R0, R1, W, (int)off});
+            P.ell_col.resize(P.ell_col.size() + (size_t)R * W, -1);
+            P.ell_val.resize(P.ell_val.size() + (size_t)R * W, 0.0);
+            for (int i = 0; i < R; ++i) {
+                const int r = R0 + i;
+                for (int j = 0; j < rp[r + 1] - rp[r]; ++j) {
+                    P.ell_col[(size_t)(off + (long long)j * R + i)] = P.col_pool[rp[r] + j];
+                    P.ell_val[(size_t)(off + (long long)j * R + i)] = P.val_pool[rp[r] + j];
+                }
+            }
+        }
+        B.ell_hi = (long long)P.ell_col.size();
+    }
+    // 10. level-ELL layout of level triangles with narrow levels (<= 1024
+    //     rows) and short rows (<= 4 entries): the cp.async-staged kernel
+    //     (level_ca.cuh).  Per level: lo, ELL width, pool offset; entries
+    //     column-major inside the level.
+    P.ca_tab.clear();
+    P.ca_col.clear();
+    P.ca_val.clear();
+    for (ExecBlock &B : P.blocks) {
+        if (!B.tri || B.kernel != RBS_K_LEVEL || !B.contiguous) continue;
+        const int *rp = P.rp_pool.data() + B.rp_off;
+        const int *lvp = P.lvl_pool.data() + B.lvl_off;
+        int wmax = 0;
+        bool ok = true;
+        for (int l = 0; l < B.nlv && ok; ++l) {
+            if (lvp[l + 1] - lvp[l] > 1024) ok = false;
+            for (int r = lvp[l]; r < lvp[l + 1]; ++r) wmax = std::max(wmax, rp[r + 1] - rp[r]);
+        }
+        if (!ok || wmax > 4) continue;
+        B.ca_ok = 1;
+        B.ca_w = wmax <= 1 ? 1 : wmax <= 2 ? 2 : 4;
+        B.ca_tab_off = (long long)P.ca_tab.size();
+        B.ca_lo = (long long)P.ca_col.size();
+        for (int l = 0; l < B.nlv; ++l) {
+            const int lo = lvp[l], w = lvp[l + 1] - lo;
+            int wl = 0;
+            for (int r = lo; r < lo + w; ++r) wl = std::max(wl, rp[r + 1] - rp[r]);
+            const long long off = (long long)P.ca_col.size() - B.ca_lo;
+            P.ca_tab.insert(P.ca_tab.end(), {lo, wl, (int)off});
+            P.ca_col.resize(P.ca_col.size() + (size_t)wl * w, -1);
+            P.ca_val.resize(P.ca_val.size() + (size_t)wl * w, 0.0);
+            for (int i = 0; i < w; ++i)
+                for (int j = 0; j < rp[lo + i + 1] - rp[lo + i]; ++j) {
+                    const size_t dst = (size_t)(B.ca_lo + off + (long long)j * w + i);
+                    P.ca_col[dst] = P.col_pool[rp[lo + i] + j];
+                    P.ca_val[dst] = P.val_pool[rp[lo + i] + j];
+                }
+        }
+        P.ca_tab.push_back(B.m);
+        B.ca_hi = (long long)P.ca_col.size();
+    }
+    if (P.ell_col.size() > (size_t)0x7fffffff || P.ca_col.size() > (size_t)0x7fffffff) {
+        err = "rbs_analyse: ELL pool too large";
+        return RBS_ERR_NOMEM;
+    }
     auto t1 = std::chrono::steady_clock::now();
     P.analyse_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     return RBS_OK;
@@ -574,6 +737,35 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
     if (name == "local_nlv") {
         iv.resize(sum);
         for (int b = 0; b < sum; ++b) iv[b] = P.blocks[b].tri ? P.blocks[b].nlv : 0;
+        return RBS_OK;
+    }
+    if (name == "ell_col") return put(P.ell_col);
+    if (name == "ell_chunks") return put(P.ell_chunks);
+    if (name == "ell_val") {
+        is_double = true;
+        dv = P.ell_val;
+        return RBS_OK;
+    }
+    if (name == "ell_block") {  // per block: first chunk, chunk count (-1 if not ELL)
+        iv.assign(2 * sum, -1);
+        for (int b = 0; b < sum; ++b)
+            if (P.blocks[b].ell_ok) {
+                iv[2 * b] = (int)P.blocks[b].ell_chunk_off;
+                iv[2 * b + 1] = P.blocks[b].ell_nchunks;
+            }
+        return RBS_OK;
+    }
+    if (name == "block_rows") {  // per block: processing-order first row, rows
+        iv.resize(2 * sum);
+        for (int b = 0; b < sum; ++b) {
+            iv[2 * b] = P.blocks[b].r0;
+            iv[2 * b + 1] = P.blocks[b].m;
+        }
+        return RBS_OK;
+    }
+    if (name == "inv_diag") {
+        is_double = true;
+        dv = P.inv_diag;
         return RBS_OK;
     }
     if (name == "block_bytes") {

@@ -53,6 +53,20 @@ struct ExecBlock {
     int longrows;       // squares: rows longer than 2048 (handled by the split kernel)
     long long long_off; // long-row list offset or -1
     int lenmax;
+    // band-scan triangles: W = power of two >= bandwidth, chunks of C rows
+    int band_w, band_c, band_nch;
+    long long band_off;  // coefficient pool offset (band_nch*band_c*band_w); inverse pool at band_off / band_w
+    // level triangles staged through shared memory: row chunks of <= 512 rows and <= 2048 entries
+    int tma_ok, nchunks;
+    long long chunk_off;  // chunk boundary pool offset (nchunks+1 entries)
+    // level triangles staged per thread with cp.async (level-ELL layout)
+    int ca_ok, ca_w;
+    long long ca_tab_off;     // level table offset in ca_tab (3*nlv+1 ints)
+    long long ca_lo, ca_hi;   // element range of the block in the level-ELL pools
+    // single-CTA triangles in ELL chunks (CTA sync-free kernel)
+    int ell_ok, ell_nchunks;
+    long long ell_chunk_off;  // first chunk in ell_chunks (4 ints per chunk: R0, R1, W, pool offset)
+    long long ell_lo, ell_hi; // element range of the block in the ELL pools
 };
 
 struct DeviceState;  // executor side (solve.cu)
@@ -73,9 +87,15 @@ struct Plan {
     std::vector<int> perm;       // processing position -> original row
     std::vector<ExecBlock> blocks;
     // pools (uploaded to the device)
-    std::vector<int> rp_pool, col_pool, lvl_pool, map_pool, rows_pool;
+    std::vector<int> rp_pool, col_pool, lvl_pool, map_pool, rows_pool, chunk_pool;
     std::vector<double> val_pool;
     std::vector<double> inv_diag;
+    std::vector<double> band_coef, band_inv;  // chunk-interleaved band layout of band-scan triangles
+    std::vector<int> ell_col;                  // ELL columns of single-CTA triangles (-1 = padding)
+    std::vector<double> ell_val;
+    std::vector<int> ell_chunks;
+    std::vector<int> ca_tab, ca_col;           // level tables and level-ELL columns (-1 = padding)
+    std::vector<double> ca_val;
     // full processing-order CSR (with diagonal) for FP64 residuals
     std::vector<int> full_rp, full_col;
     std::vector<double> full_val;

@@ -9,7 +9,11 @@
 #include <map>
 #include <vector>
 
+#include "band.cuh"
 #include "kernels.cuh"
+#include "cta_syncfree.cuh"
+#include "level_ca.cuh"
+#include "level_tma.cuh"
 #include "rbs_internal.h"
 
 namespace rbs {
@@ -25,6 +29,22 @@ struct DeviceState {
     float *val32 = nullptr, *inv32 = nullptr;
     int *full_rp = nullptr, *full_col = nullptr;
     double *full_val = nullptr;
+    double *band_coef = nullptr, *band_inv = nullptr;   // band-scan layout (f64)
+    float *band_coef32 = nullptr, *band_inv32 = nullptr;
+    double *band_maps = nullptr, *band_states = nullptr; // scratch of the band scan (f64 or f32)
+    int *chunks = nullptr;                               // chunk boundaries of staged level triangles
+    int *ell_col = nullptr;
+    double *ell_val = nullptr;
+    float *ell_val32 = nullptr;
+    EllChunk *ell_chunks = nullptr;
+    std::map<long long, CsfDesc *> ell_cache;
+    int *ca_tab = nullptr, *ca_col = nullptr;
+    double *ca_val = nullptr;
+    float *ca_val32 = nullptr;
+    std::map<long long, CaDesc *> ca_cache;
+    cudaStream_t side = nullptr;                         // L2 prefetch stream
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    std::map<long long, TmaDesc *> tma_cache;
     int *tickets = nullptr, *status = nullptr, *h_status = nullptr;
     int ntri = 0;
     // work vectors for kcap right-hand sides
@@ -60,7 +80,8 @@ namespace {
 
 template <typename T>
 int upload(DeviceState &D, T *&dst, const std::vector<T> &src, std::string &err) {
-    size_t bytes = std::max<size_t>(src.size(), 1) * sizeof(T);
+    // 256 bytes of padding: staged bulk copies round their end up to 16 bytes
+    size_t bytes = std::max<size_t>(src.size(), 1) * sizeof(T) + 256;
     cudaError_t e = cudaMalloc(&dst, bytes);
     if (e != cudaSuccess) {
         err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
@@ -73,7 +94,7 @@ int upload(DeviceState &D, T *&dst, const std::vector<T> &src, std::string &err)
 
 template <typename T>
 int alloc(DeviceState &D, T *&dst, size_t count, std::string &err) {
-    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T) + 256;
     cudaError_t e = cudaMalloc(&dst, bytes);
     if (e != cudaSuccess) {
         err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
@@ -113,6 +134,12 @@ void free_work(DeviceState &D) {
     D.bw32 = D.xw32 = nullptr;
     for (auto &kv : D.desc_cache) cudaFree(kv.second);
     D.desc_cache.clear();
+    for (auto &kv : D.tma_cache) cudaFree(kv.second);
+    D.tma_cache.clear();
+    for (auto &kv : D.ell_cache) cudaFree(kv.second);
+    D.ell_cache.clear();
+    for (auto &kv : D.ca_cache) cudaFree(kv.second);
+    D.ca_cache.clear();
 }
 
 // Work vectors sized for K right-hand sides; solution vectors start filled
@@ -149,12 +176,20 @@ template <typename VT> struct Pools;
 template <> struct Pools<double> {
     static const double *val(const DeviceState &D) { return D.val; }
     static const double *inv(const DeviceState &D) { return D.inv; }
+    static const double *bcoef(const DeviceState &D) { return D.band_coef; }
+    static const double *binv(const DeviceState &D) { return D.band_inv; }
+    static const double *ellv(const DeviceState &D) { return D.ell_val; }
+    static const double *cav(const DeviceState &D) { return D.ca_val; }
     static double *bw(const DeviceState &D) { return D.bw64; }
     static double *xw(const DeviceState &D) { return D.xw64; }
 };
 template <> struct Pools<float> {
     static const float *val(const DeviceState &D) { return D.val32; }
     static const float *inv(const DeviceState &D) { return D.inv32; }
+    static const float *bcoef(const DeviceState &D) { return D.band_coef32; }
+    static const float *binv(const DeviceState &D) { return D.band_inv32; }
+    static const float *ellv(const DeviceState &D) { return D.ell_val32; }
+    static const float *cav(const DeviceState &D) { return D.ca_val32; }
     static float *bw(const DeviceState &D) { return D.bw32; }
     static float *xw(const DeviceState &D) { return D.xw32; }
 };
@@ -193,6 +228,152 @@ int level_descs(Plan &P, LevelDesc *&out, std::string &err) {
     return RBS_OK;
 }
 
+template <typename VT>
+int tma_descs(Plan &P, TmaDesc *&out, std::string &err) {
+    DeviceState &D = *P.dev;
+    long long key = sizeof(VT) == 8 ? 0 : 1;
+    auto it = D.tma_cache.find(key);
+    if (it != D.tma_cache.end()) {
+        out = it->second;
+        return RBS_OK;
+    }
+    std::vector<TmaDesc> h;
+    for (const ExecBlock &B : P.blocks) {
+        if (!B.tri || B.kernel != RBS_K_LEVEL || !B.tma_ok) continue;
+        TmaDesc d{};
+        d.rp = D.rp + B.rp_off;
+        d.col = D.col;
+        d.val = Pools<VT>::val(D);
+        d.inv = Pools<VT>::inv(D) + B.r0;
+        d.b = Pools<VT>::bw(D) + B.r0;
+        d.x = Pools<VT>::xw(D) + B.r0;
+        d.lvl = D.lvl + B.lvl_off;
+        d.chunks = D.chunks + B.chunk_off;
+        d.m = B.m;
+        d.nlv = B.nlv;
+        d.nchunks = B.nchunks;
+        d.G = B.group;
+        h.push_back(d);
+    }
+    TmaDesc *dd = nullptr;
+    CK(cudaMalloc(&dd, std::max<size_t>(h.size(), 1) * sizeof(TmaDesc)));
+    if (!h.empty()) CK(cudaMemcpy(dd, h.data(), h.size() * sizeof(TmaDesc), cudaMemcpyHostToDevice));
+    D.tma_cache[key] = dd;
+    out = dd;
+    if (!h.empty()) {
+        static bool attr = false;
+        if (!attr) {
+            CK(cudaFuncSetAttribute(k_tri_level_tma<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)TmaLayout<VT>::total));
+            attr = true;
+        }
+    }
+    return RBS_OK;
+}
+
+template <typename VT>
+int ell_descs(Plan &P, CsfDesc *&out, std::string &err) {
+    DeviceState &D = *P.dev;
+    long long key = sizeof(VT) == 8 ? 0 : 1;
+    auto it = D.ell_cache.find(key);
+    if (it != D.ell_cache.end()) {
+        out = it->second;
+        return RBS_OK;
+    }
+    std::vector<CsfDesc> h;
+    for (const ExecBlock &B : P.blocks) {
+        if (!B.tri || B.kernel != RBS_K_LEVEL || !B.ell_ok) continue;
+        CsfDesc d{};
+        d.col = D.ell_col;
+        d.val = Pools<VT>::ellv(D);
+        d.inv = Pools<VT>::inv(D) + B.r0;
+        d.b = Pools<VT>::bw(D) + B.r0;
+        d.x = Pools<VT>::xw(D) + B.r0;
+        d.chunks = D.ell_chunks + B.ell_chunk_off;
+        d.m = B.m;
+        d.nchunks = B.ell_nchunks;
+        d.G = B.group;
+        h.push_back(d);
+    }
+    CsfDesc *dd = nullptr;
+    CK(cudaMalloc(&dd, std::max<size_t>(h.size(), 1) * sizeof(CsfDesc)));
+    if (!h.empty()) CK(cudaMemcpy(dd, h.data(), h.size() * sizeof(CsfDesc), cudaMemcpyHostToDevice));
+    D.ell_cache[key] = dd;
+    out = dd;
+    if (!h.empty()) {
+        static bool attr = false;
+        if (!attr) {
+            CK(cudaFuncSetAttribute(k_tri_cta_syncfree<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)CsfLayout<VT>::total));
+            attr = true;
+        }
+    }
+    return RBS_OK;
+}
+
+template <typename VT, int W, int S>
+int ca_attr(std::string &err) {
+    static bool done = false;
+    if (!done) {
+        CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)CaLayout<VT, W, S>::total));
+        done = true;
+    }
+    return RBS_OK;
+}
+
+template <typename VT>
+int ca_descs(Plan &P, CaDesc *&out, std::string &err) {
+    DeviceState &D = *P.dev;
+    long long key = sizeof(VT) == 8 ? 0 : 1;
+    auto it = D.ca_cache.find(key);
+    if (it != D.ca_cache.end()) {
+        out = it->second;
+        return RBS_OK;
+    }
+    std::vector<CaDesc> h;
+    for (const ExecBlock &B : P.blocks) {
+        if (!B.tri || B.kernel != RBS_K_LEVEL || !B.ca_ok) continue;
+        CaDesc d{};
+        d.col = D.ca_col + B.ca_lo;
+        d.val = Pools<VT>::cav(D) + B.ca_lo;
+        d.inv = Pools<VT>::inv(D) + B.r0;
+        d.b = Pools<VT>::bw(D) + B.r0;
+        d.x = Pools<VT>::xw(D) + B.r0;
+        d.lvl = D.ca_tab + B.ca_tab_off;
+        d.m = B.m;
+        d.nlv = B.nlv;
+        h.push_back(d);
+    }
+    CaDesc *dd = nullptr;
+    CK(cudaMalloc(&dd, std::max<size_t>(h.size(), 1) * sizeof(CaDesc)));
+    if (!h.empty()) CK(cudaMemcpy(dd, h.data(), h.size() * sizeof(CaDesc), cudaMemcpyHostToDevice));
+    D.ca_cache[key] = dd;
+    out = dd;
+    int rc;
+    if ((rc = ca_attr<VT, 1, 4>(err)) || (rc = ca_attr<VT, 2, 4>(err)) || (rc = ca_attr<VT, 4, 2>(err))) return rc;
+    return RBS_OK;
+}
+
+// Prefetch [p, p+bytes) into L2 with bulk prefetches of 16 KB.
+__global__ void k_prefetch_l2(const char *p, long long bytes) {
+    const long long piece = 16384;
+    for (long long off = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * piece; off < bytes;
+         off += (long long)gridDim.x * blockDim.x * piece) {
+        const unsigned n = (unsigned)(((bytes - off < piece ? bytes - off : piece) + 15) & ~15ll);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p + off), "r"(n) : "memory");
+    }
+}
+
+void prefetch_range(cudaStream_t st, const void *base, long long bytes) {
+    if (bytes <= 0) return;
+    const char *a = (const char *)((unsigned long long)base & ~15ull);
+    bytes += (const char *)base - a;
+    const long long pieces = (bytes + 16383) / 16384;
+    const int grid = (int)std::min<long long>((pieces + 127) / 128, 1184);
+    k_prefetch_l2<<<std::max(grid, 1), 128, 0, st>>>(a, bytes);
+}
+
 template <typename VT, int K>
 int syncfree_grid(const DeviceState &D) {
     static int per_sm = -1;
@@ -204,6 +385,31 @@ int syncfree_grid(const DeviceState &D) {
         per_sm = nb;
     }
     return per_sm * D.num_sms;
+}
+
+// Band-scan triangle: three launches per right-hand side (see band.cuh).
+template <typename VT, int W>
+int run_band(Plan &P, const ExecBlock &B, const VT *bb, VT *xx, int K, std::string &err) {
+    DeviceState &D = *P.dev;
+    cudaStream_t st = D.stream;
+    const VT *coef = Pools<VT>::bcoef(D) + B.band_off;
+    const VT *binv = Pools<VT>::binv(D) + B.band_off / W;
+    VT *maps = reinterpret_cast<VT *>(D.band_maps);
+    VT *states = reinterpret_cast<VT *>(D.band_states);
+    const int tpb = 256;
+    const size_t smem = (size_t)tpb * (W * W + W) * sizeof(VT);
+    static bool attr_set = false;
+    if (!attr_set) {
+        CK(cudaFuncSetAttribute(k_band_scan<VT, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    const int grid = (B.band_nch + 255) / 256;
+    for (int c = 0; c < K; ++c) {
+        k_band_maps<VT, W><<<grid, 256, 0, st>>>(coef, binv, bb, K, c, B.m, B.band_c, B.band_nch, maps);
+        k_band_scan<VT, W><<<1, tpb, smem, st>>>(maps, B.band_nch, states);
+        k_band_replay<VT, W><<<grid, 256, 0, st>>>(coef, binv, bb, K, c, B.m, B.band_c, B.band_nch, states, xx);
+    }
+    return RBS_OK;
 }
 
 // One pass over all blocks: triangles solve into xw, squares update bw.
@@ -218,9 +424,52 @@ int run_blocks(Plan &P, std::string &err) {
     LevelDesc *descs = nullptr;
     int rc = level_descs<VT, K>(P, descs, err);
     if (rc) return rc;
+    TmaDesc *tdescs = nullptr;
+    CsfDesc *edescs = nullptr;
+    CaDesc *cdescs = nullptr;
+    if (K == 1 && (rc = ca_descs<VT>(P, cdescs, err))) return rc;
+    if (K == 1 && (rc = tma_descs<VT>(P, tdescs, err))) return rc;
+    if (K == 1 && (rc = ell_descs<VT>(P, edescs, err))) return rc;
     if (D.ntri) CK(cudaMemsetAsync(D.tickets, 0, sizeof(int) * D.ntri, st));
     const long long limit = P.opt.spin_limit;
-    int ti = 0, li = 0;
+    // The staged level kernel runs on one SM; the others pull the data of
+    // the staged triangles into L2 meanwhile (up to 96 MB, in block order).
+    bool forked = false;
+    if (K == 1 && D.side) {
+        long long budget = 96ll << 20;
+        for (const ExecBlock &B : P.blocks) {
+            if (!B.tri || B.kernel != RBS_K_LEVEL || !(B.tma_ok || B.ell_ok || B.ca_ok) || budget <= 0) continue;
+            if (!forked) {
+                CK(cudaEventRecord(D.ev_fork, st));
+                CK(cudaStreamWaitEvent(D.side, D.ev_fork, 0));
+                forked = true;
+            }
+            if (B.ca_ok) {
+                const long long ne = B.ca_hi - B.ca_lo;
+                prefetch_range(D.side, Pools<VT>::cav(D) + B.ca_lo, ne * (long long)sizeof(VT));
+                prefetch_range(D.side, D.ca_col + B.ca_lo, ne * 4);
+                prefetch_range(D.side, inv + B.r0, (long long)B.m * sizeof(VT));
+                budget -= ne * ((long long)sizeof(VT) + 4) + (long long)B.m * sizeof(VT);
+                continue;
+            }
+            if (B.ell_ok) {
+                const long long ne = B.ell_hi - B.ell_lo;
+                prefetch_range(D.side, Pools<VT>::ellv(D) + B.ell_lo, ne * (long long)sizeof(VT));
+                prefetch_range(D.side, D.ell_col + B.ell_lo, ne * 4);
+                prefetch_range(D.side, inv + B.r0, (long long)B.m * sizeof(VT));
+                budget -= ne * ((long long)sizeof(VT) + 4) + (long long)B.m * sizeof(VT);
+                continue;
+            }
+            const long long e0 = P.rp_pool[(size_t)B.rp_off], e1 = P.rp_pool[(size_t)B.rp_off + B.m];
+            const long long ent = e1 - e0;
+            prefetch_range(D.side, val + e0, ent * (long long)sizeof(VT));
+            prefetch_range(D.side, D.col + e0, ent * 4);
+            prefetch_range(D.side, D.rp + B.rp_off, (B.m + 1) * 4ll);
+            prefetch_range(D.side, inv + B.r0, (long long)B.m * sizeof(VT));
+            budget -= ent * ((long long)sizeof(VT) + 4) + (long long)B.m * (4 + sizeof(VT));
+        }
+    }
+    int ti = 0, li = 0, tti = 0, eti = 0, cti = 0;
     for (const ExecBlock &B : P.blocks) {
         if (D.profile) CK(cudaEventRecord(D.bev[2 * B.index], st));
         if (B.tri) {
@@ -232,13 +481,39 @@ int run_blocks(Plan &P, std::string &err) {
                                                                                                B.m);
                 break;
             case RBS_K_LEVEL:
-                k_tri_level<VT, K><<<1, 1024, 0, st>>>(descs + li);
+                if (K == 1 && B.ca_ok) {
+                    if (B.ca_w == 1)
+                        k_tri_level_ca<VT, 1, 4><<<1, 1024, CaLayout<VT, 1, 4>::total, st>>>(cdescs + cti);
+                    else if (B.ca_w == 2)
+                        k_tri_level_ca<VT, 2, 4><<<1, 1024, CaLayout<VT, 2, 4>::total, st>>>(cdescs + cti);
+                    else
+                        k_tri_level_ca<VT, 4, 2><<<1, 1024, CaLayout<VT, 4, 2>::total, st>>>(cdescs + cti);
+                } else if (K == 1 && B.ell_ok) {
+                    k_tri_cta_syncfree<VT><<<1, 1024, CsfLayout<VT>::total, st>>>(edescs + eti, D.status, limit);
+                } else if (K == 1 && B.tma_ok) {
+                    k_tri_level_tma<VT><<<1, 1024, TmaLayout<VT>::total, st>>>(tdescs + tti, D.status, limit);
+                } else {
+                    k_tri_level<VT, K><<<1, 1024, 0, st>>>(descs + li);
+                }
                 ++li;
+                if (B.ell_ok) ++eti;
+                if (B.tma_ok) ++tti;
+                if (B.ca_ok) ++cti;
                 break;
             case RBS_K_SEQ:
-            case RBS_K_BANDSCAN:
                 k_tri_seq<VT, K><<<1, 32, 0, st>>>(D.rp + B.rp_off, D.col, val, inv + B.r0, bb, xx, B.m);
                 break;
+            case RBS_K_BANDSCAN: {
+                int rc2 = RBS_OK;
+                switch (B.band_w) {
+                case 1: rc2 = run_band<VT, 1>(P, B, bb, xx, K, err); break;
+                case 2: rc2 = run_band<VT, 2>(P, B, bb, xx, K, err); break;
+                case 4: rc2 = run_band<VT, 4>(P, B, bb, xx, K, err); break;
+                default: rc2 = run_band<VT, 8>(P, B, bb, xx, K, err); break;
+                }
+                if (rc2) return rc2;
+                break;
+            }
             default: {
                 const int g = K == 1 ? B.group : (K < 32 ? K : 32);
                 const long long warps = ((long long)B.m * g + 31) / 32;
@@ -262,6 +537,10 @@ int run_blocks(Plan &P, std::string &err) {
                                                                   xw + (long long)B.c0 * K, bw + (long long)B.r0 * K);
         }
         if (D.profile) CK(cudaEventRecord(D.bev[2 * B.index + 1], st));
+    }
+    if (forked) {
+        CK(cudaEventRecord(D.ev_join, D.side));
+        CK(cudaStreamWaitEvent(st, D.ev_join, 0));
     }
     CK(cudaGetLastError());
     return RBS_OK;
@@ -379,6 +658,45 @@ int device_build(Plan &P, std::string &err) {
         if ((rc = upload(D, D.full_col, P.full_col, err))) return rc;
         if ((rc = upload(D, D.full_val, P.full_val, err))) return rc;
     }
+    if ((rc = upload(D, D.band_coef, P.band_coef, err))) return rc;
+    if ((rc = upload(D, D.band_inv, P.band_inv, err))) return rc;
+    {
+        size_t maps = 1, states = 1;
+        for (const ExecBlock &B : P.blocks)
+            if (B.tri && B.kernel == RBS_K_BANDSCAN) {
+                maps = std::max(maps, (size_t)B.band_nch * (B.band_w * B.band_w + B.band_w));
+                states = std::max(states, (size_t)B.band_nch * B.band_w);
+            }
+        if ((rc = alloc(D, D.band_maps, maps, err))) return rc;
+        if ((rc = alloc(D, D.band_states, states, err))) return rc;
+    }
+    if (D.mixed) {
+        std::vector<float> c32(P.band_coef.begin(), P.band_coef.end()), i32(P.band_inv.begin(), P.band_inv.end());
+        if ((rc = upload(D, D.band_coef32, c32, err))) return rc;
+        if ((rc = upload(D, D.band_inv32, i32, err))) return rc;
+    }
+    if ((rc = upload(D, D.chunks, P.chunk_pool, err))) return rc;
+    if ((rc = upload(D, D.ell_col, P.ell_col, err))) return rc;
+    if ((rc = upload(D, D.ell_val, P.ell_val, err))) return rc;
+    {
+        std::vector<EllChunk> ec(P.ell_chunks.size() / 4);
+        std::memcpy(ec.data(), P.ell_chunks.data(), ec.size() * sizeof(EllChunk));
+        if ((rc = upload(D, D.ell_chunks, ec, err))) return rc;
+    }
+    if ((rc = upload(D, D.ca_tab, P.ca_tab, err))) return rc;
+    if ((rc = upload(D, D.ca_col, P.ca_col, err))) return rc;
+    if ((rc = upload(D, D.ca_val, P.ca_val, err))) return rc;
+    if (D.mixed) {
+        std::vector<float> c32(P.ca_val.begin(), P.ca_val.end());
+        if ((rc = upload(D, D.ca_val32, c32, err))) return rc;
+    }
+    if (D.mixed) {
+        std::vector<float> e32(P.ell_val.begin(), P.ell_val.end());
+        if ((rc = upload(D, D.ell_val32, e32, err))) return rc;
+    }
+    CK(cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&D.ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&D.ev_join, cudaEventDisableTiming));
     D.ntri = 1 << P.lv;
     if ((rc = alloc(D, D.tickets, (size_t)D.ntri, err))) return rc;
     if ((rc = alloc(D, D.status, 1, err))) return rc;
@@ -440,10 +758,24 @@ void device_free(Plan &P) {
     if (D.stream) cudaStreamSynchronize(D.stream);
     free_work(D);
     for (auto &e : D.bev) cudaEventDestroy(e);
+    if (D.side) cudaStreamSynchronize(D.side);
+    if (D.side) cudaStreamDestroy(D.side);
+    if (D.ev_fork) cudaEventDestroy(D.ev_fork);
+    if (D.ev_join) cudaEventDestroy(D.ev_join);
+    cudaFree(D.chunks);
+    cudaFree(D.ell_col);
+    cudaFree(D.ell_val);
+    cudaFree(D.ell_val32);
+    cudaFree(D.ell_chunks);
+    cudaFree(D.ca_tab);
+    cudaFree(D.ca_col);
+    cudaFree(D.ca_val);
+    cudaFree(D.ca_val32);
     cudaFree(D.stage_b);
     cudaFree(D.stage_x);
     void *ptrs[] = {D.rp, D.col, D.lvl, D.map, D.rows, D.perm, D.val, D.inv, D.val32, D.inv32,
-                    D.full_rp, D.full_col, D.full_val, D.tickets, D.status, D.norms};
+                    D.full_rp, D.full_col, D.full_val, D.tickets, D.status, D.norms, D.band_coef,
+                    D.band_inv, D.band_coef32, D.band_inv32, D.band_maps, D.band_states};
     for (void *p : ptrs) cudaFree(p);
     if (D.h_status) cudaFreeHost(D.h_status);
     if (D.h_norms) cudaFreeHost(D.h_norms);
