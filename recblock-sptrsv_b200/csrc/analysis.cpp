@@ -301,8 +301,6 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
         B.rows_off = B.long_off = B.map_off = B.lvl_off = -1;
         B.band_w = B.band_c = B.band_nch = 0;
         B.band_off = -1;
-        B.tma_ok = B.nchunks = 0;
-        B.chunk_off = -1;
         B.ell_ok = B.ell_nchunks = 0;
         B.ell_chunk_off = B.ell_lo = B.ell_hi = -1;
         B.ca_ok = B.ca_w = 0;
@@ -533,34 +531,6 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
                 P.band_coef[(size_t)(B.band_off + o * W + d)] += P.val_pool[k];
             }
         }
-    }
-    // 8. row chunks of level triangles (contiguous levels) for the staged
-    //    kernel: greedy runs of <= 512 rows and <= 2048 entries
-    P.chunk_pool.clear();
-    for (ExecBlock &B : P.blocks) {
-        if (!B.tri || B.kernel != RBS_K_LEVEL || !B.contiguous) continue;
-        std::vector<int> cuts{0};
-        bool ok = true;
-        int rows = 0;
-        long long ents = 0;
-        for (int r = 0; r < B.m; ++r) {
-            const int len = P.rp_pool[(size_t)B.rp_off + r + 1] - P.rp_pool[(size_t)B.rp_off + r];
-            if (len > 2048) { ok = false; break; }
-            if (rows == 512 || ents + len > 2048) {
-                cuts.push_back(r);
-                rows = 0;
-                ents = 0;
-            }
-            ++rows;
-            ents += len;
-        }
-        if (!ok) continue;
-        cuts.push_back(B.m);
-        B.tma_ok = 1;
-        B.nchunks = (int)cuts.size() - 1;
-        B.chunk_off = (long long)P.chunk_pool.size();
-        P.chunk_pool.insert(P.chunk_pool.end(), cuts.begin(), cuts.end());
-        for (int c : cuts) P.chunk_pool.push_back(P.rp_pool[(size_t)B.rp_off + c]);  // entry offsets
     }
     // 9. ELL chunks of single-CTA triangles (the CTA sync-free kernel,
     //    cta_syncfree.cuh): chunks of <= 512 rows and <= 2048 ELL slots,

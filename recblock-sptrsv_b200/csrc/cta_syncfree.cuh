@@ -29,7 +29,7 @@
 // waiting, finishes with NaN, and drains its copies before exiting.
 #pragma once
 
-#include "level_tma.cuh"
+#include "tma.cuh"
 
 namespace rbs {
 

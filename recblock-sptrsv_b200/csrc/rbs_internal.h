@@ -56,9 +56,6 @@ struct ExecBlock {
     // band-scan triangles: W = power of two >= bandwidth, chunks of C rows
     int band_w, band_c, band_nch;
     long long band_off;  // coefficient pool offset (band_nch*band_c*band_w); inverse pool at band_off / band_w
-    // level triangles staged through shared memory: row chunks of <= 512 rows and <= 2048 entries
-    int tma_ok, nchunks;
-    long long chunk_off;  // chunk boundary pool offset (nchunks+1 entries)
     // level triangles staged per thread with cp.async (level-ELL layout)
     int ca_ok, ca_w;
     long long ca_tab_off;     // level table offset in ca_tab (3*nlv+1 ints)
@@ -87,7 +84,7 @@ struct Plan {
     std::vector<int> perm;       // processing position -> original row
     std::vector<ExecBlock> blocks;
     // pools (uploaded to the device)
-    std::vector<int> rp_pool, col_pool, lvl_pool, map_pool, rows_pool, chunk_pool;
+    std::vector<int> rp_pool, col_pool, lvl_pool, map_pool, rows_pool;
     std::vector<double> val_pool;
     std::vector<double> inv_diag;
     std::vector<double> band_coef, band_inv;  // chunk-interleaved band layout of band-scan triangles

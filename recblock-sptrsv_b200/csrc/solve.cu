@@ -5,15 +5,16 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
+#include <set>
 #include <vector>
 
 #include "band.cuh"
 #include "kernels.cuh"
 #include "cta_syncfree.cuh"
 #include "level_ca.cuh"
-#include "level_tma.cuh"
 #include "rbs_internal.h"
 
 namespace rbs {
@@ -32,7 +33,6 @@ struct DeviceState {
     double *band_coef = nullptr, *band_inv = nullptr;   // band-scan layout (f64)
     float *band_coef32 = nullptr, *band_inv32 = nullptr;
     double *band_maps = nullptr, *band_states = nullptr; // scratch of the band scan (f64 or f32)
-    int *chunks = nullptr;                               // chunk boundaries of staged level triangles
     int *ell_col = nullptr;
     double *ell_val = nullptr;
     float *ell_val32 = nullptr;
@@ -44,7 +44,6 @@ struct DeviceState {
     std::map<long long, CaDesc *> ca_cache;
     cudaStream_t side = nullptr;                         // L2 prefetch stream
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    std::map<long long, TmaDesc *> tma_cache;
     int *tickets = nullptr, *status = nullptr, *h_status = nullptr;
     int ntri = 0;
     // work vectors for kcap right-hand sides
@@ -65,6 +64,10 @@ struct DeviceState {
     size_t stage_bytes = 0;
     int last_iters = 0;
     double last_corr = 0;
+    // captured block walks per (precision, K, profiling)
+    bool use_graphs = true;
+    std::map<long long, cudaGraphExec_t> graphs;
+    std::set<long long> graph_seen;
 };
 
 namespace {
@@ -134,19 +137,20 @@ void free_work(DeviceState &D) {
     D.bw32 = D.xw32 = nullptr;
     for (auto &kv : D.desc_cache) cudaFree(kv.second);
     D.desc_cache.clear();
-    for (auto &kv : D.tma_cache) cudaFree(kv.second);
-    D.tma_cache.clear();
     for (auto &kv : D.ell_cache) cudaFree(kv.second);
     D.ell_cache.clear();
     for (auto &kv : D.ca_cache) cudaFree(kv.second);
     D.ca_cache.clear();
 }
 
+void drop_graphs_fwd(DeviceState &D);
+
 // Work vectors sized for K right-hand sides; solution vectors start filled
 // with the sentinel and every solve leaves them that way.
 int ensure_work(Plan &P, int K, std::string &err) {
     DeviceState &D = *P.dev;
     if (K <= D.kcap) return RBS_OK;
+    drop_graphs_fwd(D);
     free_work(D);
     D.bytes -= D.work_bytes;
     const long long before = D.bytes;
@@ -225,49 +229,6 @@ int level_descs(Plan &P, LevelDesc *&out, std::string &err) {
     if (!h.empty()) CK(cudaMemcpy(dd, h.data(), h.size() * sizeof(LevelDesc), cudaMemcpyHostToDevice));
     D.desc_cache[key] = dd;
     out = dd;
-    return RBS_OK;
-}
-
-template <typename VT>
-int tma_descs(Plan &P, TmaDesc *&out, std::string &err) {
-    DeviceState &D = *P.dev;
-    long long key = sizeof(VT) == 8 ? 0 : 1;
-    auto it = D.tma_cache.find(key);
-    if (it != D.tma_cache.end()) {
-        out = it->second;
-        return RBS_OK;
-    }
-    std::vector<TmaDesc> h;
-    for (const ExecBlock &B : P.blocks) {
-        if (!B.tri || B.kernel != RBS_K_LEVEL || !B.tma_ok) continue;
-        TmaDesc d{};
-        d.rp = D.rp + B.rp_off;
-        d.col = D.col;
-        d.val = Pools<VT>::val(D);
-        d.inv = Pools<VT>::inv(D) + B.r0;
-        d.b = Pools<VT>::bw(D) + B.r0;
-        d.x = Pools<VT>::xw(D) + B.r0;
-        d.lvl = D.lvl + B.lvl_off;
-        d.chunks = D.chunks + B.chunk_off;
-        d.m = B.m;
-        d.nlv = B.nlv;
-        d.nchunks = B.nchunks;
-        d.G = B.group;
-        h.push_back(d);
-    }
-    TmaDesc *dd = nullptr;
-    CK(cudaMalloc(&dd, std::max<size_t>(h.size(), 1) * sizeof(TmaDesc)));
-    if (!h.empty()) CK(cudaMemcpy(dd, h.data(), h.size() * sizeof(TmaDesc), cudaMemcpyHostToDevice));
-    D.tma_cache[key] = dd;
-    out = dd;
-    if (!h.empty()) {
-        static bool attr = false;
-        if (!attr) {
-            CK(cudaFuncSetAttribute(k_tri_level_tma<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)TmaLayout<VT>::total));
-            attr = true;
-        }
-    }
     return RBS_OK;
 }
 
@@ -414,7 +375,7 @@ int run_band(Plan &P, const ExecBlock &B, const VT *bb, VT *xx, int K, std::stri
 
 // One pass over all blocks: triangles solve into xw, squares update bw.
 template <typename VT, int K>
-int run_blocks(Plan &P, std::string &err) {
+int launch_blocks(Plan &P, std::string &err) {
     DeviceState &D = *P.dev;
     cudaStream_t st = D.stream;
     const VT *val = Pools<VT>::val(D);
@@ -424,11 +385,9 @@ int run_blocks(Plan &P, std::string &err) {
     LevelDesc *descs = nullptr;
     int rc = level_descs<VT, K>(P, descs, err);
     if (rc) return rc;
-    TmaDesc *tdescs = nullptr;
     CsfDesc *edescs = nullptr;
     CaDesc *cdescs = nullptr;
     if (K == 1 && (rc = ca_descs<VT>(P, cdescs, err))) return rc;
-    if (K == 1 && (rc = tma_descs<VT>(P, tdescs, err))) return rc;
     if (K == 1 && (rc = ell_descs<VT>(P, edescs, err))) return rc;
     if (D.ntri) CK(cudaMemsetAsync(D.tickets, 0, sizeof(int) * D.ntri, st));
     const long long limit = P.opt.spin_limit;
@@ -438,7 +397,7 @@ int run_blocks(Plan &P, std::string &err) {
     if (K == 1 && D.side) {
         long long budget = 96ll << 20;
         for (const ExecBlock &B : P.blocks) {
-            if (!B.tri || B.kernel != RBS_K_LEVEL || !(B.tma_ok || B.ell_ok || B.ca_ok) || budget <= 0) continue;
+            if (!B.tri || B.kernel != RBS_K_LEVEL || !(B.ell_ok || B.ca_ok) || budget <= 0) continue;
             if (!forked) {
                 CK(cudaEventRecord(D.ev_fork, st));
                 CK(cudaStreamWaitEvent(D.side, D.ev_fork, 0));
@@ -460,22 +419,19 @@ int run_blocks(Plan &P, std::string &err) {
                 budget -= ne * ((long long)sizeof(VT) + 4) + (long long)B.m * sizeof(VT);
                 continue;
             }
-            const long long e0 = P.rp_pool[(size_t)B.rp_off], e1 = P.rp_pool[(size_t)B.rp_off + B.m];
-            const long long ent = e1 - e0;
-            prefetch_range(D.side, val + e0, ent * (long long)sizeof(VT));
-            prefetch_range(D.side, D.col + e0, ent * 4);
-            prefetch_range(D.side, D.rp + B.rp_off, (B.m + 1) * 4ll);
-            prefetch_range(D.side, inv + B.r0, (long long)B.m * sizeof(VT));
-            budget -= ent * ((long long)sizeof(VT) + 4) + (long long)B.m * (4 + sizeof(VT));
         }
     }
-    int ti = 0, li = 0, tti = 0, eti = 0, cti = 0;
+    int ti = 0, li = 0, eti = 0, cti = 0;
     for (const ExecBlock &B : P.blocks) {
         if (D.profile) CK(cudaEventRecord(D.bev[2 * B.index], st));
         if (B.tri) {
             const VT *bb = bw + (long long)B.r0 * K;
             VT *xx = xw + (long long)B.r0 * K;
-            switch (B.kernel) {
+            // Several right-hand sides: the single-CTA level kernels have no
+            // staged multi-RHS form, and one dependency walk of the multi-CTA
+            // sync-free kernel serves all K columns, so level triangles take it.
+            const int kernel = (K > 1 && B.kernel == RBS_K_LEVEL) ? RBS_K_SYNCFREE : B.kernel;
+            switch (kernel) {
             case RBS_K_DIAG:
                 k_tri_diag<VT, K><<<grid_for((long long)B.m * K, 256, D.num_sms), 256, 0, st>>>(inv + B.r0, bb, xx,
                                                                                                B.m);
@@ -490,15 +446,9 @@ int run_blocks(Plan &P, std::string &err) {
                         k_tri_level_ca<VT, 4, 2><<<1, 1024, CaLayout<VT, 4, 2>::total, st>>>(cdescs + cti);
                 } else if (K == 1 && B.ell_ok) {
                     k_tri_cta_syncfree<VT><<<1, 1024, CsfLayout<VT>::total, st>>>(edescs + eti, D.status, limit);
-                } else if (K == 1 && B.tma_ok) {
-                    k_tri_level_tma<VT><<<1, 1024, TmaLayout<VT>::total, st>>>(tdescs + tti, D.status, limit);
                 } else {
                     k_tri_level<VT, K><<<1, 1024, 0, st>>>(descs + li);
                 }
-                ++li;
-                if (B.ell_ok) ++eti;
-                if (B.tma_ok) ++tti;
-                if (B.ca_ok) ++cti;
                 break;
             case RBS_K_SEQ:
                 k_tri_seq<VT, K><<<1, 32, 0, st>>>(D.rp + B.rp_off, D.col, val, inv + B.r0, bb, xx, B.m);
@@ -524,6 +474,11 @@ int run_blocks(Plan &P, std::string &err) {
                 break;
             }
             }
+            if (B.kernel == RBS_K_LEVEL) {  // descriptor tables list every level triangle
+                ++li;
+                if (B.ell_ok) ++eti;
+                if (B.ca_ok) ++cti;
+            }
             ++ti;
         } else if (B.kernel == RBS_K_SPMV) {
             const int g = K == 1 ? B.group : (K < 32 ? K : 32);
@@ -545,6 +500,57 @@ int run_blocks(Plan &P, std::string &err) {
     CK(cudaGetLastError());
     return RBS_OK;
 }
+
+// The block walk of a (precision, K) pair is captured into a CUDA graph on
+// its second use (the first runs eagerly and performs the one-time set-up
+// that capture does not allow) and replayed afterwards: one launch per
+// solve pass instead of one per block.
+template <typename VT, int K>
+int run_blocks(Plan &P, std::string &err) {
+    DeviceState &D = *P.dev;
+    // per-block timing needs real event timestamps, which captured event
+    // records are not: profiled solves launch eagerly
+    if (!D.use_graphs || D.profile) return launch_blocks<VT, K>(P, err);
+    const long long key = (long long)K * 8 + (sizeof(VT) == 8 ? 0 : 2);
+    auto it = D.graphs.find(key);
+    if (it != D.graphs.end()) {
+        CK(cudaGraphLaunch(it->second, D.stream));
+        return RBS_OK;
+    }
+    if (!D.graph_seen.count(key)) {
+        D.graph_seen.insert(key);
+        return launch_blocks<VT, K>(P, err);
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(D.stream, cudaStreamCaptureModeThreadLocal));
+    int rc = launch_blocks<VT, K>(P, err);
+    cudaError_t e = cudaStreamEndCapture(D.stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e);
+        return RBS_ERR_CUDA;
+    }
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+        return RBS_ERR_CUDA;
+    }
+    D.graphs[key] = ex;
+    CK(cudaGraphLaunch(ex, D.stream));
+    return RBS_OK;
+}
+
+void drop_graphs(DeviceState &D) {
+    for (auto &kv : D.graphs) cudaGraphExecDestroy(kv.second);
+    D.graphs.clear();
+    D.graph_seen.clear();
+}
+void drop_graphs_fwd(DeviceState &D) { drop_graphs(D); }
 
 template <int K>
 int solve_fp64(Plan &P, const double *b, double *x, int k, int ld, std::string &err) {
@@ -638,6 +644,10 @@ int device_build(Plan &P, std::string &err) {
     D.own_stream = true;
     CK(cudaEventCreate(&D.ev0));
     CK(cudaEventCreate(&D.ev1));
+    {
+        const char *ng = std::getenv("RBS_NO_GRAPHS");
+        D.use_graphs = !(ng && ng[0] == '1');
+    }
     int rc;
     if ((rc = upload(D, D.rp, P.rp_pool, err))) return rc;
     if ((rc = upload(D, D.col, P.col_pool, err))) return rc;
@@ -675,7 +685,6 @@ int device_build(Plan &P, std::string &err) {
         if ((rc = upload(D, D.band_coef32, c32, err))) return rc;
         if ((rc = upload(D, D.band_inv32, i32, err))) return rc;
     }
-    if ((rc = upload(D, D.chunks, P.chunk_pool, err))) return rc;
     if ((rc = upload(D, D.ell_col, P.ell_col, err))) return rc;
     if ((rc = upload(D, D.ell_val, P.ell_val, err))) return rc;
     {
@@ -757,12 +766,12 @@ void device_free(Plan &P) {
     DeviceState &D = *P.dev;
     if (D.stream) cudaStreamSynchronize(D.stream);
     free_work(D);
+    drop_graphs(D);
     for (auto &e : D.bev) cudaEventDestroy(e);
     if (D.side) cudaStreamSynchronize(D.side);
     if (D.side) cudaStreamDestroy(D.side);
     if (D.ev_fork) cudaEventDestroy(D.ev_fork);
     if (D.ev_join) cudaEventDestroy(D.ev_join);
-    cudaFree(D.chunks);
     cudaFree(D.ell_col);
     cudaFree(D.ell_val);
     cudaFree(D.ell_val32);
@@ -877,11 +886,12 @@ int device_finish(Plan &P, rbs_stats *stats, int k, int prec, std::string &err) 
             float ms = 0;
             if (cudaEventElapsedTime(&ms, D.bev[2 * b], D.bev[2 * b + 1]) == cudaSuccess) D.bms[b] += ms;
         }
+        cudaGetLastError();  // a block without kernels has no timing: do not leave the error behind
         ++D.bsolves;
     }
     if (stats) {
         float ms = 0;
-        cudaEventElapsedTime(&ms, D.ev0, D.ev1);
+        if (cudaEventElapsedTime(&ms, D.ev0, D.ev1) != cudaSuccess) cudaGetLastError();
         const int iters = D.last_iters;
         stats->ms = ms;
         stats->iterations = iters;
