@@ -134,6 +134,51 @@ int rbs_plan_sync(rbs_plan *plan);
 int rbs_plan_set_stream(rbs_plan *plan, void *stream);
 int rbs_plan_info_get(const rbs_plan *plan, rbs_plan_info *info);
 
+/* Many independent systems as one plan (no counterpart in the reference,
+ * which solves one system per run).  The `count` systems (host arrays, each
+ * in the format of rbs_analyse, all of one direction) are placed on the
+ * diagonal of one block-diagonal matrix and analysed together: their level
+ * sets interleave in the level order, so a single solve walks all of them
+ * at once and every launch carries rows of many systems.  row_offsets
+ * (count+1 entries, output) gives where system i's rows start in the packed
+ * right-hand sides and solutions passed to rbs_solve / rbs_solve_host.
+ * lv = -1 means 0 here: one triangle, one persistent launch per pass. */
+int rbs_batch_analyse(int count, const int *const *ptr, const int *const *idx, const double *const *val,
+                      const int *n, const int *nnz, int fmt, int substitution, int lv, const rbs_options *opt,
+                      rbs_plan **plan, int *row_offsets);
+
+/* ---- request serving (no counterpart in the reference) ----------------
+ * A server keeps analysed factors resident on the device and runs one
+ * worker thread and CUDA stream per factor.  Submitted requests (host b and
+ * x, column-major n x k, a precision) queue per factor; a worker takes all
+ * queued requests of one precision that fit its batch width and solves
+ * them as ONE multi-RHS solve, so requests arriving while a batch runs join
+ * the next batch, while other factors run concurrently on their streams.
+ * A factor is admitted only if its plan plus workspace fit the remaining
+ * HBM budget (RBS_ERR_BUDGET otherwise). */
+typedef struct rbs_server rbs_server;
+typedef struct rbs_server_stats {
+    long long completed;    /* requests finished since the last reset */
+    long long solves;       /* right-hand sides solved */
+    long long batches;      /* multi-RHS solves run */
+    double mean_batch_rhs;  /* right-hand sides per batch */
+    double p50_ms, p99_ms;  /* request latency, submit -> result in x */
+    double solves_per_s;    /* right-hand sides / (last completion - first submit) */
+    int factors;
+    long long hbm_used;     /* bytes charged against the budget */
+} rbs_server_stats;
+
+int rbs_server_create(long long hbm_budget_bytes, int max_batch_rhs, rbs_server **server);
+/* On success the server owns the plan (freed by rbs_server_destroy). */
+int rbs_server_add_factor(rbs_server *server, rbs_plan *plan, int *factor_id);
+/* b and x must stay valid until rbs_server_wait returns for the ticket. */
+int rbs_server_submit(rbs_server *server, int factor_id, const double *b, double *x, int k, int prec,
+                      long long *ticket);
+int rbs_server_wait(rbs_server *server, long long ticket, double *latency_ms, int *batch_rhs);
+int rbs_server_stats_get(rbs_server *server, rbs_server_stats *stats);
+int rbs_server_reset_stats(rbs_server *server);
+int rbs_server_destroy(rbs_server *server);
+
 /* Copy a named integer (or, for "recblock_Val", double) output of the
  * analysis into dst.  Names follow the reference's variables: "levelItem",
  * "loc_off", "tmp_off", "blk_m", "blk_n", "blk_nnz", "subtri_up",

@@ -147,6 +147,16 @@ double block_bytes(const Plan &P, const ExecBlock &B) {
            (B.rows_off >= 0 ? 4.0 * B.nrows : 0.0);
 }
 
+// Layouts a triangle needs: the ones of its kernel, or, when the kernels
+// are chosen by measurement (RBS_SELECT_TUNE), every one it is eligible for.
+static bool wants_level(const ExecBlock &b, const rbs_options &opt) {
+    return b.tri && (b.kernel == RBS_K_LEVEL || (opt.select == RBS_SELECT_TUNE && b.nnz > b.m));
+}
+static bool wants_band(const ExecBlock &b, const rbs_options &opt) {
+    return b.tri && b.bandwidth <= 8 &&
+           (b.kernel == RBS_K_BANDSCAN || (opt.select == RBS_SELECT_TUNE && b.nnz > b.m));
+}
+
 int auto_lv(int m, int device_id) {
     // main.cu:245-254: smallest li >= 1 with m / 2^(li+1) below the wave size
     int li;
@@ -460,7 +470,7 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
                 ++pos;
             }
         }
-        if (B.tri && B.kernel == RBS_K_LEVEL) {
+        if (wants_level(B, opt)) {
             B.lvl_off = (long long)P.lvl_pool.size();
             P.lvl_pool.push_back(0);
             for (int L = 0; L < B.nlv; ++L) P.lvl_pool.push_back(P.lvl_pool.back() + lvl_sizes[b][L]);
@@ -511,7 +521,7 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
     P.band_coef.clear();
     P.band_inv.clear();
     for (ExecBlock &B : P.blocks) {
-        if (!B.tri || B.kernel != RBS_K_BANDSCAN) continue;
+        if (!wants_band(B, opt)) continue;
         int W = 1;
         while (W < std::max(1, B.bandwidth)) W <<= 1;
         B.band_w = W;
@@ -540,7 +550,7 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
     P.ell_chunks.clear();
     constexpr int RMAX = 512, EMAX = 2048;
     for (ExecBlock &B : P.blocks) {
-        if (!B.tri || B.kernel != RBS_K_LEVEL) continue;
+        if (!wants_level(B, opt)) continue;
         const int *rp = P.rp_pool.data() + B.rp_off;
         std::vector<int> cuts{0}, widths;
         bool ok = true;
@@ -595,7 +605,7 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
     P.ca_col.clear();
     P.ca_val.clear();
     for (ExecBlock &B : P.blocks) {
-        if (!B.tri || B.kernel != RBS_K_LEVEL || !B.contiguous) continue;
+        if (!wants_level(B, opt) || !B.contiguous) continue;
         const int *rp = P.rp_pool.data() + B.rp_off;
         const int *lvp = P.lvl_pool.data() + B.lvl_off;
         int wmax = 0;

@@ -68,6 +68,7 @@ int rbs_analyse(const int *ptr, const int *idx, const double *val, int n, int nn
     try {
         rc = rbs::analyse_host(P->p, ptr, idx, val, n, nnz, fmt, substitution, lv, o, err);
         if (rc == RBS_OK && !o.host_only) rc = rbs::device_build(P->p, err);
+        if (rc == RBS_OK && !o.host_only && o.select == RBS_SELECT_TUNE) rc = rbs::device_tune(P->p, err);
     } catch (const std::bad_alloc &) {
         rc = RBS_ERR_NOMEM;
         err = "rbs_analyse: out of host memory";
@@ -93,6 +94,42 @@ int rbs_analyse_device(const int *d_ptr, const int *d_idx, const double *d_val, 
     if (e == cudaSuccess) e = cudaMemcpy(val.data(), d_val, sizeof(double) * (size_t)nnz, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return fail(RBS_ERR_CUDA, std::string("rbs_analyse_device: ") + cudaGetErrorString(e));
     return rbs_analyse(ptr.data(), idx.data(), val.data(), n, nnz, fmt, substitution, lv, opt, plan);
+}
+
+int rbs_batch_analyse(int count, const int *const *ptr, const int *const *idx, const double *const *val,
+                      const int *n, const int *nnz, int fmt, int substitution, int lv, const rbs_options *opt,
+                      rbs_plan **plan, int *row_offsets) {
+    if (!plan || count <= 0 || !ptr || !idx || !val || !n || !nnz || !row_offsets)
+        return fail(RBS_ERR_ARG, "rbs_batch_analyse: bad arguments");
+    long long N = 0, Z = 0;
+    for (int i = 0; i < count; ++i) {
+        if (n[i] <= 0 || nnz[i] < n[i] || !ptr[i] || !idx[i] || !val[i])
+            return fail(RBS_ERR_ARG, "rbs_batch_analyse: system " + std::to_string(i) + " is malformed");
+        N += n[i];
+        Z += nnz[i];
+    }
+    if (N > 0x7fffffffLL || Z > 0x7fffffffLL) return fail(RBS_ERR_ARG, "rbs_batch_analyse: batch exceeds 2^31 rows or entries");
+    std::vector<int> bp((size_t)N + 1), bi((size_t)Z);
+    std::vector<double> bv((size_t)Z);
+    long long r0 = 0, z0 = 0;
+    row_offsets[0] = 0;
+    for (int i = 0; i < count; ++i) {
+        if (ptr[i][0] != 0 || ptr[i][n[i]] != nnz[i])
+            return fail(RBS_ERR_STRUCTURE, "rbs_batch_analyse: pointer array of system " + std::to_string(i) +
+                                               " must run from 0 to nnz");
+        for (int c = 0; c < n[i]; ++c) bp[(size_t)(r0 + c)] = (int)(z0 + ptr[i][c]);
+        for (int k = 0; k < nnz[i]; ++k) {
+            const int v = idx[i][k];
+            bi[(size_t)(z0 + k)] = (v >= 0 && v < n[i]) ? (int)(v + r0) : -1;  // -1 is rejected by the analysis
+            bv[(size_t)(z0 + k)] = val[i][k];
+        }
+        r0 += n[i];
+        z0 += nnz[i];
+        row_offsets[i + 1] = (int)r0;
+    }
+    bp[(size_t)N] = (int)Z;
+    return rbs_analyse(bp.data(), bi.data(), bv.data(), (int)N, (int)Z, fmt, substitution, lv < 0 ? 0 : lv, opt,
+                       plan);
 }
 
 static int check_solve_args(rbs_plan *plan, const double *b, const double *x, int k, int ld, int prec) {

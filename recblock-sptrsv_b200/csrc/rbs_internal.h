@@ -117,6 +117,7 @@ int device_finish(Plan &P, rbs_stats *stats, int k, int prec, std::string &err);
 void *device_stream(Plan &P);
 int device_set_stream(Plan &P, void *stream, std::string &err);
 int device_profile(Plan &P, int enable, std::string &err);
+int device_tune(Plan &P, std::string &err);
 int device_block_times(const Plan &P, std::vector<double> &ms, long long &solves);
 int device_staging(Plan &P, size_t bytes, double *&db, double *&dx, std::string &err);
 double block_bytes(const Plan &P, const ExecBlock &B);

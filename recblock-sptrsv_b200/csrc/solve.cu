@@ -761,6 +761,84 @@ int device_staging(Plan &P, size_t bytes, double *&db, double *&dx, std::string 
     return RBS_OK;
 }
 
+namespace {
+
+void drop_descs(DeviceState &D) {
+    for (auto &kv : D.desc_cache) cudaFree(kv.second);
+    D.desc_cache.clear();
+    for (auto &kv : D.ell_cache) cudaFree(kv.second);
+    D.ell_cache.clear();
+    for (auto &kv : D.ca_cache) cudaFree(kv.second);
+    D.ca_cache.clear();
+    drop_graphs(D);
+}
+
+// RBS_SELECT_TUNE: run the plan with every triangle on one candidate kernel
+// family at a time (sync-free, single-CTA level, band scan where a band
+// layout exists), time each triangle with CUDA events, and keep for every
+// triangle the fastest.  Squares keep their SpMV plan.
+int tune_kernels(Plan &P, std::string &err) {
+    DeviceState &D = *P.dev;
+    const size_t nb = P.blocks.size();
+    std::vector<int> orig(nb);
+    for (size_t b = 0; b < nb; ++b) orig[b] = P.blocks[b].kernel;
+    std::vector<double> best(nb, 1e300);
+    std::vector<int> pick(orig);
+    double *db = nullptr, *dx = nullptr;
+    CK(cudaMalloc(&db, sizeof(double) * (size_t)P.n));
+    CK(cudaMalloc(&dx, sizeof(double) * (size_t)P.n));
+    k_fill<double><<<grid_for(P.n, 256, D.num_sms), 256, 0, D.stream>>>(db, P.n, 1.0);
+    int rc = RBS_OK;
+    const int cands[3] = {RBS_K_SYNCFREE, RBS_K_LEVEL, RBS_K_BANDSCAN};
+    for (int ci = 0; ci < 3 && rc == RBS_OK; ++ci) {
+        const int cand = cands[ci];
+        bool any = false;
+        for (size_t b = 0; b < nb; ++b) {
+            ExecBlock &B = P.blocks[b];
+            if (!B.tri || B.nnz == B.m) continue;
+            const bool ok = cand != RBS_K_BANDSCAN || B.band_w > 0;
+            B.kernel = ok ? cand : orig[b];
+            any = any || ok;
+        }
+        if (!any) continue;
+        drop_descs(D);
+        if ((rc = device_profile(P, 1, err))) break;
+        for (int rep = 0; rep < 3 && rc == RBS_OK; ++rep) {
+            if (rep == 1 && (rc = device_profile(P, 1, err))) break;  // first solve is the warm-up
+            rc = device_solve(P, db, dx, 1, P.n, RBS_PREC_FP64, true, nullptr, err);
+        }
+        if (rc) break;
+        std::vector<double> ms;
+        long long solves = 0;
+        device_block_times(P, ms, solves);
+        for (size_t b = 0; b < nb; ++b) {
+            const ExecBlock &B = P.blocks[b];
+            if (!B.tri || B.nnz == B.m || B.kernel != cand) continue;
+            const double t = ms[b] / std::max(1ll, solves);
+            if (t < best[b]) {
+                best[b] = t;
+                pick[b] = cand;
+            }
+        }
+    }
+    for (size_t b = 0; b < nb; ++b) P.blocks[b].kernel = rc == RBS_OK ? pick[b] : orig[b];
+    drop_descs(D);
+    device_profile(P, 0, err);
+    cudaFree(db);
+    cudaFree(dx);
+    return rc;
+}
+
+}  // namespace
+
+int device_tune(Plan &P, std::string &err) {
+    if (!P.dev) {
+        err = "plan has no device state";
+        return RBS_ERR_ARG;
+    }
+    return tune_kernels(P, err);
+}
+
 void device_free(Plan &P) {
     if (!P.dev) return;
     DeviceState &D = *P.dev;

@@ -73,6 +73,20 @@ class PlanInfo(ctypes.Structure):
     ]
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("completed", ctypes.c_longlong),
+        ("solves", ctypes.c_longlong),
+        ("batches", ctypes.c_longlong),
+        ("mean_batch_rhs", ctypes.c_double),
+        ("p50_ms", ctypes.c_double),
+        ("p99_ms", ctypes.c_double),
+        ("solves_per_s", ctypes.c_double),
+        ("factors", ctypes.c_int),
+        ("hbm_used", ctypes.c_longlong),
+    ]
+
+
 class GenSpec(ctypes.Structure):
     _fields_ = [
         ("kind", ctypes.c_int),
@@ -93,7 +107,8 @@ EXPORTS = [
     "rbs_solve_async", "rbs_plan_sync", "rbs_plan_set_stream", "rbs_plan_info_get", "rbs_plan_export",
     "rbs_plan_free", "rbs_last_error", "rbs_auto_lv", "recblocking_solver_cuda", "recblocking_solver",
     "rbs_gen_lower_csr", "rbs_gen_uniform", "rbs_gen_free", "rbs_plan_profile", "rbs_plan_block_times",
-    "rbs_sptrsv_csr_noalloc",
+    "rbs_sptrsv_csr_noalloc", "rbs_batch_analyse", "rbs_server_create", "rbs_server_add_factor",
+    "rbs_server_submit", "rbs_server_wait", "rbs_server_stats_get", "rbs_server_reset_stats", "rbs_server_destroy",
 ]
 
 
@@ -138,6 +153,17 @@ def _load():
     lib.rbs_plan_profile.argtypes = [P, ctypes.c_int]
     lib.rbs_plan_block_times.argtypes = [P, dp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
     lib.rbs_sptrsv_csr_noalloc.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, P, P, P]
+    lib.rbs_server_create.argtypes = [ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(P)]
+    lib.rbs_server_add_factor.argtypes = [P, P, ip]
+    lib.rbs_server_submit.argtypes = [P, ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_longlong)]
+    lib.rbs_server_wait.argtypes = [P, ctypes.c_longlong, dp, ip]
+    lib.rbs_server_stats_get.argtypes = [P, ctypes.POINTER(ServerStats)]
+    lib.rbs_server_reset_stats.argtypes = [P]
+    lib.rbs_server_destroy.argtypes = [P]
+    lib.rbs_batch_analyse.argtypes = [ctypes.c_int, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(dp), ip, ip,
+                                      ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Options),
+                                      ctypes.POINTER(P), ip]
     return lib
 
 
@@ -184,9 +210,9 @@ class Plan:
         self.free()
 
     def free(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and lib is not None:
             lib.rbs_plan_free(self._h)
-            self._h = None
+        self._h = None
 
     @property
     def handle(self):
@@ -260,6 +286,70 @@ def analyse(ptr: np.ndarray, idx: np.ndarray, val: np.ndarray, substitution: int
     _check(lib.rbs_analyse(_ip(ptr), _ip(idx), _dp(val), n, len(idx), fmt, substitution, lv,
                            ctypes.byref(opts) if opts is not None else None, ctypes.byref(h)))
     return Plan(h, n)
+
+
+def batch_analyse(systems, substitution: int = FORWARD, lv: int = -1, fmt: int = FMT_CSC,
+                  opts: Options | None = None):
+    """rbs_batch_analyse: systems is a list of (ptr, idx, val); returns (Plan, row_offsets)."""
+    cnt = len(systems)
+    keep = [(np.ascontiguousarray(p, np.int32), np.ascontiguousarray(i, np.int32), np.ascontiguousarray(v, np.float64))
+            for p, i, v in systems]
+    P = (ctypes.POINTER(ctypes.c_int) * cnt)(*[_ip(k[0]) for k in keep])
+    I = (ctypes.POINTER(ctypes.c_int) * cnt)(*[_ip(k[1]) for k in keep])
+    V = (ctypes.POINTER(ctypes.c_double) * cnt)(*[_dp(k[2]) for k in keep])
+    ns = np.array([len(k[0]) - 1 for k in keep], np.int32)
+    zs = np.array([len(k[1]) for k in keep], np.int32)
+    offs = np.zeros(cnt + 1, np.int32)
+    h = ctypes.c_void_p()
+    _check(lib.rbs_batch_analyse(cnt, P, I, V, _ip(ns), _ip(zs), fmt, substitution, lv,
+                                 ctypes.byref(opts) if opts is not None else None, ctypes.byref(h), _ip(offs)))
+    return Plan(h, int(offs[-1])), offs
+
+
+class Server:
+    """rbs_server: device-resident factors, continuous batching, latency stats."""
+
+    def __init__(self, hbm_budget_bytes: int, max_batch_rhs: int = 16):
+        self._h = ctypes.c_void_p()
+        _check(lib.rbs_server_create(hbm_budget_bytes, max_batch_rhs, ctypes.byref(self._h)))
+        self._keep = {}
+
+    def add_factor(self, plan: Plan) -> int:
+        fid = ctypes.c_int()
+        _check(lib.rbs_server_add_factor(self._h, plan.handle, ctypes.byref(fid)))
+        plan._h = None  # owned by the server now
+        return fid.value
+
+    def submit(self, factor: int, b: np.ndarray, x: np.ndarray, k: int = 1, prec: int = PREC_FP64) -> int:
+        assert b.dtype == np.float64 and x.dtype == np.float64 and b.flags.c_contiguous and x.flags.c_contiguous
+        t = ctypes.c_longlong()
+        _check(lib.rbs_server_submit(self._h, factor, _dp(b), _dp(x), k, prec, ctypes.byref(t)))
+        self._keep[t.value] = (b, x)
+        return t.value
+
+    def wait(self, ticket: int):
+        lat = ctypes.c_double()
+        bk = ctypes.c_int()
+        rc = lib.rbs_server_wait(self._h, ticket, ctypes.byref(lat), ctypes.byref(bk))
+        self._keep.pop(ticket, None)
+        _check(rc)
+        return lat.value, bk.value
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        _check(lib.rbs_server_stats_get(self._h, ctypes.byref(st)))
+        return st
+
+    def reset_stats(self):
+        _check(lib.rbs_server_reset_stats(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) and lib is not None:
+            lib.rbs_server_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 def analyse_device(ptr, idx, val, n: int, nnz: int, substitution: int = FORWARD, lv: int = -1,
