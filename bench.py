@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-sweep", action="store_true", help="skip the structure/variant side measurements")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 512-system batched measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, side measurements and the CPU baseline "
                                                                "(short runs for profilers)")
     return ap.parse_args()
@@ -73,6 +75,7 @@ def make_system(kind, sub, seed_x=1):
         "c1b": dict(kind=rbs.GEN_ZIPF, n=2000000, zipf_alpha=2.1, zipf_max=1000, seed=102),
         "c1c": dict(kind=rbs.GEN_CHAIN, n=1000000, chain_bw=3, seed=103),
         "c0": dict(kind=rbs.GEN_BAND_POISSON, n=16384, lam=6, band=512, seed=100),
+        "c2r": dict(kind=rbs.GEN_BAND_POISSON, n=4000000, lam=10, band=4096, seed=104),
     }
     rp, ci, va = rbs.gen_lower_csr(**specs[kind])
     n = len(rp) - 1
@@ -200,6 +203,279 @@ def timed_solves(plan, db, dx, steps, flush, k=1, prec=0):
         st = plan.solve(db, dx, k=k, prec=prec)
         ms.append(st.ms)
     return ms, st
+
+
+def rel(x, ref):
+    return float(np.linalg.norm(x - ref) / np.linalg.norm(ref))
+
+
+def measure(plan, dB, dX, flush, reps, k=1, prec=0):
+    """Mean device ms of `reps` solves after two warm-up solves."""
+    timed_solves(plan, dB, dX, 2, flush, k=k, prec=prec)
+    ms, st = timed_solves(plan, dB, dX, reps, flush, k=k, prec=prec)
+    return float(np.mean(ms)), st
+
+
+def side_multi_rhs(plan, sysm, dev, flush, args):
+    """Multi-RHS column blocks on the 2D-Laplacian factor: k in {1, 8, 32,
+    128}, FP64 and FP32 sweeps + FP64 refinement.  Columns of X_true are
+    U(-1,1); B = L X_true."""
+    import torch
+
+    import rbs
+
+    out = {}
+    reps = max(3, args.steps // 10)
+    A = sysm["A"]
+    for k in (1, 8, 32, 128):
+        Xt = np.stack([sysm["x_true"]] + [rbs.gen_uniform(1000 + c, sysm["n"]) for c in range(1, k)])
+        B = np.ascontiguousarray((A @ Xt.T).T)
+        dB = torch.tensor(B, dtype=torch.float64, device=dev).reshape(-1)
+        dX = torch.empty_like(dB)
+        for pname, prec in (("fp64", rbs.PREC_FP64), ("mixed", rbs.PREC_MIXED)):
+            ms, st = measure(plan, dB, dX, flush, reps, k=k, prec=prec)
+            X = dX.cpu().numpy().reshape(k, -1)
+            out[f"{pname}_k{k}"] = {"solves_per_s": k * 1000.0 / ms, "ms": ms, "iterations": st.iterations,
+                                    "rel_err_vs_x_true": max(rel(X[c], Xt[c]) for c in range(k)),
+                                    "useful_gb": st.useful_bytes / 1e9, "moved_gb": st.moved_bytes / 1e9,
+                                    "gb_per_s": st.useful_bytes / (ms / 1000) / 1e9}
+        del dB, dX
+    base = out["fp64_k1"]["solves_per_s"]
+    for v in out.values():
+        v["x_plain_fp64_k1"] = v["solves_per_s"] / base
+    return out
+
+
+def side_structures(dev, flush, args):
+    """Config-1 structures and directions other than the headline."""
+    import torch
+
+    import rbs
+
+    sweep = {}
+    for kind, sub in (("c1a", rbs.BACKWARD), ("c1b", rbs.FORWARD), ("c1b", rbs.BACKWARD), ("c1c", rbs.FORWARD),
+                      ("c1c", rbs.BACKWARD)):
+        s2 = make_system(kind, sub)
+        p2 = rbs.analyse(s2["cp"], s2["ri"], s2["cv"], substitution=sub, lv=-1)
+        d_b = torch.tensor(s2["b"], dtype=torch.float64, device=dev)
+        d_x = torch.empty_like(d_b)
+        ms, st = measure(p2, d_b, d_x, flush, max(3, args.steps // 10))
+        xs = d_x.cpu().numpy()
+        inf2 = p2.info()
+        sweep[f"{kind}_{'fwd' if sub == 0 else 'bwd'}"] = {
+            "solves_per_s": 1000.0 / ms, "ms": ms, "gb_per_s": st.useful_bytes / (ms / 1000) / 1e9,
+            "rel_err_vs_x_true": rel(xs, s2["x_true"]), "n": s2["n"], "nnz": s2["nnz"], "nlevel": inf2.nlevel,
+            "lv": inf2.lv, "analyse_ms": inf2.analyse_ms,
+            "kernels": {rbs.KERNEL_NAMES[i]: inf2.kernels[i] for i in range(7) if inf2.kernels[i]}}
+        del p2
+    return sweep
+
+
+def side_mixed(dev, flush, args):
+    """FP32 sweeps + FP64 refinement against the plain FP64 solve on the
+    2D-Laplacian factor, the power-law factor and the n = 4M Poisson(10)
+    band-4096 factor; errors against the serial FP64 oracle."""
+    import torch
+
+    import rbs
+    from oracle import oracle
+
+    out = {}
+    for kind in ("c1a", "c1b", "c2r"):
+        s2 = make_system(kind, rbs.FORWARD)
+        A = s2["A"]
+        xo = oracle.sptrsv_csr(A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data, rbs.FORWARD, s2["b"])
+        p2 = rbs.analyse(s2["cp"], s2["ri"], s2["cv"], substitution=rbs.FORWARD, lv=-1)
+        d_b = torch.tensor(s2["b"], dtype=torch.float64, device=dev)
+        d_x = torch.empty_like(d_b)
+        reps = max(3, args.steps // 10)
+        ms64, st64 = measure(p2, d_b, d_x, flush, reps)
+        e64 = rel(d_x.cpu().numpy(), xo)
+        msmx, stmx = measure(p2, d_b, d_x, flush, reps, prec=rbs.PREC_MIXED)
+        emx = rel(d_x.cpu().numpy(), xo)
+        out[kind] = {"n": s2["n"], "nnz": s2["nnz"], "nlevel": p2.info().nlevel,
+                     "fp64": {"ms": ms64, "solves_per_s": 1000.0 / ms64, "rel_err_vs_oracle": e64,
+                              "gb_per_s": st64.useful_bytes / (ms64 / 1000) / 1e9},
+                     "mixed": {"ms": msmx, "solves_per_s": 1000.0 / msmx, "rel_err_vs_oracle": emx,
+                               "iterations": stmx.iterations, "useful_gb": stmx.useful_bytes / 1e9,
+                               "moved_gb": stmx.moved_bytes / 1e9,
+                               "gb_per_s_useful": stmx.useful_bytes / (msmx / 1000) / 1e9}}
+        del p2, d_b, d_x
+    return out
+
+
+def side_batched(dev, args):
+    """512 independent lower-triangular systems (n log-uniform in [1k, 200k],
+    Poisson(8) off-diagonals in a band of 256, one RHS each) solved as one
+    block-diagonal plan (one graph-captured walk, measured kernel choice),
+    against the plain FP64 path: each system alone through its own plan."""
+    import torch
+
+    import rbs
+
+    rng = np.random.default_rng(303)
+    ns = np.exp(rng.uniform(np.log(1000), np.log(200000), 512)).astype(int)
+    systems, bs, xts = [], [], []
+    for i, n in enumerate(ns):
+        rp, ci, va = rbs.gen_lower_csr(rbs.GEN_BAND_POISSON, n=int(n), lam=8, band=256, seed=5000 + i)
+        xt = rbs.gen_uniform(9000 + i, int(n))
+        import scipy.sparse as sp
+        b = sp.csr_matrix((va, ci, rp), shape=(int(n), int(n))) @ xt
+        systems.append((rp, ci, va))
+        bs.append(b)
+        xts.append(xt)
+    t0 = time.perf_counter()
+    plan, offs = rbs.batch_analyse(systems, substitution=rbs.FORWARD, fmt=rbs.FMT_CSR,
+                                   opts=rbs.options(select=rbs.SELECT_TUNE))
+    t_an = time.perf_counter() - t0
+    B = np.concatenate(bs)
+    Xt = np.concatenate(xts)
+    dB = torch.tensor(B, dtype=torch.float64, device=dev)
+    dX = torch.empty_like(dB)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    res = {"systems": 512, "rows": int(ns.sum()), "nnz": int(sum(len(s[1]) for s in systems)),
+           "analyse_s": t_an, "nlevel": plan.info().nlevel, "lv": plan.info().lv}
+    for pname, prec in (("fp64", rbs.PREC_FP64), ("mixed", rbs.PREC_MIXED)):
+        ms, st = measure(plan, dB, dX, flush, 5, prec=prec)
+        X = dX.cpu().numpy()
+        err = max(rel(X[offs[i]:offs[i + 1]], xts[i]) for i in range(512))
+        res[f"batched_{pname}"] = {"ms": ms, "solves_per_s": 512 * 1000.0 / ms, "iterations": st.iterations,
+                                   "max_rel_err_vs_x_true": err, "gb_per_s": st.useful_bytes / (ms / 1000) / 1e9}
+    del plan, dB, dX
+    # plain FP64, one plan and one solve per system (warm L2: conservative for the ratio)
+    plain_ms = 0.0
+    perr = 0.0
+    for i, (rp, ci, va) in enumerate(systems):
+        p1 = rbs.analyse(rp, ci, va, substitution=rbs.FORWARD, lv=-1, fmt=rbs.FMT_CSR)
+        d_b = torch.tensor(bs[i], dtype=torch.float64, device=dev)
+        d_x = torch.empty_like(d_b)
+        for _ in range(2):
+            p1.solve(d_b, d_x)
+        ms = [p1.solve(d_b, d_x).ms for _ in range(3)]
+        plain_ms += float(np.mean(ms))
+        perr = max(perr, rel(d_x.cpu().numpy(), xts[i]))
+        del p1
+    res["plain_fp64_per_system"] = {"ms_total": plain_ms, "solves_per_s": 512 * 1000.0 / plain_ms,
+                                    "max_rel_err_vs_x_true": perr}
+    for pname in ("fp64", "mixed"):
+        res[f"batched_{pname}"]["x_plain_fp64"] = res[f"batched_{pname}"]["solves_per_s"] / \
+            res["plain_fp64_per_system"]["solves_per_s"]
+    return res
+
+
+def serving_factors(count=64, seed=404):
+    """64 factors, n log-uniform in [10k, 2M], structures cycling through
+    the 2D Laplacian, power-law rows and the banded chain."""
+    import rbs
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+        kind = i % 3
+        if kind == 0:
+            L = rbs.gen_lower_csr(rbs.GEN_LAPLACE2D, grid=max(2, int(round(np.sqrt(n)))), seed=7000 + i)
+        elif kind == 1:
+            L = rbs.gen_lower_csr(rbs.GEN_ZIPF, n=n, zipf_alpha=2.1, zipf_max=1000, seed=7000 + i)
+        else:
+            L = rbs.gen_lower_csr(rbs.GEN_CHAIN, n=n, chain_bw=3, seed=7000 + i)
+        out.append(L)
+    return out
+
+
+def side_serving(dev, args, n_requests=1500, loads=(1000, 10000, 50000)):
+    """Poisson request arrivals over 64 device-resident factors; each request
+    carries 1-16 RHS; the server batches across and within factors and runs
+    FP32 sweeps + FP64 refinement.  The plain arm serves the same arrivals
+    one request at a time with an FP64 solve (host arrays in and out)."""
+    import threading
+
+    import rbs
+
+    facs = serving_factors()
+    ns = [len(L[0]) - 1 for L in facs]
+    t0 = time.perf_counter()
+    plans = [rbs.analyse(*L, substitution=rbs.FORWARD, lv=-1, fmt=rbs.FMT_CSR) for L in facs]
+    t_an = time.perf_counter() - t0
+    rng = np.random.default_rng(505)
+    Bh = [rbs.gen_uniform(11000 + i, 16 * n).reshape(16, n) for i, n in enumerate(ns)]
+    Xh = [np.empty((16, n)) for n in ns]
+    res = {"factors": 64, "rows": int(sum(ns)), "nnz": int(sum(len(L[1]) for L in facs)), "analyse_s": t_an,
+           "requests_per_load": n_requests, "rhs_per_request": "uniform 1..16", "loads": {}}
+
+    def schedule(rate):
+        gaps = rng.exponential(1.0 / rate, n_requests)
+        return np.cumsum(gaps), rng.integers(0, 64, n_requests), rng.integers(1, 17, n_requests)
+
+    scheds = {rate: schedule(rate) for rate in loads}
+    # plain: one FP64 solve per request, in arrival order, on the caller's thread
+    plain = {}
+    for rate in loads:
+        arr, fid, ks = scheds[rate]
+        lat = []
+        t_start = time.perf_counter()
+        for a, f, k in zip(arr, fid, ks):
+            while time.perf_counter() - t_start < a:
+                pass
+            plans[f].solve_host(Bh[f][:k], k=int(k), x=Xh[f][:k])
+            lat.append(time.perf_counter() - t_start - a)
+        span = time.perf_counter() - t_start
+        plain[rate] = {"p50_ms": 1000 * float(np.percentile(lat, 50)), "p99_ms": 1000 * float(np.percentile(lat, 99)),
+                       "solves_per_s": float(ks.sum()) / span, "requests_per_s": n_requests / span}
+    srv = rbs.Server(150 << 30, max_batch_rhs=16)
+    old_si = sys.getswitchinterval()
+    sys.setswitchinterval(1e-4)  # the submit loop and the waiter share the interpreter
+    for p in plans:
+        srv.add_factor(p)
+    plans = None
+    for rate in loads:
+        arr, fid, ks = scheds[rate]
+        srv.reset_stats()
+        tickets = []
+        done = threading.Event()
+        lats = []
+
+        def waiter():
+            i = 0
+            while i < n_requests:
+                while i >= len(tickets):
+                    time.sleep(0)
+                lats.append(srv.wait(tickets[i])[0])
+                i += 1
+            done.set()
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        lag = []
+        t_start = time.perf_counter()
+        for a, f, k in zip(arr, fid, ks):
+            while time.perf_counter() - t_start < a:
+                pass
+            lag.append(1000 * (time.perf_counter() - t_start - a))
+            tickets.append(srv.submit(int(f), Bh[f][:k], Xh[f][:k], k=int(k), prec=rbs.PREC_MIXED))
+        th.join()
+        lats = np.array(lats) + np.array(lag)  # latency from the scheduled arrival, as for the plain arm
+        span = time.perf_counter() - t_start
+        st = srv.stats()
+        res["loads"][str(rate)] = {
+            "served_mixed": {"p50_ms": float(np.percentile(lats, 50)), "p99_ms": float(np.percentile(lats, 99)),
+                             "solves_per_s": float(ks.sum()) / span, "requests_per_s": n_requests / span,
+                             "mean_batch_rhs": st.mean_batch_rhs, "batches": st.batches},
+            "plain_fp64": plain[rate]}
+        res["loads"][str(rate)]["x_plain_fp64"] = float(ks.sum()) / span / plain[rate]["solves_per_s"]
+    # accuracy: every factor once, b = L x_true, served mixed vs x_true
+    import scipy.sparse as sp
+    worst = 0.0
+    for i, (rp, ci, va) in enumerate(facs):
+        xt = rbs.gen_uniform(13000 + i, ns[i])
+        b = sp.csr_matrix((va, ci, rp), shape=(ns[i], ns[i])) @ xt
+        x = np.empty_like(b)
+        srv.wait(srv.submit(i, b, x, k=1, prec=rbs.PREC_MIXED))
+        worst = max(worst, rel(x, xt))
+    res["max_rel_err_vs_x_true"] = worst
+    sys.setswitchinterval(old_si)
+    srv.close()
+    return res
 
 
 def launches_per_solve(plan):
@@ -334,43 +610,14 @@ def run_ours(args):
     }
 
     if not args.no_sweep:
-        side = {}
-        # precision / batching variants on the same factor
-        for name, k, prec in (("mixed_k1", 1, rbs.PREC_MIXED), ("fp64_k8", 8, rbs.PREC_FP64),
-                              ("mixed_k8", 8, rbs.PREC_MIXED), ("fp64_k32", 32, rbs.PREC_FP64),
-                              ("mixed_k32", 32, rbs.PREC_MIXED)):
-            B = np.stack([sysm["b"]] * k)
-            dB = torch.tensor(B, dtype=torch.float64, device=dev).reshape(-1)
-            dX = torch.empty_like(dB)
-            timed_solves(plan, dB, dX, 2, flush, k=k, prec=prec)
-            vms, vst = timed_solves(plan, dB, dX, max(3, args.steps // 10), flush, k=k, prec=prec)
-            X = dX.cpu().numpy().reshape(k, -1)
-            verr = max(float(np.linalg.norm(X[c] - sysm["x_true"]) / np.linalg.norm(sysm["x_true"])) for c in range(k))
-            side[name] = {"solves_per_s": k * 1000.0 / float(np.mean(vms)), "ms": float(np.mean(vms)),
-                          "iterations": vst.iterations, "rel_err_vs_x_true": verr,
-                          "moved_gb": vst.moved_bytes / 1e9}
-        line["variants_c1a"] = side
+        line["config3_multi_rhs_c1a"] = side_multi_rhs(plan, sysm, dev, flush, args)
         del plan
-        # the other config-1 structures and directions
-        sweep = {}
-        for kind, sub in (("c1a", rbs.BACKWARD), ("c1b", rbs.FORWARD), ("c1b", rbs.BACKWARD), ("c1c", rbs.FORWARD),
-                          ("c1c", rbs.BACKWARD)):
-            s2 = make_system(kind, sub)
-            p2 = rbs.analyse(s2["cp"], s2["ri"], s2["cv"], substitution=sub, lv=-1)
-            d_b = torch.tensor(s2["b"], dtype=torch.float64, device=dev)
-            d_x = torch.empty_like(d_b)
-            timed_solves(p2, d_b, d_x, 2, flush)
-            sms, sst = timed_solves(p2, d_b, d_x, max(3, args.steps // 10), flush)
-            xs = d_x.cpu().numpy()
-            inf2 = p2.info()
-            sweep[f"{kind}_{'fwd' if sub == 0 else 'bwd'}"] = {
-                "solves_per_s": 1000.0 / float(np.mean(sms)), "ms": float(np.mean(sms)),
-                "gb_per_s": sst.useful_bytes / (float(np.mean(sms)) / 1000) / 1e9,
-                "rel_err_vs_x_true": float(np.linalg.norm(xs - s2["x_true"]) / np.linalg.norm(s2["x_true"])),
-                "n": s2["n"], "nnz": s2["nnz"], "nlevel": inf2.nlevel, "lv": inf2.lv,
-                "kernels": {rbs.KERNEL_NAMES[i]: inf2.kernels[i] for i in range(7) if inf2.kernels[i]}}
-            del p2
-        line["sweep_config1"] = sweep
+        line["sweep_config1"] = side_structures(dev, flush, args)
+        line["config2_mixed"] = side_mixed(dev, flush, args)
+    if not args.no_batch:
+        line["config3_batched_512"] = side_batched(dev, args)
+    if not args.no_serve:
+        line["config4_serving"] = side_serving(dev, args)
 
     if rank == 0 and world == 1:
         xo, times = cpu_serial(sysm, budget_s=8.0, max_reps=200)

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "lc_layout.h"
 #include "rbs_internal.h"
 
 namespace rbs {
@@ -157,6 +158,215 @@ static bool wants_band(const ExecBlock &b, const rbs_options &opt) {
            (b.kernel == RBS_K_BANDSCAN || (opt.select == RBS_SELECT_TUNE && b.nnz > b.m));
 }
 
+// Level-chunk layout of every level triangle (level_lc.cuh).  Rows of each
+// independent segment (the whole triangle, or the rows of one system of a
+// batch) are listed level by level; a chunk takes consecutive rows of one
+// level while it stays within LC_RMAX rows and LC_FMAX bytes of ring
+// footprint.  Entries whose dependency lies LC_D or more chunks back are
+// "old" (gathered ahead), the others "recent" (window).  Records are placed
+// in the kernel's shared-memory ring in order, wrapping to 0 when the next
+// one does not fit; a record's copy is issued once every chunk whose ring
+// bytes it reuses has been solved and its mbarrier slot is free.
+static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &level) {
+    P.lc_rec64.clear();
+    P.lc_rec32.clear();
+    P.lc_tab.clear();
+    P.lc_segs.clear();
+    for (ExecBlock &B : P.blocks) {
+        B.lc_ok = 0;
+        B.lc_nseg = 0;
+        B.lc_seg_off = -1;
+        if (!wants_level(B, opt) || B.nnz == B.m) continue;
+        const int m = B.m;
+        const int *rp = P.rp_pool.data() + B.rp_off;
+        const int *cl = P.col_pool.data();
+        const double *vl = P.val_pool.data();
+        // segment of every row (ids in order of first appearance)
+        int nseg = 1;
+        std::vector<int> seg((size_t)m, 0);
+        if (!P.seg_rows.empty()) {
+            std::vector<int> id(P.seg_rows.size(), -1);
+            nseg = 0;
+            for (int r = 0; r < m; ++r) {
+                const int o = P.perm[(size_t)B.r0 + r];
+                const int sgi = (int)(std::upper_bound(P.seg_rows.begin(), P.seg_rows.end(), o) - P.seg_rows.begin()) - 1;
+                if (id[(size_t)sgi] < 0) id[(size_t)sgi] = nseg++;
+                seg[(size_t)r] = id[(size_t)sgi];
+            }
+        }
+        // rows level by level (stable), then split by segment
+        std::vector<int> lstart((size_t)B.nlv + 1, 0);
+        for (int r = 0; r < m; ++r) lstart[(size_t)level[(size_t)B.r0 + r] + 1]++;
+        for (int l = 0; l < B.nlv; ++l) lstart[(size_t)l + 1] += lstart[(size_t)l];
+        std::vector<int> bylev((size_t)m);
+        {
+            std::vector<int> fill(lstart.begin(), lstart.end() - 1);
+            for (int r = 0; r < m; ++r) bylev[(size_t)fill[(size_t)level[(size_t)B.r0 + r]]++] = r;
+        }
+        std::vector<int> scount((size_t)nseg + 1, 0);
+        for (int r = 0; r < m; ++r) scount[(size_t)seg[(size_t)r] + 1]++;
+        for (int q = 0; q < nseg; ++q) scount[(size_t)q + 1] += scount[(size_t)q];
+        std::vector<int> seq((size_t)m), vpos((size_t)m);
+        {
+            std::vector<int> fill(scount.begin(), scount.end() - 1);
+            for (int t = 0; t < m; ++t) {
+                const int r = bylev[(size_t)t], q = seg[(size_t)r];
+                vpos[(size_t)r] = fill[(size_t)q] - scount[(size_t)q];
+                seq[(size_t)fill[(size_t)q]++] = r;
+            }
+        }
+        struct Ch { int v0, nr, no, nrec; };
+        std::vector<std::vector<Ch>> chunks((size_t)nseg);
+        bool ok = true;
+        for (int q = 0; q < nseg && ok; ++q) {
+            const int *sq = seq.data() + scount[(size_t)q];
+            const int len = scount[(size_t)q + 1] - scount[(size_t)q];
+            auto &ch = chunks[(size_t)q];
+            int i = 0;
+            while (i < len) {
+                const int L = level[(size_t)B.r0 + sq[i]];
+                const int j = (int)ch.size();
+                const int vlim = j >= LC_D ? ch[(size_t)(j - LC_D)].v0 : 0;
+                int nr = 0, no = 0, nrec = 0;
+                while (i + nr < len && nr < LC_RMAX && level[(size_t)B.r0 + sq[i + nr]] == L) {
+                    const int r = sq[i + nr];
+                    int ro = 0, rr = 0;
+                    for (int k = rp[r]; k < rp[r + 1]; ++k) (vpos[(size_t)cl[k]] < vlim ? ro : rr)++;
+                    if (lc_foot_bytes(nr + 1, no + ro, nrec + rr, 8) > LC_FMAX) break;
+                    ++nr;
+                    no += ro;
+                    nrec += rr;
+                }
+                if (nr == 0) {  // one row alone does not fit the ring
+                    ok = false;
+                    break;
+                }
+                ch.push_back({i, nr, no, nrec});
+                i += nr;
+            }
+        }
+        if (!ok) continue;
+        // ring placement and issue iterations
+        std::vector<std::vector<int>> roff((size_t)nseg), iss((size_t)nseg);
+        for (int q = 0; q < nseg && ok; ++q) {
+            const auto &ch = chunks[(size_t)q];
+            const int nch = (int)ch.size();
+            auto &ro = roff[(size_t)q];
+            auto &is = iss[(size_t)q];
+            ro.resize((size_t)nch);
+            is.resize((size_t)nch);
+            long long head = 0;
+            std::vector<long long> fb((size_t)nch);
+            for (int j = 0; j < nch; ++j) {
+                const long long F = lc_foot_bytes(ch[(size_t)j].nr, ch[(size_t)j].no, ch[(size_t)j].nrec, 8);
+                fb[(size_t)j] = F;
+                if (head + F > LC_RING) head = 0;
+                ro[(size_t)j] = (int)(head / 16);
+                head += F;
+                // mbarrier slot j % LC_NB: every thread must have seen chunk j - LC_NB
+                // land (its gather, at chunk iteration j - LC_NB - LC_D or in the
+                // prologue) and passed a CTA barrier since, i.e. the end of that
+                // iteration (iteration 0 for chunks gathered in the prologue)
+                int at = j > 0 ? is[(size_t)j - 1] : 0;
+                if (j >= LC_NB) at = std::max(at, std::max(1, j - LC_NB - LC_D + 1));
+                long long scanned = 0;
+                for (int k = j - 1; k >= 0 && scanned <= 2LL * LC_RING; --k) {
+                    const long long a0 = 16LL * ro[(size_t)k], a1 = a0 + fb[(size_t)k];
+                    const long long b0 = 16LL * ro[(size_t)j], b1 = b0 + F;
+                    if (a0 < b1 && b0 < a1) {
+                        at = std::max(at, k + 1);
+                        break;
+                    }
+                    scanned += fb[(size_t)k];
+                }
+                at = std::max(at, 0);
+                if (at > std::max(0, j - LC_D)) ok = false;
+                is[(size_t)j] = at;
+            }
+        }
+        if (!ok) continue;
+        // records
+        B.lc_ok = 1;
+        B.lc_nseg = nseg;
+        B.lc_seg_off = (long long)P.lc_segs.size() / 3;
+        std::vector<int> order((size_t)nseg);
+        for (int q = 0; q < nseg; ++q) order[(size_t)q] = q;
+        auto work = [&](int q) {
+            long long e = 0;
+            for (const Ch &c : chunks[(size_t)q]) e += c.no + c.nrec;
+            return (long long)chunks[(size_t)q].size() * 4096 + e;
+        };
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+        std::vector<int> colo, colr, dest, rpo, rpr;
+        std::vector<double> valo, valr, inv;
+        for (int q : order) {
+            const int *sq = seq.data() + scount[(size_t)q];
+            const auto &ch = chunks[(size_t)q];
+            const int nch = (int)ch.size();
+            P.lc_segs.insert(P.lc_segs.end(), {(int)(P.lc_tab.size() / 6), nch, nch ? roff[(size_t)q][0] : 0});
+            for (int j = 0; j < nch; ++j) {
+                const Ch &c = ch[(size_t)j];
+                const int vlim = j >= LC_D ? ch[(size_t)(j - LC_D)].v0 : 0;
+                dest.clear(); rpo.assign(1, 0); rpr.assign(1, 0); inv.clear();
+                colo.clear(); valo.clear(); colr.clear(); valr.clear();
+                for (int t = 0; t < c.nr; ++t) {
+                    const int r = sq[c.v0 + t];
+                    dest.push_back(r);
+                    inv.push_back(P.inv_diag[(size_t)B.r0 + r]);
+                    for (int k = rp[r]; k < rp[r + 1]; ++k) {
+                        const int d = cl[k], vd = vpos[(size_t)d];
+                        if (vd < vlim) {
+                            colo.push_back(d);
+                            valo.push_back(vl[k]);
+                        } else {
+                            colr.push_back(vd & (LC_XW - 1));
+                            valr.push_back(vl[k]);
+                        }
+                    }
+                    rpo.push_back((int)colo.size());
+                    rpr.push_back((int)colr.size());
+                }
+                const int rnext = j + 1 < nch ? roff[(size_t)q][(size_t)j + 1] : 0;
+                auto emit = [&](std::vector<uint32_t> &pool, int es) -> std::pair<int, int> {
+                    const size_t base = pool.size();
+                    const long long bytes = lc_static_bytes(c.nr, c.no, c.nrec, es);
+                    pool.resize(base + (size_t)(bytes / 4), 0u);
+                    uint32_t *w = pool.data() + base;
+                    const int hdr[LC_HDR_INTS] = {c.nr, c.no, c.nrec, c.v0, rnext, 0, 0, 0};
+                    std::memcpy(w, hdr, sizeof(hdr));
+                    size_t o = LC_HDR_INTS;
+                    auto put_i = [&](const std::vector<int> &v) {
+                        std::memcpy(w + o, v.data(), v.size() * 4);
+                        o += (size_t)lc_pad4((int)v.size());
+                    };
+                    auto put_v = [&](const std::vector<double> &v) {
+                        if (es == 8) std::memcpy(w + o, v.data(), v.size() * 8);
+                        else
+                            for (size_t t = 0; t < v.size(); ++t) {
+                                const float f = (float)v[t];
+                                std::memcpy(w + o + t, &f, 4);
+                            }
+                        o += (size_t)(lc_padv((int)v.size(), es) / 4);
+                    };
+                    put_i(dest);
+                    put_i(rpo);
+                    put_i(rpr);
+                    put_v(inv);
+                    put_i(colo);
+                    put_v(valo);
+                    put_i(colr);
+                    put_v(valr);
+                    return {(int)(base / 4), (int)(bytes / 16)};
+                };
+                const auto r64 = emit(P.lc_rec64, 8);
+                const auto r32 = emit(P.lc_rec32, 4);
+                P.lc_tab.insert(P.lc_tab.end(), {r64.first, r64.second, r32.first, r32.second,
+                                                 roff[(size_t)q][(size_t)j], iss[(size_t)q][(size_t)j]});
+            }
+        }
+    }
+}
+
 int auto_lv(int m, int device_id) {
     // main.cu:245-254: smallest li >= 1 with m / 2^(li+1) below the wave size
     int li;
@@ -166,8 +376,11 @@ int auto_lv(int m, int device_id) {
 }
 
 int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int n, int nnz, int fmt,
-                 int substitution, int lv, const rbs_options &opt, std::string &err) {
+                 int substitution, int lv, const rbs_options &opt, std::string &err,
+                 const std::vector<int> *seg_rows) {
     auto t0 = std::chrono::steady_clock::now();
+    P.seg_rows.clear();
+    if (seg_rows) P.seg_rows = *seg_rows;
     if (n <= 0 || nnz < n || !ptr || !idx || !val) {
         err = "rbs_analyse: need n > 0, nnz >= n and non-null arrays";
         return RBS_ERR_ARG;
@@ -315,6 +528,9 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
         B.ell_chunk_off = B.ell_lo = B.ell_hi = -1;
         B.ca_ok = B.ca_w = 0;
         B.ca_tab_off = B.ca_lo = B.ca_hi = -1;
+        B.lc_ok = B.lc_nseg = 0;
+        B.lc_seg_off = -1;
+        B.lvl_var = LVL_PLAIN;
         if (B.tri) {
             int i = b / 2;
             B.r0 = i * s;
@@ -641,6 +857,13 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
         err = "rbs_analyse: ELL pool too large";
         return RBS_ERR_NOMEM;
     }
+    // 11. level-chunk records (level_lc.cuh) and the level kernel of every
+    //     level triangle
+    build_lc(P, opt, level);
+    for (ExecBlock &B : P.blocks) {
+        if (!B.tri || B.kernel != RBS_K_LEVEL) continue;
+        B.lvl_var = B.lc_ok ? LVL_LC : B.ca_ok ? LVL_CA : B.ell_ok ? LVL_CSF : LVL_PLAIN;
+    }
     auto t1 = std::chrono::steady_clock::now();
     P.analyse_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     return RBS_OK;
@@ -733,6 +956,29 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
                 iv[2 * b] = (int)P.blocks[b].ell_chunk_off;
                 iv[2 * b + 1] = P.blocks[b].ell_nchunks;
             }
+        return RBS_OK;
+    }
+    if (name == "lc_consts") {  // the layout constants the records were built for
+        iv = {LC_XW, LC_NB, LC_D, LC_RMAX, LC_T, LC_RING, LC_FMAX, LC_HDR_INTS};
+        return RBS_OK;
+    }
+    if (name == "lc_tab") return put(P.lc_tab);
+    if (name == "lc_segs") return put(P.lc_segs);
+    if (name == "lc_rec64" || name == "lc_rec32") {  // 16-byte-aligned words, returned as int32
+        const auto &w = name == "lc_rec64" ? P.lc_rec64 : P.lc_rec32;
+        iv.resize(w.size());
+        if (!w.empty()) std::memcpy(iv.data(), w.data(), w.size() * 4);
+        return RBS_OK;
+    }
+    if (name == "lc_block") {  // per block: first segment, segments (-1 if none), level kernel variant
+        iv.assign(3 * sum, -1);
+        for (int b = 0; b < sum; ++b) {
+            if (P.blocks[b].lc_ok) {
+                iv[3 * b] = (int)P.blocks[b].lc_seg_off;
+                iv[3 * b + 1] = P.blocks[b].lc_nseg;
+            }
+            iv[3 * b + 2] = P.blocks[b].lvl_var;
+        }
         return RBS_OK;
     }
     if (name == "block_rows") {  // per block: processing-order first row, rows

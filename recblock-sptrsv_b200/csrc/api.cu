@@ -48,8 +48,12 @@ void rbs_options_default(rbs_options *opt) {
 
 int rbs_auto_lv(int m, int device_id) { return rbs::auto_lv(m, device_id); }
 
-int rbs_analyse(const int *ptr, const int *idx, const double *val, int n, int nnz, int fmt, int substitution, int lv,
-                const rbs_options *opt, rbs_plan **plan) {
+}  // extern "C"
+
+// rbs_analyse, optionally with the original-row offsets of independent
+// systems (a batch), which the level-chunk layout solves one CTA each.
+static int analyse_impl(const int *ptr, const int *idx, const double *val, int n, int nnz, int fmt, int substitution,
+                        int lv, const rbs_options *opt, rbs_plan **plan, const std::vector<int> *segs) {
     if (!plan) return fail(RBS_ERR_ARG, "rbs_analyse: plan is NULL");
     *plan = nullptr;
     rbs_options o;
@@ -66,7 +70,7 @@ int rbs_analyse(const int *ptr, const int *idx, const double *val, int n, int nn
     std::string err;
     int rc;
     try {
-        rc = rbs::analyse_host(P->p, ptr, idx, val, n, nnz, fmt, substitution, lv, o, err);
+        rc = rbs::analyse_host(P->p, ptr, idx, val, n, nnz, fmt, substitution, lv, o, err, segs);
         if (rc == RBS_OK && !o.host_only) rc = rbs::device_build(P->p, err);
         if (rc == RBS_OK && !o.host_only && o.select == RBS_SELECT_TUNE) rc = rbs::device_tune(P->p, err);
     } catch (const std::bad_alloc &) {
@@ -81,6 +85,13 @@ int rbs_analyse(const int *ptr, const int *idx, const double *val, int n, int nn
     *plan = P;
     set_error("");
     return RBS_OK;
+}
+
+extern "C" {
+
+int rbs_analyse(const int *ptr, const int *idx, const double *val, int n, int nnz, int fmt, int substitution, int lv,
+                const rbs_options *opt, rbs_plan **plan) {
+    return analyse_impl(ptr, idx, val, n, nnz, fmt, substitution, lv, opt, plan, nullptr);
 }
 
 int rbs_analyse_device(const int *d_ptr, const int *d_idx, const double *d_val, int n, int nnz, int fmt,
@@ -128,8 +139,9 @@ int rbs_batch_analyse(int count, const int *const *ptr, const int *const *idx, c
         row_offsets[i + 1] = (int)r0;
     }
     bp[(size_t)N] = (int)Z;
-    return rbs_analyse(bp.data(), bi.data(), bv.data(), (int)N, (int)Z, fmt, substitution, lv < 0 ? 0 : lv, opt,
-                       plan);
+    const std::vector<int> segs(row_offsets, row_offsets + count);
+    return analyse_impl(bp.data(), bi.data(), bv.data(), (int)N, (int)Z, fmt, substitution, lv < 0 ? 0 : lv, opt, plan,
+                        &segs);
 }
 
 static int check_solve_args(rbs_plan *plan, const double *b, const double *x, int k, int ld, int prec) {

@@ -1,0 +1,43 @@
+// lc_layout.h -- constants and record sizes of the level-chunk layout
+// shared by the host analysis (which builds the records) and the kernel
+// (level_lc.cuh, which reads them).
+#pragma once
+
+#ifdef __CUDACC__
+#define LC_HD __host__ __device__
+#else
+#define LC_HD
+#endif
+
+namespace rbs {
+
+constexpr int LC_XW = 4096;  // window rows
+constexpr int LC_NB = 32;    // mbarrier slots (chunks in flight at most)
+constexpr int LC_D = 2;      // gather distance in chunks
+constexpr int LC_RMAX = 1024;
+constexpr int LC_T = 512;    // threads of the CTA
+constexpr int LC_SMEM = 232448 - 1024;  // dynamic shared memory (227 KB less room for the static part)
+constexpr int LC_RING = ((LC_SMEM - LC_XW * 8 - LC_NB * 8) / 16) * 16;
+constexpr int LC_FMAX = ((LC_RING / (LC_D + 2)) / 16) * 16;
+constexpr int LC_HDR_INTS = 8;
+
+struct LcChunk {  // 16-byte units unless noted
+    int src64, bytes64;  // static record, FP64 layout
+    int src32, bytes32;  // static record, FP32 layout
+    int ring;            // ring offset
+    int issue;           // chunk iteration at whose start the copy is issued
+};
+
+LC_HD constexpr int lc_pad4(int n) { return (n + 3) & ~3; }  // ints up to a 16-byte multiple
+LC_HD constexpr long long lc_padv(int n, int es) { return (long long)((n * es + 15) / 16) * 16; }  // bytes
+
+// bytes of the copied part of a chunk record and of its ring footprint
+LC_HD constexpr long long lc_static_bytes(int nr, int no, int nrec, int es) {
+    return 4LL * LC_HDR_INTS + 4LL * lc_pad4(nr) + 8LL * lc_pad4(nr + 1) + lc_padv(nr, es) + 4LL * lc_pad4(no) +
+           lc_padv(no, es) + 4LL * lc_pad4(nrec) + lc_padv(nrec, es);
+}
+LC_HD constexpr long long lc_foot_bytes(int nr, int no, int nrec, int es) {
+    return lc_static_bytes(nr, no, nrec, es) + lc_padv(no, es) + lc_padv(nr, es);
+}
+
+}  // namespace rbs

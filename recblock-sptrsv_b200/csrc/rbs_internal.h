@@ -64,7 +64,15 @@ struct ExecBlock {
     int ell_ok, ell_nchunks;
     long long ell_chunk_off;  // first chunk in ell_chunks (4 ints per chunk: R0, R1, W, pool offset)
     long long ell_lo, ell_hi; // element range of the block in the ELL pools
+    // single-CTA triangles in level chunks (bulk-copied records, level_lc.cuh)
+    int lc_ok, lc_nseg;
+    long long lc_seg_off;     // first segment in lc_segs (3 ints per segment)
+    // which single-CTA level kernel runs a RBS_K_LEVEL triangle
+    int lvl_var;              // LVL_* below
 };
+
+// single-CTA level kernels of a RBS_K_LEVEL triangle
+enum { LVL_PLAIN = 0, LVL_CA = 1, LVL_CSF = 2, LVL_LC = 3 };
 
 struct DeviceState;  // executor side (solve.cu)
 
@@ -93,6 +101,15 @@ struct Plan {
     std::vector<int> ell_chunks;
     std::vector<int> ca_tab, ca_col;           // level tables and level-ELL columns (-1 = padding)
     std::vector<double> ca_val;
+    // level-chunk records (level_lc.cuh): 16-byte words of the FP64 and FP32
+    // layouts, 6 ints per chunk (src64, bytes64, src32, bytes32, ring, issue;
+    // 16-byte units), 3 ints per segment (first chunk, chunks, ring offset of
+    // the first chunk)
+    std::vector<uint32_t> lc_rec64, lc_rec32;
+    std::vector<int> lc_tab, lc_segs;
+    // original-row offsets of independent systems (batched plans); empty
+    // for a single system
+    std::vector<int> seg_rows;
     // full processing-order CSR (with diagonal) for FP64 residuals
     std::vector<int> full_rp, full_col;
     std::vector<double> full_val;
@@ -102,7 +119,8 @@ struct Plan {
 
 // analysis.cpp
 int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int n, int nnz, int fmt,
-                 int substitution, int lv, const rbs_options &opt, std::string &err);
+                 int substitution, int lv, const rbs_options &opt, std::string &err,
+                 const std::vector<int> *seg_rows = nullptr);
 int export_reference(const Plan &P, const std::string &name, std::vector<int> &iv, std::vector<double> &dv,
                      bool &is_double, std::string &err);
 int auto_lv(int m, int device_id);

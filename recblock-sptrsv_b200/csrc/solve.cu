@@ -15,6 +15,7 @@
 #include "kernels.cuh"
 #include "cta_syncfree.cuh"
 #include "level_ca.cuh"
+#include "level_lc.cuh"
 #include "rbs_internal.h"
 
 namespace rbs {
@@ -42,6 +43,10 @@ struct DeviceState {
     double *ca_val = nullptr;
     float *ca_val32 = nullptr;
     std::map<long long, CaDesc *> ca_cache;
+    uint32_t *lc_rec64 = nullptr, *lc_rec32 = nullptr;  // level-chunk records (16-byte aligned words)
+    LcChunk *lc_tab = nullptr;
+    LcSeg *lc_segs = nullptr;
+    int *lc_queue = nullptr;                              // one segment counter per triangle
     cudaStream_t side = nullptr;                         // L2 prefetch stream
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int *tickets = nullptr, *status = nullptr, *h_status = nullptr;
@@ -184,6 +189,7 @@ template <> struct Pools<double> {
     static const double *binv(const DeviceState &D) { return D.band_inv; }
     static const double *ellv(const DeviceState &D) { return D.ell_val; }
     static const double *cav(const DeviceState &D) { return D.ca_val; }
+    static const unsigned char *lcrec(const DeviceState &D) { return reinterpret_cast<const unsigned char *>(D.lc_rec64); }
     static double *bw(const DeviceState &D) { return D.bw64; }
     static double *xw(const DeviceState &D) { return D.xw64; }
 };
@@ -194,6 +200,7 @@ template <> struct Pools<float> {
     static const float *binv(const DeviceState &D) { return D.band_inv32; }
     static const float *ellv(const DeviceState &D) { return D.ell_val32; }
     static const float *cav(const DeviceState &D) { return D.ca_val32; }
+    static const unsigned char *lcrec(const DeviceState &D) { return reinterpret_cast<const unsigned char *>(D.lc_rec32); }
     static float *bw(const DeviceState &D) { return D.bw32; }
     static float *xw(const DeviceState &D) { return D.xw32; }
 };
@@ -316,6 +323,20 @@ int ca_descs(Plan &P, CaDesc *&out, std::string &err) {
     return RBS_OK;
 }
 
+template <typename VT>
+constexpr int lc_smem() {
+    return LC_RING + LC_XW * (int)sizeof(VT) + LC_NB * 8;
+}
+template <typename VT>
+int lc_attr(std::string &err) {
+    static bool done = false;
+    if (!done) {
+        CK(cudaFuncSetAttribute(k_tri_lc<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lc_smem<VT>()));
+        done = true;
+    }
+    return RBS_OK;
+}
+
 // Prefetch [p, p+bytes) into L2 with bulk prefetches of 16 KB.
 __global__ void k_prefetch_l2(const char *p, long long bytes) {
     const long long piece = 16384;
@@ -390,6 +411,10 @@ int launch_blocks(Plan &P, std::string &err) {
     if (K == 1 && (rc = ca_descs<VT>(P, cdescs, err))) return rc;
     if (K == 1 && (rc = ell_descs<VT>(P, edescs, err))) return rc;
     if (D.ntri) CK(cudaMemsetAsync(D.tickets, 0, sizeof(int) * D.ntri, st));
+    if (K == 1 && D.lc_queue) {
+        CK(cudaMemsetAsync(D.lc_queue, 0, sizeof(int) * D.ntri, st));
+        if ((rc = lc_attr<VT>(err))) return rc;
+    }
     const long long limit = P.opt.spin_limit;
     // The staged level kernel runs on one SM; the others pull the data of
     // the staged triangles into L2 meanwhile (up to 96 MB, in block order).
@@ -397,13 +422,26 @@ int launch_blocks(Plan &P, std::string &err) {
     if (K == 1 && D.side) {
         long long budget = 96ll << 20;
         for (const ExecBlock &B : P.blocks) {
-            if (!B.tri || B.kernel != RBS_K_LEVEL || !(B.ell_ok || B.ca_ok) || budget <= 0) continue;
+            if (!B.tri || B.kernel != RBS_K_LEVEL || B.lvl_var == LVL_PLAIN || budget <= 0) continue;
             if (!forked) {
                 CK(cudaEventRecord(D.ev_fork, st));
                 CK(cudaStreamWaitEvent(D.side, D.ev_fork, 0));
                 forked = true;
             }
-            if (B.ca_ok) {
+            if (B.lvl_var == LVL_LC && B.lc_ok) {
+                const int *sg = P.lc_segs.data() + 3 * B.lc_seg_off;
+                const int c0 = sg[0], c1 = P.lc_segs[(size_t)(3 * (B.lc_seg_off + B.lc_nseg - 1))] +
+                                           P.lc_segs[(size_t)(3 * (B.lc_seg_off + B.lc_nseg - 1) + 1)];
+                if (c1 > c0) {
+                    const bool f64 = sizeof(VT) == 8;
+                    const int *t0 = P.lc_tab.data() + 6 * (size_t)c0, *t1 = P.lc_tab.data() + 6 * (size_t)(c1 - 1);
+                    const long long a = 16LL * (f64 ? t0[0] : t0[2]), e = 16LL * ((f64 ? t1[0] : t1[2]) + (f64 ? t1[1] : t1[3]));
+                    prefetch_range(D.side, Pools<VT>::lcrec(D) + a, e - a);
+                    budget -= e - a;
+                }
+                continue;
+            }
+            if (B.ca_ok && B.lvl_var == LVL_CA) {
                 const long long ne = B.ca_hi - B.ca_lo;
                 prefetch_range(D.side, Pools<VT>::cav(D) + B.ca_lo, ne * (long long)sizeof(VT));
                 prefetch_range(D.side, D.ca_col + B.ca_lo, ne * 4);
@@ -411,7 +449,7 @@ int launch_blocks(Plan &P, std::string &err) {
                 budget -= ne * ((long long)sizeof(VT) + 4) + (long long)B.m * sizeof(VT);
                 continue;
             }
-            if (B.ell_ok) {
+            if (B.ell_ok && B.lvl_var == LVL_CSF) {
                 const long long ne = B.ell_hi - B.ell_lo;
                 prefetch_range(D.side, Pools<VT>::ellv(D) + B.ell_lo, ne * (long long)sizeof(VT));
                 prefetch_range(D.side, D.ell_col + B.ell_lo, ne * 4);
@@ -437,14 +475,19 @@ int launch_blocks(Plan &P, std::string &err) {
                                                                                                B.m);
                 break;
             case RBS_K_LEVEL:
-                if (K == 1 && B.ca_ok) {
+                if (K == 1 && B.lvl_var == LVL_LC && B.lc_ok) {
+                    const int grid = std::min(B.lc_nseg, D.num_sms);
+                    k_tri_lc<VT><<<grid, LC_T, lc_smem<VT>(), st>>>(D.lc_segs + B.lc_seg_off, B.lc_nseg,
+                                                                   Pools<VT>::lcrec(D), sizeof(VT) == 4 ? 1 : 0, bb,
+                                                                   xx, D.lc_queue + ti, D.status, limit);
+                } else if (K == 1 && B.lvl_var == LVL_CA && B.ca_ok) {
                     if (B.ca_w == 1)
                         k_tri_level_ca<VT, 1, 4><<<1, 1024, CaLayout<VT, 1, 4>::total, st>>>(cdescs + cti);
                     else if (B.ca_w == 2)
                         k_tri_level_ca<VT, 2, 4><<<1, 1024, CaLayout<VT, 2, 4>::total, st>>>(cdescs + cti);
                     else
                         k_tri_level_ca<VT, 4, 2><<<1, 1024, CaLayout<VT, 4, 2>::total, st>>>(cdescs + cti);
-                } else if (K == 1 && B.ell_ok) {
+                } else if (K == 1 && B.lvl_var == LVL_CSF && B.ell_ok) {
                     k_tri_cta_syncfree<VT><<<1, 1024, CsfLayout<VT>::total, st>>>(edescs + eti, D.status, limit);
                 } else {
                     k_tri_level<VT, K><<<1, 1024, 0, st>>>(descs + li);
@@ -703,6 +746,18 @@ int device_build(Plan &P, std::string &err) {
         std::vector<float> e32(P.ell_val.begin(), P.ell_val.end());
         if ((rc = upload(D, D.ell_val32, e32, err))) return rc;
     }
+    if (!P.lc_tab.empty()) {
+        std::vector<LcChunk> tab(P.lc_tab.size() / 6);
+        std::memcpy(tab.data(), P.lc_tab.data(), tab.size() * sizeof(LcChunk));
+        if ((rc = upload(D, D.lc_tab, tab, err))) return rc;
+        if ((rc = upload(D, D.lc_rec64, P.lc_rec64, err))) return rc;
+        if (D.mixed && (rc = upload(D, D.lc_rec32, P.lc_rec32, err))) return rc;
+        std::vector<LcSeg> segs(P.lc_segs.size() / 3);
+        for (size_t q = 0; q < segs.size(); ++q)
+            segs[q] = LcSeg{D.lc_tab + P.lc_segs[3 * q], P.lc_segs[3 * q + 1], P.lc_segs[3 * q + 2]};
+        if ((rc = upload(D, D.lc_segs, segs, err))) return rc;
+        if ((rc = alloc(D, D.lc_queue, (size_t)(1 << P.lv), err))) return rc;
+    }
     CK(cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&D.ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&D.ev_join, cudaEventDisableTiming));
@@ -774,30 +829,40 @@ void drop_descs(DeviceState &D) {
 }
 
 // RBS_SELECT_TUNE: run the plan with every triangle on one candidate kernel
-// family at a time (sync-free, single-CTA level, band scan where a band
-// layout exists), time each triangle with CUDA events, and keep for every
-// triangle the fastest.  Squares keep their SpMV plan.
+// at a time (sync-free; the single-CTA level kernels: level chunks, staged
+// level-ELL, CTA sync-free, plain; band scan where a band layout exists),
+// time each triangle with CUDA events, and keep for every triangle the
+// fastest.  Squares keep their SpMV plan.
 int tune_kernels(Plan &P, std::string &err) {
     DeviceState &D = *P.dev;
     const size_t nb = P.blocks.size();
-    std::vector<int> orig(nb);
-    for (size_t b = 0; b < nb; ++b) orig[b] = P.blocks[b].kernel;
+    std::vector<int> orig(nb), origv(nb);
+    for (size_t b = 0; b < nb; ++b) {
+        orig[b] = P.blocks[b].kernel;
+        origv[b] = P.blocks[b].lvl_var;
+    }
     std::vector<double> best(nb, 1e300);
-    std::vector<int> pick(orig);
+    std::vector<int> pick(orig), pickv(origv);
     double *db = nullptr, *dx = nullptr;
     CK(cudaMalloc(&db, sizeof(double) * (size_t)P.n));
     CK(cudaMalloc(&dx, sizeof(double) * (size_t)P.n));
     k_fill<double><<<grid_for(P.n, 256, D.num_sms), 256, 0, D.stream>>>(db, P.n, 1.0);
     int rc = RBS_OK;
-    const int cands[3] = {RBS_K_SYNCFREE, RBS_K_LEVEL, RBS_K_BANDSCAN};
-    for (int ci = 0; ci < 3 && rc == RBS_OK; ++ci) {
-        const int cand = cands[ci];
+    // (kernel, single-CTA level variant) candidates
+    const int cands[6][2] = {{RBS_K_SYNCFREE, LVL_PLAIN}, {RBS_K_LEVEL, LVL_LC},  {RBS_K_LEVEL, LVL_CA},
+                             {RBS_K_LEVEL, LVL_CSF},      {RBS_K_LEVEL, LVL_PLAIN}, {RBS_K_BANDSCAN, LVL_PLAIN}};
+    for (int ci = 0; ci < 6 && rc == RBS_OK; ++ci) {
+        const int cand = cands[ci][0], var = cands[ci][1];
         bool any = false;
         for (size_t b = 0; b < nb; ++b) {
             ExecBlock &B = P.blocks[b];
             if (!B.tri || B.nnz == B.m) continue;
-            const bool ok = cand != RBS_K_BANDSCAN || B.band_w > 0;
+            bool ok = true;
+            if (cand == RBS_K_BANDSCAN) ok = B.band_w > 0;
+            if (cand == RBS_K_LEVEL)
+                ok = var == LVL_LC ? B.lc_ok : var == LVL_CA ? B.ca_ok : var == LVL_CSF ? B.ell_ok : B.lvl_off >= 0;
             B.kernel = ok ? cand : orig[b];
+            B.lvl_var = ok ? var : origv[b];
             any = any || ok;
         }
         if (!any) continue;
@@ -813,15 +878,19 @@ int tune_kernels(Plan &P, std::string &err) {
         device_block_times(P, ms, solves);
         for (size_t b = 0; b < nb; ++b) {
             const ExecBlock &B = P.blocks[b];
-            if (!B.tri || B.nnz == B.m || B.kernel != cand) continue;
+            if (!B.tri || B.nnz == B.m || B.kernel != cand || B.lvl_var != var) continue;
             const double t = ms[b] / std::max(1ll, solves);
             if (t < best[b]) {
                 best[b] = t;
                 pick[b] = cand;
+                pickv[b] = var;
             }
         }
     }
-    for (size_t b = 0; b < nb; ++b) P.blocks[b].kernel = rc == RBS_OK ? pick[b] : orig[b];
+    for (size_t b = 0; b < nb; ++b) {
+        P.blocks[b].kernel = rc == RBS_OK ? pick[b] : orig[b];
+        P.blocks[b].lvl_var = rc == RBS_OK ? pickv[b] : origv[b];
+    }
     drop_descs(D);
     device_profile(P, 0, err);
     cudaFree(db);
@@ -858,6 +927,11 @@ void device_free(Plan &P) {
     cudaFree(D.ca_col);
     cudaFree(D.ca_val);
     cudaFree(D.ca_val32);
+    cudaFree(D.lc_rec64);
+    cudaFree(D.lc_rec32);
+    cudaFree(D.lc_tab);
+    cudaFree(D.lc_segs);
+    cudaFree(D.lc_queue);
     cudaFree(D.stage_b);
     cudaFree(D.stage_x);
     void *ptrs[] = {D.rp, D.col, D.lvl, D.map, D.rows, D.perm, D.val, D.inv, D.val32, D.inv32,
