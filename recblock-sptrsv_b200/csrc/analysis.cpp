@@ -160,13 +160,16 @@ static bool wants_band(const ExecBlock &b, const rbs_options &opt) {
 
 // Level-chunk layout of every level triangle (level_lc.cuh).  Rows of each
 // independent segment (the whole triangle, or the rows of one system of a
-// batch) are listed level by level; a chunk takes consecutive rows of one
+// batch) are taken level by level; a chunk takes consecutive rows of one
 // level while it stays within LC_RMAX rows and LC_FMAX bytes of ring
-// footprint.  Entries whose dependency lies LC_D or more chunks back are
-// "old" (gathered ahead), the others "recent" (window).  Records are placed
-// in the kernel's shared-memory ring in order, wrapping to 0 when the next
-// one does not fit; a record's copy is issued once every chunk whose ring
-// bytes it reuses has been solved and its mbarrier slot is free.
+// footprint.  Within a chunk rows are ordered by their count of recent
+// entries (largest first, ties in level order), which fixes their virtual
+// row numbers.  An entry is "recent" when its dependency is still in the
+// window of the last LC_XW virtual rows after the chunk is solved, "old"
+// otherwise (gathered ahead).  Records are placed in the kernel's
+// shared-memory ring in order, wrapping to 0 when the next one does not
+// fit; a record's copy is issued once every chunk whose ring bytes it reuses
+// has been solved and its mbarrier slot is free.
 static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &level) {
     P.lc_rec64.clear();
     P.lc_rec32.clear();
@@ -206,42 +209,77 @@ static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &le
         std::vector<int> scount((size_t)nseg + 1, 0);
         for (int r = 0; r < m; ++r) scount[(size_t)seg[(size_t)r] + 1]++;
         for (int q = 0; q < nseg; ++q) scount[(size_t)q + 1] += scount[(size_t)q];
-        std::vector<int> seq((size_t)m), vpos((size_t)m);
+        std::vector<int> seq((size_t)m);
         {
             std::vector<int> fill(scount.begin(), scount.end() - 1);
             for (int t = 0; t < m; ++t) {
-                const int r = bylev[(size_t)t], q = seg[(size_t)r];
-                vpos[(size_t)r] = fill[(size_t)q] - scount[(size_t)q];
-                seq[(size_t)fill[(size_t)q]++] = r;
+                const int r = bylev[(size_t)t];
+                seq[(size_t)fill[(size_t)seg[(size_t)r]]++] = r;
             }
         }
-        struct Ch { int v0, nr, no, nrec; };
+        // chunks; seq is reordered inside every chunk and vpos assigned
+        struct Ch { int v0, nr, no, nrec, ncols, maxlen; };
         std::vector<std::vector<Ch>> chunks((size_t)nseg);
+        std::vector<int> vpos((size_t)m, -1), rl((size_t)LC_RMAX);
+        auto counts = [&](const int *rows, int nr, int thr, int &no, int &nrec, int &ncols) {
+            no = nrec = ncols = 0;
+            for (int t = 0; t < nr; ++t) {
+                const int r = rows[t];
+                int rr = 0;
+                for (int k = rp[r]; k < rp[r + 1]; ++k) rr += vpos[(size_t)cl[k]] >= thr;
+                rl[(size_t)t] = rr;
+                nrec += rr;
+                no += rp[r + 1] - rp[r] - rr;
+                ncols = std::max(ncols, rr);
+            }
+        };
         bool ok = true;
         for (int q = 0; q < nseg && ok; ++q) {
-            const int *sq = seq.data() + scount[(size_t)q];
+            int *sq = seq.data() + scount[(size_t)q];
             const int len = scount[(size_t)q + 1] - scount[(size_t)q];
             auto &ch = chunks[(size_t)q];
             int i = 0;
             while (i < len) {
                 const int L = level[(size_t)B.r0 + sq[i]];
-                const int j = (int)ch.size();
-                const int vlim = j >= LC_D ? ch[(size_t)(j - LC_D)].v0 : 0;
-                int nr = 0, no = 0, nrec = 0;
+                const int thr_c = i + LC_RMAX - LC_XW;  // no later threshold is larger
+                int nr = 0, no = 0, nrec = 0, ncols = 0;
                 while (i + nr < len && nr < LC_RMAX && level[(size_t)B.r0 + sq[i + nr]] == L) {
                     const int r = sq[i + nr];
                     int ro = 0, rr = 0;
-                    for (int k = rp[r]; k < rp[r + 1]; ++k) (vpos[(size_t)cl[k]] < vlim ? ro : rr)++;
-                    if (lc_foot_bytes(nr + 1, no + ro, nrec + rr, 8) > LC_FMAX) break;
+                    for (int k = rp[r]; k < rp[r + 1]; ++k) (vpos[(size_t)cl[k]] < thr_c ? ro : rr)++;
+                    if (lc_foot_bytes(nr + 1, no + ro, nrec + rr, std::max(ncols, rr), 8) > LC_FMAX) break;
                     ++nr;
                     no += ro;
                     nrec += rr;
+                    ncols = std::max(ncols, rr);
                 }
                 if (nr == 0) {  // one row alone does not fit the ring
                     ok = false;
                     break;
                 }
-                ch.push_back({i, nr, no, nrec});
+                // exact split with this chunk's own threshold
+                for (;;) {
+                    counts(sq + i, nr, i + nr - LC_XW, no, nrec, ncols);
+                    if (lc_foot_bytes(nr, no, nrec, ncols, 8) <= LC_FMAX || nr == 1) break;
+                    --nr;
+                }
+                if (lc_foot_bytes(nr, no, nrec, ncols, 8) > LC_FMAX) {
+                    ok = false;
+                    break;
+                }
+                // rows by recent count, largest first (stable)
+                std::vector<int> idx((size_t)nr);
+                for (int t = 0; t < nr; ++t) idx[(size_t)t] = t;
+                std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return rl[(size_t)a] > rl[(size_t)b]; });
+                std::vector<int> rows((size_t)nr);
+                for (int t = 0; t < nr; ++t) rows[(size_t)t] = sq[i + idx[(size_t)t]];
+                for (int t = 0; t < nr; ++t) {
+                    sq[i + t] = rows[(size_t)t];
+                    vpos[(size_t)rows[(size_t)t]] = i + t;
+                }
+                int maxlen = 0;
+                for (int t = 0; t < nr; ++t) maxlen = std::max(maxlen, rp[rows[(size_t)t] + 1] - rp[rows[(size_t)t]]);
+                ch.push_back({i, nr, no, nrec, ncols, maxlen});
                 i += nr;
             }
         }
@@ -258,7 +296,8 @@ static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &le
             long long head = 0;
             std::vector<long long> fb((size_t)nch);
             for (int j = 0; j < nch; ++j) {
-                const long long F = lc_foot_bytes(ch[(size_t)j].nr, ch[(size_t)j].no, ch[(size_t)j].nrec, 8);
+                const Ch &c = ch[(size_t)j];
+                const long long F = lc_foot_bytes(c.nr, c.no, c.nrec, c.ncols, 8);
                 fb[(size_t)j] = F;
                 if (head + F > LC_RING) head = 0;
                 ro[(size_t)j] = (int)(head / 16);
@@ -279,7 +318,6 @@ static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &le
                     }
                     scanned += fb[(size_t)k];
                 }
-                at = std::max(at, 0);
                 if (at > std::max(0, j - LC_D)) ok = false;
                 is[(size_t)j] = at;
             }
@@ -297,8 +335,8 @@ static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &le
             return (long long)chunks[(size_t)q].size() * 4096 + e;
         };
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
-        std::vector<int> colo, colr, dest, rpo, rpr;
-        std::vector<double> valo, valr, inv;
+        std::vector<int> dest, rlen, rpo, cs, colr, colo;
+        std::vector<double> inv, valr, valo;
         for (int q : order) {
             const int *sq = seq.data() + scount[(size_t)q];
             const auto &ch = chunks[(size_t)q];
@@ -306,56 +344,78 @@ static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &le
             P.lc_segs.insert(P.lc_segs.end(), {(int)(P.lc_tab.size() / 6), nch, nch ? roff[(size_t)q][0] : 0});
             for (int j = 0; j < nch; ++j) {
                 const Ch &c = ch[(size_t)j];
-                const int vlim = j >= LC_D ? ch[(size_t)(j - LC_D)].v0 : 0;
-                dest.clear(); rpo.assign(1, 0); rpr.assign(1, 0); inv.clear();
-                colo.clear(); valo.clear(); colr.clear(); valr.clear();
+                const int thr = c.v0 + c.nr - LC_XW;
+                dest.assign((size_t)c.nr, 0);
+                rlen.assign((size_t)c.nr, 0);
+                rpo.assign(1, 0);
+                inv.assign((size_t)c.nr, 0.0);
+                colo.clear();
+                valo.clear();
                 for (int t = 0; t < c.nr; ++t) {
                     const int r = sq[c.v0 + t];
-                    dest.push_back(r);
-                    inv.push_back(P.inv_diag[(size_t)B.r0 + r]);
+                    dest[(size_t)t] = r;
+                    inv[(size_t)t] = P.inv_diag[(size_t)B.r0 + r];
                     for (int k = rp[r]; k < rp[r + 1]; ++k) {
-                        const int d = cl[k], vd = vpos[(size_t)d];
-                        if (vd < vlim) {
-                            colo.push_back(d);
+                        if (vpos[(size_t)cl[k]] >= thr) rlen[(size_t)t]++;
+                        else {
+                            colo.push_back(cl[k]);
                             valo.push_back(vl[k]);
-                        } else {
-                            colr.push_back(vd & (LC_XW - 1));
-                            valr.push_back(vl[k]);
                         }
                     }
                     rpo.push_back((int)colo.size());
-                    rpr.push_back((int)colr.size());
+                }
+                cs.assign((size_t)c.ncols + 1, 0);
+                for (int k = 0; k < c.ncols; ++k) {
+                    int cnt = 0;
+                    while (cnt < c.nr && rlen[(size_t)cnt] > k) ++cnt;  // rlen is non-increasing
+                    cs[(size_t)k + 1] = cs[(size_t)k] + cnt;
+                }
+                colr.assign((size_t)c.nrec, 0);
+                valr.assign((size_t)c.nrec, 0.0);
+                for (int t = 0; t < c.nr; ++t) {
+                    const int r = sq[c.v0 + t];
+                    int kk = 0;
+                    for (int k = rp[r]; k < rp[r + 1]; ++k) {
+                        const int vd = vpos[(size_t)cl[k]];
+                        if (vd < thr) continue;
+                        colr[(size_t)(cs[(size_t)kk] + t)] = vd & (LC_XW - 1);
+                        valr[(size_t)(cs[(size_t)kk] + t)] = vl[k];
+                        ++kk;
+                    }
                 }
                 const int rnext = j + 1 < nch ? roff[(size_t)q][(size_t)j + 1] : 0;
                 auto emit = [&](std::vector<uint32_t> &pool, int es) -> std::pair<int, int> {
                     const size_t base = pool.size();
-                    const long long bytes = lc_static_bytes(c.nr, c.no, c.nrec, es);
+                    const long long bytes = lc_static_bytes(c.nr, c.no, c.nrec, c.ncols, es);
                     pool.resize(base + (size_t)(bytes / 4), 0u);
                     uint32_t *w = pool.data() + base;
-                    const int hdr[LC_HDR_INTS] = {c.nr, c.no, c.nrec, c.v0, rnext, 0, 0, 0};
+                    const int hdr[LC_HDR_INTS] = {c.nr, c.no, c.nrec, c.v0, rnext, c.ncols, c.maxlen, 0};
                     std::memcpy(w, hdr, sizeof(hdr));
                     size_t o = LC_HDR_INTS;
                     auto put_i = [&](const std::vector<int> &v) {
-                        std::memcpy(w + o, v.data(), v.size() * 4);
+                        if (!v.empty()) std::memcpy(w + o, v.data(), v.size() * 4);
                         o += (size_t)lc_pad4((int)v.size());
                     };
                     auto put_v = [&](const std::vector<double> &v) {
-                        if (es == 8) std::memcpy(w + o, v.data(), v.size() * 8);
-                        else
+                        if (es == 8) {
+                            if (!v.empty()) std::memcpy(w + o, v.data(), v.size() * 8);
+                        } else {
                             for (size_t t = 0; t < v.size(); ++t) {
                                 const float f = (float)v[t];
                                 std::memcpy(w + o + t, &f, 4);
                             }
+                        }
                         o += (size_t)(lc_padv((int)v.size(), es) / 4);
                     };
                     put_i(dest);
+                    put_i(rlen);
                     put_i(rpo);
-                    put_i(rpr);
+                    put_i(cs);
                     put_v(inv);
-                    put_i(colo);
-                    put_v(valo);
                     put_i(colr);
                     put_v(valr);
+                    put_i(colo);
+                    put_v(valo);
                     return {(int)(base / 4), (int)(bytes / 16)};
                 };
                 const auto r64 = emit(P.lc_rec64, 8);
@@ -862,7 +922,9 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
     build_lc(P, opt, level);
     for (ExecBlock &B : P.blocks) {
         if (!B.tri || B.kernel != RBS_K_LEVEL) continue;
-        B.lvl_var = B.lc_ok ? LVL_LC : B.ca_ok ? LVL_CA : B.ell_ok ? LVL_CSF : LVL_PLAIN;
+        // staged level-ELL first (short rows, narrow levels: its per-level cost
+        // is lowest), then level chunks, then the CTA sync-free and plain kernels
+        B.lvl_var = B.ca_ok ? LVL_CA : B.lc_ok ? LVL_LC : B.ell_ok ? LVL_CSF : LVL_PLAIN;
     }
     auto t1 = std::chrono::steady_clock::now();
     P.analyse_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();

@@ -11,15 +11,16 @@
 
 namespace rbs {
 
-constexpr int LC_XW = 4096;  // window rows
+constexpr int LC_XW = 8192;  // window rows
 constexpr int LC_NB = 32;    // mbarrier slots (chunks in flight at most)
 constexpr int LC_D = 2;      // gather distance in chunks
 constexpr int LC_RMAX = 1024;
 constexpr int LC_T = 512;    // threads of the CTA
 constexpr int LC_SMEM = 232448 - 1024;  // dynamic shared memory (227 KB less room for the static part)
 constexpr int LC_RING = ((LC_SMEM - LC_XW * 8 - LC_NB * 8) / 16) * 16;
-constexpr int LC_FMAX = ((LC_RING / (LC_D + 2)) / 16) * 16;
+constexpr int LC_FMAX = ((LC_RING / 6) / 16) * 16;  // about six chunks in flight
 constexpr int LC_HDR_INTS = 8;
+static_assert(LC_XW >= (LC_D + 1) * LC_RMAX, "old dependencies must be final when gathered");
 
 struct LcChunk {  // 16-byte units unless noted
     int src64, bytes64;  // static record, FP64 layout
@@ -29,15 +30,19 @@ struct LcChunk {  // 16-byte units unless noted
 };
 
 LC_HD constexpr int lc_pad4(int n) { return (n + 3) & ~3; }  // ints up to a 16-byte multiple
-LC_HD constexpr long long lc_padv(int n, int es) { return (long long)((n * es + 15) / 16) * 16; }  // bytes
+LC_HD constexpr long long lc_padv(int n, int es) { return (long long)((n * (long long)es + 15) / 16) * 16; }  // bytes
 
-// bytes of the copied part of a chunk record and of its ring footprint
-LC_HD constexpr long long lc_static_bytes(int nr, int no, int nrec, int es) {
-    return 4LL * LC_HDR_INTS + 4LL * lc_pad4(nr) + 8LL * lc_pad4(nr + 1) + lc_padv(nr, es) + 4LL * lc_pad4(no) +
-           lc_padv(no, es) + 4LL * lc_pad4(nrec) + lc_padv(nrec, es);
+// Record of a chunk of nr rows with no old and nrec recent entries whose
+// recent entries form ncols jagged columns.  Ints: header, dest[nr],
+// rlen[nr], rpo[nr+1], cs[ncols+1]; then inv[nr] (VT), colr[nrec] (int),
+// valr[nrec] (VT), colo[no] (int), valo[no] (VT); the ring also reserves
+// gx[no] and bs[nr] (VT) behind the copied part.
+LC_HD constexpr long long lc_static_bytes(int nr, int no, int nrec, int ncols, int es) {
+    return 4LL * (LC_HDR_INTS + 2 * lc_pad4(nr) + lc_pad4(nr + 1) + lc_pad4(ncols + 1)) + lc_padv(nr, es) +
+           4LL * lc_pad4(nrec) + lc_padv(nrec, es) + 4LL * lc_pad4(no) + lc_padv(no, es);
 }
-LC_HD constexpr long long lc_foot_bytes(int nr, int no, int nrec, int es) {
-    return lc_static_bytes(nr, no, nrec, es) + lc_padv(no, es) + lc_padv(nr, es);
+LC_HD constexpr long long lc_foot_bytes(int nr, int no, int nrec, int ncols, int es) {
+    return lc_static_bytes(nr, no, nrec, ncols, es) + lc_padv(no, es) + lc_padv(nr, es);
 }
 
 }  // namespace rbs

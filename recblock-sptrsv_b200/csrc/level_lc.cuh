@@ -1,37 +1,44 @@
 // level_lc.cuh -- single-CTA level-chunk triangle: bulk-copied (TMA) chunk
-// records, a gather of the long-settled dependencies a few chunks ahead,
-// and a shared-memory window for the recent ones.
+// records, a shared-memory window of the last LC_XW solved rows, and a
+// gather of the few dependencies that lie further back.
 //
 // A triangle (or every independent segment of one, e.g. the systems of a
-// batch) is cut by the host into chunks: consecutive rows of one level, at
-// most LC_RMAX rows, with a footprint of at most LC_FMAX bytes.  Rows of a
-// chunk are independent, so a CTA solves the chunks in order with one CTA
-// barrier between them.  For chunk j the host splits every row's entries
-// into
-//   old    -- dependencies in chunks < j - LC_D, final when chunk j - LC_D
-//             starts; their x values are copied (cp.async) into the chunk's
-//             shared-memory record LC_D chunks ahead, off the critical path;
-//   recent -- dependencies in chunks j - LC_D .. j - 1, read from the
-//             shared-memory window of the last LC_XW rows (slot = virtual row
-//             index mod LC_XW; the host keeps the rows of LC_D + 1
-//             consecutive chunks within LC_XW so no slot is reused early).
-// The static part of a record (row map, row pointers, inverse diagonal,
-// columns, values) is one contiguous 16-byte-aligned piece of global memory
-// copied by one bulk copy into a shared-memory ring; the host places every
-// record in the ring and precomputes the chunk iteration at which its copy
-// may be issued (the ring bytes and mbarrier slot it needs are free by
-// then), always at least LC_D chunks before it is used.
+// batch) is cut by the host into chunks: rows of one level, at most LC_RMAX
+// rows and LC_FMAX bytes of ring footprint.  Rows of a chunk are
+// independent, so a CTA solves the chunks in order with one CTA barrier
+// between them.  Rows are numbered by their position in the segment's chunk
+// sequence ("virtual row"); the window keeps x of virtual row v in slot
+// v mod LC_XW.  For chunk j the host splits every row's entries into
+//   recent -- the dependency is still in the window when chunk j is solved
+//             (virtual row >= end of chunk j - LC_XW): read from the window;
+//   old    -- further back, so final since before chunk j - LC_D started:
+//             its x is copied (cp.async) into the chunk's shared-memory
+//             record LC_D chunks ahead, off the critical path.
+// Recent entries are stored as jagged columns (rows sorted by their recent
+// count, entry k of row t at cs[k] + t), so a warp's loads of one column are
+// consecutive words: no bank conflicts.
+//
+// The copied part of a record is one contiguous 16-byte-aligned piece of
+// global memory moved by one bulk copy into a shared-memory ring; the host
+// places every record in the ring and precomputes the chunk iteration at
+// which its copy may be issued (the ring bytes and mbarrier slot it reuses
+// are free by then), always at least LC_D chunks before it is used.  The
+// last warp (rows are sorted longest first, so its rows are the shortest)
+// issues the copies from a 32-entry window of the chunk table held in its
+// registers (the next window is loaded 32 chunks ahead).
 //
 // Record layout (sections 16-byte aligned, element type VT):
-//   int hdr[8]: nrows, ne_old, ne_rec, vbase, ring offset of the next chunk (16-byte units)
+//   int hdr[8]: nrows, ne_old, ne_rec, vbase, ring offset of the next chunk
+//               (16-byte units), jagged columns, longest row
 //   int dest[nrows]          block row of each chunk row
+//   int rlen[nrows]          recent entries of each row (non-increasing)
 //   int rpo[nrows+1]         old-entry pointer
-//   int rpr[nrows+1]         recent-entry pointer
+//   int cs[ncols+1]          start of each jagged column
 //   VT  inv[nrows]           inverse diagonal
-//   int colo[ne_old]         block row of the dependency
-//   VT  valo[ne_old]
 //   int colr[ne_rec]         window slot of the dependency
 //   VT  valr[ne_rec]
+//   int colo[ne_old]         block row of the dependency
+//   VT  valo[ne_old]
 //   -- end of the copied part; the ring also reserves --
 //   VT  gx[ne_old]           gathered x of the old entries
 //   VT  bs[nrows]            gathered right-hand side
@@ -51,34 +58,36 @@ struct LcSeg {
 
 template <typename VT>
 struct LcView {
-    const int *dest, *rpo, *rpr, *colo, *colr;
-    const VT *inv, *valo, *valr;
+    const int *dest, *rlen, *rpo, *cs, *colr, *colo;
+    const VT *inv, *valr, *valo;
     VT *gx, *bs;
-    __device__ __forceinline__ LcView(unsigned char *rb, int nrows, int ne_old, int ne_rec) {
+    __device__ __forceinline__ LcView(unsigned char *rb, int nrows, int ne_old, int ne_rec, int ncols) {
         constexpr int vq = 16 / sizeof(VT);  // VTs per 16 bytes
         auto padv = [](int n) { return (n + vq - 1) / vq * vq; };
         int *ip = reinterpret_cast<int *>(rb) + LC_HDR_INTS;
         dest = ip;
         ip += lc_pad4(nrows);
+        rlen = ip;
+        ip += lc_pad4(nrows);
         rpo = ip;
         ip += lc_pad4(nrows + 1);
-        rpr = ip;
-        ip += lc_pad4(nrows + 1);
+        cs = ip;
+        ip += lc_pad4(ncols + 1);
         VT *vp = reinterpret_cast<VT *>(ip);
         inv = vp;
         vp += padv(nrows);
-        ip = reinterpret_cast<int *>(vp);
-        colo = ip;
-        ip += lc_pad4(ne_old);
-        vp = reinterpret_cast<VT *>(ip);
-        valo = vp;
-        vp += padv(ne_old);
         ip = reinterpret_cast<int *>(vp);
         colr = ip;
         ip += lc_pad4(ne_rec);
         vp = reinterpret_cast<VT *>(ip);
         valr = vp;
         vp += padv(ne_rec);
+        ip = reinterpret_cast<int *>(vp);
+        colo = ip;
+        ip += lc_pad4(ne_old);
+        vp = reinterpret_cast<VT *>(ip);
+        valo = vp;
+        vp += padv(ne_old);
         gx = vp;
         vp += padv(ne_old);
         bs = vp;
@@ -105,8 +114,8 @@ __global__ void __launch_bounds__(LC_T, 1)
     unsigned char *ring = sm;
     VT *xs = reinterpret_cast<VT *>(sm + LC_RING);
     unsigned long long *mbar = reinterpret_cast<unsigned long long *>(sm + LC_RING + LC_XW * sizeof(VT));
-    __shared__ int s_seg;
-    const int tid = threadIdx.x;
+    __shared__ int s_seg, s_roff[4];
+    const int tid = threadIdx.x, lane = tid & 31;
     bool inited = false;
     for (;;) {
         __syncthreads();  // the previous segment is finished by every thread
@@ -128,32 +137,50 @@ __global__ void __launch_bounds__(LC_T, 1)
         const int nch = sd.nch;
         const LcChunk *tab = sd.tab;
 
-        // producer (thread 0): issue every chunk whose issue iteration has come
-        int nxt = 0;
-        LcChunk ck{};
-        if (tid == 0 && nch > 0) ck = tab[0];
-        auto issue = [&](int it) {
-            while (nxt < nch && ck.issue <= it) {
-                const int src = layout32 ? ck.src32 : ck.src64;
-                const unsigned by = (unsigned)(layout32 ? ck.bytes32 : ck.bytes64) * 16u;
-                unsigned long long *mb = mbar + (nxt % LC_NB);
-                mbar_arrive_expect_tx(mb, by);
-                bulk_g2s(ring + (size_t)ck.ring * 16, rec + (size_t)src * 16, by, mb);
-                if (++nxt < nch) ck = tab[nxt];
+        // producer (the last warp, whose rows are the shortest): lane l holds
+        // table entries base + l (cur) and base + 32 + l (nxw); copies are
+        // issued in chunk order
+        int nxt = 0, base = 0;
+        LcChunk cur{}, nxw{};
+        const LcChunk none{0, 0, 0, 0, 0, 0x7fffffff};
+        const bool producer = tid >= LC_T - 32;
+        if (producer) {
+            cur = lane < nch ? tab[lane] : none;
+            nxw = 32 + lane < nch ? tab[32 + lane] : none;
+        }
+        auto issue = [&](int it) {  // producer warp, converged
+            for (;;) {
+                if (nxt >= nch) break;
+                if (nxt - base >= 32) {
+                    base += 32;
+                    cur = nxw;
+                    nxw = base + 32 + lane < nch ? tab[base + 32 + lane] : none;
+                }
+                const int k = nxt - base;
+                if (__shfl_sync(0xffffffffu, cur.issue, k) > it) break;
+                const int src = __shfl_sync(0xffffffffu, layout32 ? cur.src32 : cur.src64, k);
+                const int by = __shfl_sync(0xffffffffu, layout32 ? cur.bytes32 : cur.bytes64, k);
+                const int rg = __shfl_sync(0xffffffffu, cur.ring, k);
+                if (lane == 0) {
+                    unsigned long long *mb = mbar + (nxt % LC_NB);
+                    mbar_arrive_expect_tx(mb, (unsigned)by * 16u);
+                    bulk_g2s(ring + (size_t)rg * 16, rec + (size_t)src * 16, (unsigned)by * 16u, mb);
+                }
+                ++nxt;
             }
         };
-        int waited = 0;  // chunks whose copy this thread has seen land
-        // wait for chunk j's record, then copy the x of its old entries and
-        // its right-hand side into the record (thread-per-row, the mapping
-        // the compute step uses, so each thread reads only its own copies)
+        int waited = 0;  // chunks whose copy the producer has seen land
+        // producer: wait for chunk j's record, then copy the x of its old
+        // entries and its right-hand side into the record
         auto gather = [&](int j, int rj, int &rnext) -> bool {
             if (!mbar_wait_bounded(mbar + (j % LC_NB), (unsigned)((j / LC_NB) & 1), limit)) return false;
             waited = j + 1;
             unsigned char *rb = ring + (size_t)rj * 16;
             const int4 h = *reinterpret_cast<const int4 *>(rb);
-            rnext = reinterpret_cast<const int *>(rb)[4];
-            LcView<VT> v(rb, h.x, h.y, h.z);
-            for (int r = tid; r < h.x; r += LC_T) {
+            const int4 h2 = *reinterpret_cast<const int4 *>(rb + 16);
+            rnext = h2.x;
+            LcView<VT> v(rb, h.x, h.y, h.z, h2.y);
+            for (int r = lane; r < h.x; r += 32) {
                 const int s0 = v.rpo[r], s1 = v.rpo[r + 1];
                 for (int e = s0; e < s1; ++e) cp_async_v<VT>(v.gx + e, x + v.colo[e]);
                 cp_async_v<VT>(v.bs + r, b + v.dest[r]);
@@ -161,56 +188,70 @@ __global__ void __launch_bounds__(LC_T, 1)
             return true;
         };
 
+        // The producer runs LC_D chunks ahead: in iteration c it issues the
+        // copies due, gathers chunk c + LC_D and waits for its own gathers
+        // of chunk c + 1, so after the iteration's barrier every thread may
+        // read chunk c + 1's record (ring offset in s_roff).
         bool abort = false;
         int roff[LC_D + 1];
-        if (tid == 0) issue(0);
-        int rcur = sd.ring0;
+        if (producer) {
+            issue(0);
+            int rcur = sd.ring0;
 #pragma unroll
-        for (int j = 0; j < LC_D; ++j) {
-            roff[j] = rcur;
-            if (j < nch && !abort) {
-                int rn = 0;
-                if (gather(j, rcur, rn)) rcur = rn;
-                else abort = true;
+            for (int j = 0; j < LC_D; ++j) {
+                roff[j] = rcur;
+                if (j < nch && !abort) {
+                    int rn = 0;
+                    if (gather(j, rcur, rn)) rcur = rn;
+                    else abort = true;
+                }
+                cp_async_commit();
             }
-            cp_async_commit();
+            roff[LC_D] = rcur;
+            cp_async_wait<LC_D - 1>();  // chunk 0's gathers
+            if (lane == 0) s_roff[0] = roff[0];
         }
-        roff[LC_D] = rcur;
+        if (__syncthreads_or(abort)) abort = true;
 #pragma unroll 1
-        for (int c = 0; c < nch; ++c) {
-            if (tid == 0) issue(c);
-            const int j = c + LC_D;
-            int rn = 0;
-            if (j < nch && !abort && !gather(j, roff[LC_D], rn)) abort = true;
-            cp_async_commit();
-            cp_async_wait<LC_D>();  // this thread's copies for chunk c have landed
-            if (!abort) {
-                unsigned char *rb = ring + (size_t)roff[0] * 16;
+        for (int c = 0; c < nch && !abort; ++c) {
+            if (producer) {
+                issue(c);
+                const int j = c + LC_D;
+                int rn = 0;
+                if (j < nch && !abort && !gather(j, roff[LC_D], rn)) abort = true;
+                cp_async_commit();
+                cp_async_wait<LC_D - 1>();  // chunk c + 1's gathers have landed
+#pragma unroll
+                for (int q = 0; q < LC_D; ++q) roff[q] = roff[q + 1];
+                roff[LC_D] = rn;
+                if (lane == 0) s_roff[(c + 1) & 3] = roff[0];
+            }
+            {
+                unsigned char *rb = ring + (size_t)s_roff[c & 3] * 16;
                 const int4 h = *reinterpret_cast<const int4 *>(rb);
-                LcView<VT> v(rb, h.x, h.y, h.z);
+                const int4 h2 = *reinterpret_cast<const int4 *>(rb + 16);
+                LcView<VT> v(rb, h.x, h.y, h.z, h2.y);
                 for (int r = tid; r < h.x; r += LC_T) {
                     VT sum = 0;
+                    const int L = v.rlen[r];
+#pragma unroll 4
+                    for (int k = 0; k < L; ++k) {
+                        const int e = v.cs[k] + r;
+                        sum += v.valr[e] * xs[v.colr[e]];
+                    }
                     const int o0 = v.rpo[r], o1 = v.rpo[r + 1];
                     for (int e = o0; e < o1; ++e) sum += v.valo[e] * v.gx[e];
-                    const int q0 = v.rpr[r], q1 = v.rpr[r + 1];
-                    for (int e = q0; e < q1; ++e) sum += v.valr[e] * xs[v.colr[e]];
                     const VT xv = finalize((v.bs[r] - sum) * v.inv[r]);
                     xs[(h.w + r) & (LC_XW - 1)] = xv;
                     x[v.dest[r]] = xv;
                 }
             }
-#pragma unroll
-            for (int q = 0; q < LC_D; ++q) roff[q] = roff[q + 1];
-            roff[LC_D] = rn;
-            if (__syncthreads_or(abort)) {
-                abort = true;
-                break;
-            }
+            if (__syncthreads_or(abort)) abort = true;
         }
         cp_async_wait<0>();
         if (abort) {
             // drain: every copy issued must land before the CTA exits
-            if (tid == 0) {
+            if (tid == LC_T - 32) {  // the producer's lane 0
                 atomicOr(status, RBS_STATUS_TIMEOUT);
                 for (int j = waited; j < nxt; ++j)
                     mbar_wait_bounded(mbar + (j % LC_NB), (unsigned)((j / LC_NB) & 1), limit);

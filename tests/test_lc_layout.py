@@ -24,20 +24,26 @@ def _padv(n, es):
     return ((n * es + 15) // 16) * 16 // es
 
 
-def _foot(nr, no, nrec, hdr):
-    ints = hdr + _pad4(nr) + 2 * _pad4(nr + 1) + _pad4(no) + _pad4(nrec)
-    dbl = _padv(nr, 8) * 2 + _padv(no, 8) * 2 + _padv(nrec, 8)
-    return 4 * ints + 8 * dbl
+def _static(nr, no, nrec, ncols, hdr):
+    ints = hdr + 2 * _pad4(nr) + _pad4(nr + 1) + _pad4(ncols + 1) + _pad4(nrec) + _pad4(no)
+    return 4 * ints + 8 * (_padv(nr, 8) + _padv(nrec, 8) + _padv(no, 8))
+
+
+def _foot(nr, no, nrec, ncols, hdr):
+    return _static(nr, no, nrec, ncols, hdr) + 8 * (_padv(no, 8) + _padv(nr, 8))
 
 
 def _parse(words, src16, hdr):
     """Sections of one FP64 record (mirrors LcView)."""
     w = words[src16 * 4:]
-    nr, no, nrec, vbase, rnext = (int(v) for v in w[:5])
+    nr, no, nrec, vbase, rnext, ncols = (int(v) for v in w[:6])
     o = hdr
-    dest = w[o:o + nr]; o += _pad4(nr)
-    rpo = w[o:o + nr + 1]; o += _pad4(nr + 1)
-    rpr = w[o:o + nr + 1]; o += _pad4(nr + 1)
+
+    def ints(cnt):
+        nonlocal o
+        v = w[o:o + cnt]
+        o += _pad4(cnt)
+        return v
 
     def dbl(cnt):
         nonlocal o
@@ -45,13 +51,17 @@ def _parse(words, src16, hdr):
         o += 2 * _padv(cnt, 8)
         return v
 
+    dest = ints(nr)
+    rlen = ints(nr)
+    rpo = ints(nr + 1)
+    cs = ints(ncols + 1)
     inv = dbl(nr)
-    colo = w[o:o + no]; o += _pad4(no)
-    valo = dbl(no)
-    colr = w[o:o + nrec]; o += _pad4(nrec)
+    colr = ints(nrec)
     valr = dbl(nrec)
-    return dict(nr=nr, no=no, nrec=nrec, vbase=vbase, rnext=rnext, dest=dest, rpo=rpo, rpr=rpr, inv=inv,
-                colo=colo, valo=valo, colr=colr, valr=valr)
+    colo = ints(no)
+    valo = dbl(no)
+    return dict(nr=nr, no=no, nrec=nrec, vbase=vbase, rnext=rnext, ncols=ncols, dest=dest, rlen=rlen, rpo=rpo,
+                cs=cs, inv=inv, colr=colr, valr=valr, colo=colo, valo=valo)
 
 
 def emulate(plan, b_proc):
@@ -82,11 +92,9 @@ def emulate(plan, b_proc):
                     j = issued[0]
                     r = recs[j]
                     lo = int(tab[c0 + j, 4]) * 16
-                    f = _foot(r["nr"], r["no"], r["nrec"], HDR)
+                    f = _foot(r["nr"], r["no"], r["nrec"], r["ncols"], HDR)
                     assert f <= FMAX and lo + f <= RING
-                    assert int(tab[c0 + j, 1]) * 16 == 4 * (HDR + _pad4(r["nr"]) + 2 * _pad4(r["nr"] + 1) +
-                                                            _pad4(r["no"]) + _pad4(r["nrec"])) + \
-                        8 * (_padv(r["nr"], 8) + _padv(r["no"], 8) + _padv(r["nrec"], 8))
+                    assert int(tab[c0 + j, 1]) * 16 == _static(r["nr"], r["no"], r["nrec"], r["ncols"], HDR)
                     for k, (a, e) in live.items():
                         assert not (a < lo + f and lo < e), f"chunk {j} overwrites live chunk {k}"
                     if j >= NB:  # slot reuse: the previous user was gathered before a barrier that precedes `it`
@@ -115,12 +123,15 @@ def emulate(plan, b_proc):
                 if c + 1 < nch:
                     assert r["rnext"] == int(tab[c0 + c + 1, 4])
                 gx, bs = gathered.pop(c)
+                rl = r["rlen"]
+                assert (np.diff(rl) <= 0).all() and (len(rl) == 0 or rl[0] <= r["ncols"])
                 for t in range(r["nr"]):
                     o0, o1 = r["rpo"][t], r["rpo"][t + 1]
-                    q0, q1 = r["rpr"][t], r["rpr"][t + 1]
-                    wv = win[r["colr"][q0:q1]]
+                    es = r["cs"][:rl[t]] + t
+                    assert (es < r["cs"][1:rl[t] + 1]).all(), "jagged column overrun"
+                    wv = win[r["colr"][es]]
                     assert not np.isnan(wv).any(), "recent dependency missing from the window"
-                    ssum = np.dot(r["valo"][o0:o1], gx[o0:o1]) + np.dot(r["valr"][q0:q1], wv)
+                    ssum = np.dot(r["valr"][es], wv) + np.dot(r["valo"][o0:o1], gx[o0:o1])
                     xv = (bs[t] - ssum) * r["inv"][t]
                     win[(r["vbase"] + t) & (XW - 1)] = xv
                     assert np.isnan(xb[r["dest"][t]])
