@@ -341,7 +341,7 @@ static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &le
             const int *sq = seq.data() + scount[(size_t)q];
             const auto &ch = chunks[(size_t)q];
             const int nch = (int)ch.size();
-            P.lc_segs.insert(P.lc_segs.end(), {(int)(P.lc_tab.size() / 6), nch, nch ? roff[(size_t)q][0] : 0});
+            P.lc_segs.insert(P.lc_segs.end(), {(int)(P.lc_tab.size() / LC_TAB_INTS), nch, nch ? roff[(size_t)q][0] : 0});
             for (int j = 0; j < nch; ++j) {
                 const Ch &c = ch[(size_t)j];
                 const int thr = c.v0 + c.nr - LC_XW;
@@ -384,12 +384,19 @@ static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &le
                     }
                 }
                 const int rnext = j + 1 < nch ? roff[(size_t)q][(size_t)j + 1] : 0;
+                // contiguous block rows: the kernel bulk-copies their right-hand side
+                int dmin = dest[0], dmax = dest[0];
+                for (int t = 1; t < c.nr; ++t) {
+                    dmin = std::min(dmin, dest[(size_t)t]);
+                    dmax = std::max(dmax, dest[(size_t)t]);
+                }
+                const int blo = dmax - dmin + 1 == c.nr ? dmin : -1;
                 auto emit = [&](std::vector<uint32_t> &pool, int es) -> std::pair<int, int> {
                     const size_t base = pool.size();
                     const long long bytes = lc_static_bytes(c.nr, c.no, c.nrec, c.ncols, es);
                     pool.resize(base + (size_t)(bytes / 4), 0u);
                     uint32_t *w = pool.data() + base;
-                    const int hdr[LC_HDR_INTS] = {c.nr, c.no, c.nrec, c.v0, rnext, c.ncols, c.maxlen, 0};
+                    const int hdr[LC_HDR_INTS] = {c.nr, c.no, c.nrec, c.v0, rnext, c.ncols, c.maxlen, blo};
                     std::memcpy(w, hdr, sizeof(hdr));
                     size_t o = LC_HDR_INTS;
                     auto put_i = [&](const std::vector<int> &v) {
@@ -420,8 +427,10 @@ static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &le
                 };
                 const auto r64 = emit(P.lc_rec64, 8);
                 const auto r32 = emit(P.lc_rec32, 4);
-                P.lc_tab.insert(P.lc_tab.end(), {r64.first, r64.second, r32.first, r32.second,
-                                                 roff[(size_t)q][(size_t)j], iss[(size_t)q][(size_t)j]});
+                const int bs64 = (int)((lc_static_bytes(c.nr, c.no, c.nrec, c.ncols, 8) + lc_padv(c.no, 8)) / 16);
+                const int bs32 = (int)((lc_static_bytes(c.nr, c.no, c.nrec, c.ncols, 4) + lc_padv(c.no, 4)) / 16);
+                P.lc_tab.insert(P.lc_tab.end(), {r64.first, r64.second, r32.first, r32.second, roff[(size_t)q][(size_t)j],
+                                                 iss[(size_t)q][(size_t)j], blo, blo >= 0 ? c.nr : 0, bs64, bs32});
             }
         }
     }

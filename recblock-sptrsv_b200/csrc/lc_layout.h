@@ -27,7 +27,11 @@ struct LcChunk {  // 16-byte units unless noted
     int src32, bytes32;  // static record, FP32 layout
     int ring;            // ring offset
     int issue;           // chunk iteration at whose start the copy is issued
+    int blo, bn;         // rows: the chunk's block rows are [blo, blo + bn) (blo = -1: scattered)
+    int bs64, bs32;      // offset of the right-hand-side area from the record start
 };
+constexpr int LC_TAB_INTS = 10;
+static_assert(sizeof(LcChunk) == LC_TAB_INTS * sizeof(int), "table rows are LC_TAB_INTS ints");
 
 LC_HD constexpr int lc_pad4(int n) { return (n + 3) & ~3; }  // ints up to a 16-byte multiple
 LC_HD constexpr long long lc_padv(int n, int es) { return (long long)((n * (long long)es + 15) / 16) * 16; }  // bytes
@@ -36,13 +40,15 @@ LC_HD constexpr long long lc_padv(int n, int es) { return (long long)((n * (long
 // recent entries form ncols jagged columns.  Ints: header, dest[nr],
 // rlen[nr], rpo[nr+1], cs[ncols+1]; then inv[nr] (VT), colr[nrec] (int),
 // valr[nrec] (VT), colo[no] (int), valo[no] (VT); the ring also reserves
-// gx[no] and bs[nr] (VT) behind the copied part.
+// gx[no] and the right-hand-side area bs (VT) behind the copied part: nr
+// values, or a 16-byte-aligned bulk copy of b[blo, blo+nr) with up to
+// 16 bytes of slack at either end.
 LC_HD constexpr long long lc_static_bytes(int nr, int no, int nrec, int ncols, int es) {
     return 4LL * (LC_HDR_INTS + 2 * lc_pad4(nr) + lc_pad4(nr + 1) + lc_pad4(ncols + 1)) + lc_padv(nr, es) +
            4LL * lc_pad4(nrec) + lc_padv(nrec, es) + 4LL * lc_pad4(no) + lc_padv(no, es);
 }
 LC_HD constexpr long long lc_foot_bytes(int nr, int no, int nrec, int ncols, int es) {
-    return lc_static_bytes(nr, no, nrec, ncols, es) + lc_padv(no, es) + lc_padv(nr, es);
+    return lc_static_bytes(nr, no, nrec, ncols, es) + lc_padv(no, es) + lc_padv(nr + 32 / es, es);
 }
 
 }  // namespace rbs

@@ -24,12 +24,14 @@
 // which its copy may be issued (the ring bytes and mbarrier slot it reuses
 // are free by then), always at least LC_D chunks before it is used.  The
 // last warp (rows are sorted longest first, so its rows are the shortest)
-// issues the copies from a 32-entry window of the chunk table held in its
-// registers (the next window is loaded 32 chunks ahead).
+// issues the copies: lane l holds entry base + l of a 32-entry window of the
+// chunk table (the next window is loaded 32 chunks ahead) and issues that
+// chunk's copies itself once it is due.
 //
 // Record layout (sections 16-byte aligned, element type VT):
 //   int hdr[8]: nrows, ne_old, ne_rec, vbase, ring offset of the next chunk
-//               (16-byte units), jagged columns, longest row
+//               (16-byte units), jagged columns, longest row, blo (first block
+//               row when the rows are contiguous, else -1)
 //   int dest[nrows]          block row of each chunk row
 //   int rlen[nrows]          recent entries of each row (non-increasing)
 //   int rpo[nrows+1]         old-entry pointer
@@ -41,7 +43,10 @@
 //   VT  valo[ne_old]
 //   -- end of the copied part; the ring also reserves --
 //   VT  gx[ne_old]           gathered x of the old entries
-//   VT  bs[nrows]            gathered right-hand side
+//   VT  bs[...]              right-hand side: gathered per row (bs[r]), or, when the
+//                            chunk's rows are contiguous block rows [blo, blo+nrows),
+//                            bulk-copied with the record from the 16-byte boundary
+//                            at or below b + blo
 #pragma once
 
 #include "lc_layout.h"
@@ -142,7 +147,7 @@ __global__ void __launch_bounds__(LC_T, 1)
         // issued in chunk order
         int nxt = 0, base = 0;
         LcChunk cur{}, nxw{};
-        const LcChunk none{0, 0, 0, 0, 0, 0x7fffffff};
+        const LcChunk none{0, 0, 0, 0, 0, 0x7fffffff, -1, 0, 0, 0};
         const bool producer = tid >= LC_T - 32;
         if (producer) {
             cur = lane < nch ? tab[lane] : none;
@@ -156,17 +161,26 @@ __global__ void __launch_bounds__(LC_T, 1)
                     cur = nxw;
                     nxw = base + 32 + lane < nch ? tab[base + 32 + lane] : none;
                 }
-                const int k = nxt - base;
-                if (__shfl_sync(0xffffffffu, cur.issue, k) > it) break;
-                const int src = __shfl_sync(0xffffffffu, layout32 ? cur.src32 : cur.src64, k);
-                const int by = __shfl_sync(0xffffffffu, layout32 ? cur.bytes32 : cur.bytes64, k);
-                const int rg = __shfl_sync(0xffffffffu, cur.ring, k);
-                if (lane == 0) {
-                    unsigned long long *mb = mbar + (nxt % LC_NB);
-                    mbar_arrive_expect_tx(mb, (unsigned)by * 16u);
-                    bulk_g2s(ring + (size_t)rg * 16, rec + (size_t)src * 16, (unsigned)by * 16u, mb);
+                // chunks due now form a run starting at nxt: each lane issues its own
+                const bool ready = base + lane >= nxt && cur.issue <= it;
+                const unsigned due = __ballot_sync(0xffffffffu, ready);
+                if (ready) {
+                    const int j = base + lane;
+                    unsigned long long *mb = mbar + (j % LC_NB);
+                    const int by = (layout32 ? cur.bytes32 : cur.bytes64) * 16;
+                    unsigned bb = 0;
+                    const void *bsrc = nullptr;
+                    if (cur.blo >= 0) {  // contiguous rows: their right-hand side in the same transaction
+                        int delta;
+                        bb = bulk_window(b + cur.blo, cur.bn, (int)sizeof(VT), bsrc, delta);
+                    }
+                    mbar_arrive_expect_tx(mb, (unsigned)by + bb);
+                    bulk_g2s(ring + (size_t)cur.ring * 16, rec + (size_t)(layout32 ? cur.src32 : cur.src64) * 16,
+                             (unsigned)by, mb);
+                    if (bb) bulk_g2s(ring + (size_t)(cur.ring + (layout32 ? cur.bs32 : cur.bs64)) * 16, bsrc, bb, mb);
                 }
-                ++nxt;
+                nxt += __popc(due);
+                if (nxt - base < 32) break;  // the run ended inside this window
             }
         };
         int waited = 0;  // chunks whose copy the producer has seen land
@@ -180,11 +194,13 @@ __global__ void __launch_bounds__(LC_T, 1)
             const int4 h2 = *reinterpret_cast<const int4 *>(rb + 16);
             rnext = h2.x;
             LcView<VT> v(rb, h.x, h.y, h.z, h2.y);
-            for (int r = lane; r < h.x; r += 32) {
-                const int s0 = v.rpo[r], s1 = v.rpo[r + 1];
-                for (int e = s0; e < s1; ++e) cp_async_v<VT>(v.gx + e, x + v.colo[e]);
-                cp_async_v<VT>(v.bs + r, b + v.dest[r]);
-            }
+            const int blo = h2.w;
+            if (h.y > 0 || blo < 0)
+                for (int r = lane; r < h.x; r += 32) {
+                    const int s0 = v.rpo[r], s1 = v.rpo[r + 1];
+                    for (int e = s0; e < s1; ++e) cp_async_v<VT>(v.gx + e, x + v.colo[e]);
+                    if (blo < 0) cp_async_v<VT>(v.bs + r, b + v.dest[r]);
+                }
             return true;
         };
 
@@ -231,6 +247,9 @@ __global__ void __launch_bounds__(LC_T, 1)
                 const int4 h = *reinterpret_cast<const int4 *>(rb);
                 const int4 h2 = *reinterpret_cast<const int4 *>(rb + 16);
                 LcView<VT> v(rb, h.x, h.y, h.z, h2.y);
+                const int blo = h2.w;
+                // contiguous rows: bs holds b[blo - delta, ...) from a 16-byte boundary
+                const int bshift = blo >= 0 ? (int)(((unsigned long long)(b + blo) & 15ull) / sizeof(VT)) - blo : 0;
                 for (int r = tid; r < h.x; r += LC_T) {
                     VT sum = 0;
                     const int L = v.rlen[r];
@@ -241,9 +260,10 @@ __global__ void __launch_bounds__(LC_T, 1)
                     }
                     const int o0 = v.rpo[r], o1 = v.rpo[r + 1];
                     for (int e = o0; e < o1; ++e) sum += v.valo[e] * v.gx[e];
-                    const VT xv = finalize((v.bs[r] - sum) * v.inv[r]);
+                    const int d = v.dest[r];
+                    const VT xv = finalize((v.bs[blo >= 0 ? d + bshift : r] - sum) * v.inv[r]);
                     xs[(h.w + r) & (LC_XW - 1)] = xv;
-                    x[v.dest[r]] = xv;
+                    x[d] = xv;
                 }
             }
             if (__syncthreads_or(abort)) abort = true;

@@ -102,9 +102,8 @@ struct Plan {
     std::vector<int> ca_tab, ca_col;           // level tables and level-ELL columns (-1 = padding)
     std::vector<double> ca_val;
     // level-chunk records (level_lc.cuh): 16-byte words of the FP64 and FP32
-    // layouts, 6 ints per chunk (src64, bytes64, src32, bytes32, ring, issue;
-    // 16-byte units), 3 ints per segment (first chunk, chunks, ring offset of
-    // the first chunk)
+    // layouts, one LcChunk (lc_layout.h) per chunk, 3 ints per segment (first
+    // chunk, chunks, ring offset of the first chunk)
     std::vector<uint32_t> lc_rec64, lc_rec32;
     std::vector<int> lc_tab, lc_segs;
     // original-row offsets of independent systems (batched plans); empty

@@ -434,7 +434,8 @@ int launch_blocks(Plan &P, std::string &err) {
                                            P.lc_segs[(size_t)(3 * (B.lc_seg_off + B.lc_nseg - 1) + 1)];
                 if (c1 > c0) {
                     const bool f64 = sizeof(VT) == 8;
-                    const int *t0 = P.lc_tab.data() + 6 * (size_t)c0, *t1 = P.lc_tab.data() + 6 * (size_t)(c1 - 1);
+                    const int *t0 = P.lc_tab.data() + LC_TAB_INTS * (size_t)c0,
+                              *t1 = P.lc_tab.data() + LC_TAB_INTS * (size_t)(c1 - 1);
                     const long long a = 16LL * (f64 ? t0[0] : t0[2]), e = 16LL * ((f64 ? t1[0] : t1[2]) + (f64 ? t1[1] : t1[3]));
                     prefetch_range(D.side, Pools<VT>::lcrec(D) + a, e - a);
                     budget -= e - a;
@@ -747,7 +748,7 @@ int device_build(Plan &P, std::string &err) {
         if ((rc = upload(D, D.ell_val32, e32, err))) return rc;
     }
     if (!P.lc_tab.empty()) {
-        std::vector<LcChunk> tab(P.lc_tab.size() / 6);
+        std::vector<LcChunk> tab(P.lc_tab.size() / LC_TAB_INTS);
         std::memcpy(tab.data(), P.lc_tab.data(), tab.size() * sizeof(LcChunk));
         if ((rc = upload(D, D.lc_tab, tab, err))) return rc;
         if ((rc = upload(D, D.lc_rec64, P.lc_rec64, err))) return rc;

@@ -30,13 +30,15 @@ def _static(nr, no, nrec, ncols, hdr):
 
 
 def _foot(nr, no, nrec, ncols, hdr):
-    return _static(nr, no, nrec, ncols, hdr) + 8 * (_padv(no, 8) + _padv(nr, 8))
+    # gathered x of the old entries, then the right-hand-side area with
+    # 32 bytes of slack for a 16-byte-aligned bulk copy
+    return _static(nr, no, nrec, ncols, hdr) + 8 * (_padv(no, 8) + _padv(nr + 4, 8))
 
 
 def _parse(words, src16, hdr):
     """Sections of one FP64 record (mirrors LcView)."""
     w = words[src16 * 4:]
-    nr, no, nrec, vbase, rnext, ncols = (int(v) for v in w[:6])
+    nr, no, nrec, vbase, rnext, ncols, maxlen, blo = (int(v) for v in w[:8])
     o = hdr
 
     def ints(cnt):
@@ -60,13 +62,14 @@ def _parse(words, src16, hdr):
     valr = dbl(nrec)
     colo = ints(no)
     valo = dbl(no)
-    return dict(nr=nr, no=no, nrec=nrec, vbase=vbase, rnext=rnext, ncols=ncols, dest=dest, rlen=rlen, rpo=rpo,
+    return dict(nr=nr, no=no, nrec=nrec, vbase=vbase, rnext=rnext, ncols=ncols, maxlen=maxlen, blo=blo, dest=dest,
+                rlen=rlen, rpo=rpo,
                 cs=cs, inv=inv, colr=colr, valr=valr, colo=colo, valo=valo)
 
 
 def emulate(plan, b_proc):
     XW, NB, D, RMAX, T, RING, FMAX, HDR = (int(v) for v in plan.export("lc_consts"))
-    tab = plan.export("lc_tab").reshape(-1, 6)
+    tab = plan.export("lc_tab").reshape(-1, 10)
     segs = plan.export("lc_segs").reshape(-1, 3)
     words = plan.export("lc_rec64")
     blk = plan.export("lc_block").reshape(-1, 3)
@@ -95,6 +98,12 @@ def emulate(plan, b_proc):
                     f = _foot(r["nr"], r["no"], r["nrec"], r["ncols"], HDR)
                     assert f <= FMAX and lo + f <= RING
                     assert int(tab[c0 + j, 1]) * 16 == _static(r["nr"], r["no"], r["nrec"], r["ncols"], HDR)
+                    blo, bn = int(tab[c0 + j, 6]), int(tab[c0 + j, 7])
+                    assert blo == r["blo"]
+                    if blo >= 0:  # contiguous rows: bulk right-hand side
+                        assert bn == r["nr"] and sorted(r["dest"]) == list(range(blo, blo + bn))
+                    assert int(tab[c0 + j, 8]) * 16 == _static(r["nr"], r["no"], r["nrec"], r["ncols"], HDR) + \
+                        8 * _padv(r["no"], 8)
                     for k, (a, e) in live.items():
                         assert not (a < lo + f and lo < e), f"chunk {j} overwrites live chunk {k}"
                     if j >= NB:  # slot reuse: the previous user was gathered before a barrier that precedes `it`
