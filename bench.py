@@ -205,6 +205,14 @@ def timed_solves(plan, db, dx, steps, flush, k=1, prec=0):
     return ms, st
 
 
+def replica_throughput(rank_total_ms, steps, world, allmax):
+    """Whole-job solves/s of `world` independent replicas that each timed
+    `steps` solves: all ranks' solves over the slowest rank's time (max over
+    ranks, `allmax`), and that time per step."""
+    total = allmax(rank_total_ms)
+    return world * steps * 1000.0 / total, total / steps
+
+
 def rel(x, ref):
     return float(np.linalg.norm(x - ref) / np.linalg.norm(ref))
 
@@ -478,6 +486,18 @@ def side_serving(dev, args, n_requests=1500, loads=(1000, 10000, 50000)):
     return res
 
 
+def profiled_traffic(kind):
+    """DRAM bytes (read + write) per launch of the dominant kernel from the
+    committed ncu summary of the same workload (profiles/), or None."""
+    path = {"level": os.path.join(ROOT, "profiles", "k_tri_level_ca_c1a.md")}.get(kind)
+    if not path or not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
 def launches_per_solve(plan):
     import rbs
     kern = plan.export("kernel")
@@ -530,9 +550,7 @@ def run_ours(args):
     clk = clocks.stop()
     x = dx.cpu().numpy()
     rel = float(np.linalg.norm(x - sysm["x_true"]) / np.linalg.norm(sysm["x_true"]))
-    total_ms = allmax(float(sum(ms)))
-    value = world * args.steps * 1000.0 / total_ms
-    ms_per_step = total_ms / args.steps
+    value, ms_per_step = replica_throughput(float(sum(ms)), args.steps, world, allmax)
     useful = st.useful_bytes
     # per-block device time -> dominant kernel kind and its roofline
     bms, bbytes, solves = plan.block_times()
@@ -549,13 +567,7 @@ def run_ours(args):
     dom_bytes_per_launch = by_kind[dom][1] / by_kind[dom][2]
     peak, peak_kind = peaks()
     achieved = dom_bytes_per_launch / (dom_launch_ms / 1000) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get(rbs.KERNEL_NAMES[dom])
-        except Exception:
-            traffic = None
+    traffic = profiled_traffic(rbs.KERNEL_NAMES[dom])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": peak_kind, "kernel": rbs.KERNEL_NAMES[dom],
                 "kernel_share": by_kind[dom][0] / max(sum(v[0] for v in by_kind.values()), 1e-30),
@@ -609,14 +621,16 @@ def run_ours(args):
         "analyse_ms": info.analyse_ms,
     }
 
-    if not args.no_sweep:
+    # side measurements (other configurations) on a single GPU only: with
+    # N replicas they would repeat the same numbers N times
+    if not args.no_sweep and world == 1:
         line["config3_multi_rhs_c1a"] = side_multi_rhs(plan, sysm, dev, flush, args)
         del plan
         line["sweep_config1"] = side_structures(dev, flush, args)
         line["config2_mixed"] = side_mixed(dev, flush, args)
-    if not args.no_batch:
+    if not args.no_batch and world == 1:
         line["config3_batched_512"] = side_batched(dev, args)
-    if not args.no_serve:
+    if not args.no_serve and world == 1:
         line["config4_serving"] = side_serving(dev, args)
 
     if rank == 0 and world == 1:

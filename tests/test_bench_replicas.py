@@ -1,0 +1,56 @@
+"""The multi-GPU arm of bench.py runs independent replicas (a triangular
+solve has no data-path collective); the only cross-rank step is the max of
+the ranks' timed totals.  Checked here with world_size 2 over gloo on CPU."""
+import os
+import sys
+
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _rank(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    sys.path.insert(0, ROOT)
+    import bench
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+
+    def allmax(v):
+        t = torch.tensor([v], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # rank r timed 10 solves in (100 + 50 r) ms
+    value, ms_per_step = bench.replica_throughput(100.0 + 50.0 * rank, 10, world, allmax)
+    q.put((rank, value, ms_per_step))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_replica_throughput_uses_slowest_rank():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29000 + os.getpid() % 1000
+    procs = [ctx.Process(target=_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, value, ms_per_step in out:
+        assert ms_per_step == pytest.approx(15.0)          # slowest rank: 150 ms / 10 solves
+        assert value == pytest.approx(2 * 10 * 1000.0 / 150.0)
+
+
+def test_reference_arm_runs_on_rank0_only(monkeypatch, capsys):
+    sys.path.insert(0, ROOT)
+    import bench
+    monkeypatch.setenv("RANK", "1")
+    args = type("A", (), {"steps": 1, "warmup": 0, "gpus": 2})()
+    bench.run_reference(args)  # returns without work or output on rank 1
+    assert capsys.readouterr().out == ""
