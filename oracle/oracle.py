@@ -79,6 +79,20 @@ def auto_lv(m, device_id=0):
     return lib.orc_auto_lv(m, device_id)
 
 
+def reorder_colrow(colptr, rowidx, val, substitution):
+    """Restated levelset_reordering_colrow_csc: (colptr_new, rowidx_new,
+    val_new, levelItem) of the level-permuted CSC."""
+    cp, ri, va = _i(colptr), _i(rowidx), _d(val)
+    m, nnz = len(cp) - 1, len(ri)
+    ncp, nri, nva, item = np.zeros(m + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz), np.zeros(m, np.int32)
+    rc = lib.orc_reorder_colrow(cp.ctypes.data_as(_ip), ri.ctypes.data_as(_ip), va.ctypes.data_as(_dp), m, nnz,
+                                substitution, ncp.ctypes.data_as(_ip), nri.ctypes.data_as(_ip),
+                                nva.ctypes.data_as(_dp), item.ctypes.data_as(_ip))
+    if rc != 0:
+        raise RuntimeError("oracle reorder: level search stuck")
+    return ncp, nri, nva, item
+
+
 def analyse(colptr, rowidx, val, substitution, lv):
     """Restated reference analysis; returns a dict of numpy arrays named like the reference's variables."""
     cp, ri, va = _i(colptr), _i(rowidx), _d(val)

@@ -448,8 +448,6 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
                  int substitution, int lv, const rbs_options &opt, std::string &err,
                  const std::vector<int> *seg_rows) {
     auto t0 = std::chrono::steady_clock::now();
-    P.seg_rows.clear();
-    if (seg_rows) P.seg_rows = *seg_rows;
     if (n <= 0 || nnz < n || !ptr || !idx || !val) {
         err = "rbs_analyse: need n > 0, nnz >= n and non-null arrays";
         return RBS_ERR_ARG;
@@ -521,21 +519,6 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
             }
         }
     }
-    // 2. recursion depth (main.cu:245-254 for lv == -1)
-    if (lv == -1) {
-        lv = auto_lv(n, opt.lv_device_id);
-        while (lv > 0 && (1 << lv) > n) --lv;
-    }
-    if (lv < 0 || lv > 24 || (1 << lv) > n) {
-        err = "rbs_analyse: lv must satisfy 0 <= lv and 2^lv <= n";
-        return RBS_ERR_ARG;
-    }
-    P.lv = lv;
-    const int T = 1 << lv;
-    P.sum_block = 2 * T - 1;
-    P.step = n / T;
-    const int s = P.step;
-
     // 3. level sets in the reference's discovery order
     int nlevel = bfs_levels(cp, ri, n, P.bfs_ptr, P.bfs_item);
     if (nlevel < 0) {
@@ -580,6 +563,39 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
             P.full_val[d] = va[k];
         }
     }
+    P.analyse_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return analyse_after_levels(P, n, nnz, substitution, lv, opt, err, seg_rows);
+}
+
+// Steps after the level sets: recursion depth, blocks, statistics, kernel
+// choice and pools, from the processing-order CSR (full_rp/col/val), the
+// BFS order and the labels -- computed by analyse_host above or on the
+// device (dev_analysis.cu).
+int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, const rbs_options &opt, std::string &err,
+                         const std::vector<int> *seg_rows) {
+    auto t0 = std::chrono::steady_clock::now();
+    (void)nnz;
+    P.opt = opt;
+    P.n = n;
+    P.nnz = nnz;
+    P.sub = substitution;
+    P.seg_rows.clear();
+    if (seg_rows) P.seg_rows = *seg_rows;
+    // 2. recursion depth (main.cu:245-254 for lv == -1)
+    if (lv == -1) {
+        lv = auto_lv(n, opt.lv_device_id);
+        while (lv > 0 && (1 << lv) > n) --lv;
+    }
+    if (lv < 0 || lv > 24 || (1 << lv) > n) {
+        err = "rbs_analyse: lv must satisfy 0 <= lv and 2^lv <= n";
+        return RBS_ERR_ARG;
+    }
+    P.lv = lv;
+    const int T = 1 << lv;
+    P.sum_block = 2 * T - 1;
+    P.step = n / T;
+    const int s = P.step;
+
     const int *frp = P.full_rp.data(), *fcol = P.full_col.data();
     const double *fval = P.full_val.data();
 
@@ -936,7 +952,7 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
         B.lvl_var = B.ca_ok ? LVL_CA : B.lc_ok ? LVL_LC : B.ell_ok ? LVL_CSF : LVL_PLAIN;
     }
     auto t1 = std::chrono::steady_clock::now();
-    P.analyse_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    P.analyse_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
     return RBS_OK;
 }
 
@@ -1027,6 +1043,24 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
                 iv[2 * b] = (int)P.blocks[b].ell_chunk_off;
                 iv[2 * b + 1] = P.blocks[b].ell_nchunks;
             }
+        return RBS_OK;
+    }
+    if (name == "reordered_colptr" || name == "reordered_rowidx") {
+        // the reference's level-permuted CSC (utils_reordering.h:102-187):
+        // the device analysis's own arrays when it ran, else rebuilt here
+        if (!P.dev_reorder_cp.empty()) return put(name == "reordered_colptr" ? P.dev_reorder_cp : P.dev_reorder_ri);
+        std::vector<int> ncp((size_t)n + 1, 0), nri;
+        nri.reserve((size_t)nnz);
+        for (int i = 0; i < n; ++i) {
+            const int src = P.bfs_item[(size_t)(fwd ? i : n - 1 - i)];
+            for (int k = P.in_cp[(size_t)src]; k < P.in_cp[(size_t)src + 1]; ++k) nri.push_back(P.label[(size_t)P.in_ri[(size_t)k]]);
+            ncp[(size_t)i + 1] = (int)nri.size();
+        }
+        return put(name == "reordered_colptr" ? ncp : nri);
+    }
+    if (name == "analyse_ms") {  // total analysis, of which on the device
+        is_double = true;
+        dv = {P.analyse_ms, P.device_analyse_ms};
         return RBS_OK;
     }
     if (name == "lc_consts") {  // the layout constants the records were built for

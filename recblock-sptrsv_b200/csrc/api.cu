@@ -96,15 +96,52 @@ int rbs_analyse(const int *ptr, const int *idx, const double *val, int n, int nn
 
 int rbs_analyse_device(const int *d_ptr, const int *d_idx, const double *d_val, int n, int nnz, int fmt,
                        int substitution, int lv, const rbs_options *opt, rbs_plan **plan) {
-    if (!plan || !d_ptr || !d_idx || !d_val || n <= 0 || nnz < n)
-        return fail(RBS_ERR_ARG, "rbs_analyse_device: bad arguments");
-    std::vector<int> ptr((size_t)n + 1), idx((size_t)nnz);
-    std::vector<double> val((size_t)nnz);
-    cudaError_t e = cudaMemcpy(ptr.data(), d_ptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(idx.data(), d_idx, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(val.data(), d_val, sizeof(double) * (size_t)nnz, cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return fail(RBS_ERR_CUDA, std::string("rbs_analyse_device: ") + cudaGetErrorString(e));
-    return rbs_analyse(ptr.data(), idx.data(), val.data(), n, nnz, fmt, substitution, lv, opt, plan);
+    if (!plan) return fail(RBS_ERR_ARG, "rbs_analyse_device: plan is NULL");
+    *plan = nullptr;
+    if (!d_ptr || !d_idx || !d_val || n <= 0 || nnz < n)
+        return fail(RBS_ERR_ARG, "rbs_analyse_device: need n > 0, nnz >= n and non-null arrays");
+    if (substitution != RBS_FORWARD && substitution != RBS_BACKWARD)
+        return fail(RBS_ERR_ARG, "rbs_analyse: substitution must be RBS_FORWARD or RBS_BACKWARD");
+    if (fmt != RBS_FMT_CSC && fmt != RBS_FMT_CSR) return fail(RBS_ERR_ARG, "rbs_analyse: fmt must be RBS_FMT_CSC or RBS_FMT_CSR");
+    rbs_options o;
+    rbs_options_default(&o);
+    if (opt) o = *opt;
+    if (o.max_rhs < 1) o.max_rhs = 1;
+    if (o.spin_limit <= 0) o.spin_limit = 1LL << 22;
+    if (o.ir_max_iter <= 0) o.ir_max_iter = 8;
+    if (!(o.ir_tol > 0)) o.ir_tol = 1e-13;
+    if (o.select < RBS_SELECT_REFERENCE || o.select > RBS_SELECT_TUNE)
+        return fail(RBS_ERR_ARG, "rbs_analyse: unknown select mode");
+    if (o.device >= 0) {
+        cudaError_t e = cudaSetDevice(o.device);
+        if (e != cudaSuccess) return fail(RBS_ERR_CUDA, std::string("rbs_analyse_device: ") + cudaGetErrorString(e));
+    }
+    rbs_plan *P = new (std::nothrow) rbs_plan();
+    if (!P) return fail(RBS_ERR_NOMEM, "rbs_analyse: out of host memory");
+    std::string err;
+    int rc;
+    try {
+        // validation, level sets, reordering and the processing-order CSR on
+        // the device; the execution layout on the host
+        auto t0 = std::chrono::steady_clock::now();
+        rc = rbs::device_analyse(P->p, d_ptr, d_idx, d_val, n, nnz, fmt, substitution, err);
+        P->p.analyse_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        P->p.device_analyse_ms = P->p.analyse_ms;
+        if (rc == RBS_OK) rc = rbs::analyse_after_levels(P->p, n, nnz, substitution, lv, o, err);
+        if (rc == RBS_OK && !o.host_only) rc = rbs::device_build(P->p, err);
+        if (rc == RBS_OK && !o.host_only && o.select == RBS_SELECT_TUNE) rc = rbs::device_tune(P->p, err);
+    } catch (const std::bad_alloc &) {
+        rc = RBS_ERR_NOMEM;
+        err = "rbs_analyse: out of host memory";
+    }
+    if (rc != RBS_OK) {
+        rbs::device_free(P->p);
+        delete P;
+        return fail(rc, err);
+    }
+    *plan = P;
+    set_error("");
+    return RBS_OK;
 }
 
 int rbs_batch_analyse(int count, const int *const *ptr, const int *const *idx, const double *const *val,

@@ -80,6 +80,7 @@ struct Plan {
     int n = 0, nnz = 0, lv = 0, sub = 0, nlevel = 0, sum_block = 0, step = 0;
     rbs_options opt{};
     double analyse_ms = 0;
+    double device_analyse_ms = 0;  // part of analyse_ms spent in the device analysis (0: host analysis)
 
     // inputs kept for the reference-format export (CSC, caller's entry order)
     std::vector<int> in_cp, in_ri;
@@ -109,6 +110,9 @@ struct Plan {
     // original-row offsets of independent systems (batched plans); empty
     // for a single system
     std::vector<int> seg_rows;
+    // the reference's reordered CSC (utils_reordering.h:102-210) as computed
+    // by the device analysis (rbs_analyse_device); empty after a host analysis
+    std::vector<int> dev_reorder_cp, dev_reorder_ri;
     // full processing-order CSR (with diagonal) for FP64 residuals
     std::vector<int> full_rp, full_col;
     std::vector<double> full_val;
@@ -123,6 +127,15 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
 int export_reference(const Plan &P, const std::string &name, std::vector<int> &iv, std::vector<double> &dv,
                      bool &is_double, std::string &err);
 int auto_lv(int m, int device_id);
+
+// dev_analysis.cu: validation, findlevel, reordering and the processing-order
+// CSR on the device (fills in_*, bfs_*, nlevel, label, perm, full_*, dev_reorder_*)
+int device_analyse(Plan &P, const int *d_ptr, const int *d_idx, const double *d_val, int n, int nnz, int fmt,
+                   int substitution, std::string &err);
+// analysis.cpp: the layout steps after the level sets, from the fields
+// device_analyse filled
+int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, const rbs_options &opt, std::string &err,
+                         const std::vector<int> *seg_rows = nullptr);
 
 // solve.cu
 int device_build(Plan &P, std::string &err);
