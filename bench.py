@@ -279,6 +279,36 @@ def side_structures(dev, flush, args):
     return sweep
 
 
+def side_analysis(dev, args):
+    """Analysis time: host (rbs_analyse on host arrays) against device
+    (rbs_analyse_device on device arrays: level sets, reordering and the
+    processing-order CSR on the GPU, the execution layout on the host); the
+    integer outputs are identical (tests/test_device_analysis_gpu.py)."""
+    import torch
+
+    import rbs
+
+    out = {}
+    for kind in ("c1a", "c1b", "c1c", "c2r"):
+        s2 = make_system(kind, rbs.FORWARD)
+        t0 = time.perf_counter()
+        ph = rbs.analyse(s2["cp"], s2["ri"], s2["cv"], substitution=rbs.FORWARD, lv=-1, opts=rbs.options(host_only=1))
+        host_s = time.perf_counter() - t0
+        d = [torch.tensor(s2[k], device=dev) for k in ("cp", "ri", "cv")]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pd = rbs.analyse_device(d[0], d[1], d[2], s2["n"], s2["nnz"], substitution=rbs.FORWARD, lv=-1,
+                                opts=rbs.options(host_only=1))
+        dev_s = time.perf_counter() - t0
+        same = bool((ph.export("levelItem") == pd.export("levelItem")).all() and
+                    (ph.export("recblock_Index") == pd.export("recblock_Index")).all())
+        out[kind] = {"n": s2["n"], "nnz": s2["nnz"], "nlevel": ph.info().nlevel,
+                     "host_ms": 1000 * host_s, "device_path_ms": 1000 * dev_s,
+                     "device_part_ms": float(pd.export("analyse_ms")[1]), "identical": same}
+        del ph, pd, d
+    return out
+
+
 def side_mixed(dev, flush, args):
     """FP32 sweeps + FP64 refinement against the plain FP64 solve on the
     2D-Laplacian factor, the power-law factor and the n = 4M Poisson(10)
@@ -391,11 +421,12 @@ def serving_factors(count=64, seed=404):
     return out
 
 
-def side_serving(dev, args, n_requests=1500, loads=(1000, 10000, 50000)):
+def side_serving(dev, args, n_requests=1500, loads=(200, 1000, 10000, 50000), batch_rhs=32):
     """Poisson request arrivals over 64 device-resident factors; each request
     carries 1-16 RHS; the server batches across and within factors and runs
-    FP32 sweeps + FP64 refinement.  The plain arm serves the same arrivals
-    one request at a time with an FP64 solve (host arrays in and out)."""
+    FP32 sweeps + FP64 refinement.  Baselines: the same arrivals served one
+    request at a time with one FP64 solve of its k columns (host arrays in
+    and out), and the plain FP64 single-RHS path (one solve per column)."""
     import threading
 
     import rbs
@@ -409,7 +440,8 @@ def side_serving(dev, args, n_requests=1500, loads=(1000, 10000, 50000)):
     Bh = [rbs.gen_uniform(11000 + i, 16 * n).reshape(16, n) for i, n in enumerate(ns)]
     Xh = [np.empty((16, n)) for n in ns]
     res = {"factors": 64, "rows": int(sum(ns)), "nnz": int(sum(len(L[1]) for L in facs)), "analyse_s": t_an,
-           "requests_per_load": n_requests, "rhs_per_request": "uniform 1..16", "loads": {}}
+           "requests_per_load": n_requests, "rhs_per_request": "uniform 1..16", "max_batch_rhs": batch_rhs,
+           "hbm_budget_gb": 150, "loads": {}}
 
     def schedule(rate):
         gaps = rng.exponential(1.0 / rate, n_requests)
@@ -430,7 +462,18 @@ def side_serving(dev, args, n_requests=1500, loads=(1000, 10000, 50000)):
         span = time.perf_counter() - t_start
         plain[rate] = {"p50_ms": 1000 * float(np.percentile(lat, 50)), "p99_ms": 1000 * float(np.percentile(lat, 99)),
                        "solves_per_s": float(ks.sum()) / span, "requests_per_s": n_requests / span}
-    srv = rbs.Server(150 << 30, max_batch_rhs=16)
+    # plain FP64 single-RHS path (one solve per right-hand side, host arrays),
+    # on the first requests of the 1000 req/s schedule, back to back
+    arr, fid, ks = scheds[loads[1] if len(loads) > 1 else loads[0]]
+    t_start = time.perf_counter()
+    nsol = 0
+    for f, k in zip(fid[:200], ks[:200]):
+        for c in range(int(k)):
+            plans[f].solve_host(Bh[f][c], k=1, x=Xh[f][c])
+            nsol += 1
+    single = nsol / (time.perf_counter() - t_start)
+    res["plain_fp64_single_rhs"] = {"solves_per_s": single, "sample": "first 200 requests, one solve per RHS"}
+    srv = rbs.Server(150 << 30, max_batch_rhs=batch_rhs)
     old_si = sys.getswitchinterval()
     sys.setswitchinterval(1e-4)  # the submit loop and the waiter share the interpreter
     for p in plans:
@@ -471,6 +514,7 @@ def side_serving(dev, args, n_requests=1500, loads=(1000, 10000, 50000)):
                              "mean_batch_rhs": st.mean_batch_rhs, "batches": st.batches},
             "plain_fp64": plain[rate]}
         res["loads"][str(rate)]["x_plain_fp64"] = float(ks.sum()) / span / plain[rate]["solves_per_s"]
+        res["loads"][str(rate)]["x_plain_fp64_single_rhs"] = float(ks.sum()) / span / single
     # accuracy: every factor once, b = L x_true, served mixed vs x_true
     import scipy.sparse as sp
     worst = 0.0
@@ -628,6 +672,7 @@ def run_ours(args):
         del plan
         line["sweep_config1"] = side_structures(dev, flush, args)
         line["config2_mixed"] = side_mixed(dev, flush, args)
+        line["analysis_host_vs_device"] = side_analysis(dev, args)
     if not args.no_batch and world == 1:
         line["config3_batched_512"] = side_batched(dev, args)
     if not args.no_serve and world == 1:
