@@ -900,8 +900,9 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
     }
     // 10. level-ELL layout of level triangles with narrow levels (<= 1024
     //     rows) and short rows (<= 4 entries): the cp.async-staged kernel
-    //     (level_ca.cuh).  Per level: lo, ELL width, pool offset; entries
-    //     column-major inside the level.
+    //     (level_ca.cuh).  Per level a table entry {lo, off, w, 0}; the block's
+    //     ELL width W in {1, 2, 4}; entry j of row lo+i at off + i*W + j
+    //     (row-major, padding column -1), blocks start on a 4-entry boundary.
     P.ca_tab.clear();
     P.ca_col.clear();
     P.ca_val.clear();
@@ -916,26 +917,28 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
             for (int r = lvp[l]; r < lvp[l + 1]; ++r) wmax = std::max(wmax, rp[r + 1] - rp[r]);
         }
         if (!ok || wmax > 4) continue;
+        const int W = wmax <= 1 ? 1 : wmax <= 2 ? 2 : 4;
         B.ca_ok = 1;
-        B.ca_w = wmax <= 1 ? 1 : wmax <= 2 ? 2 : 4;
+        B.ca_w = W;
+        while (P.ca_col.size() % 4) {
+            P.ca_col.push_back(-1);
+            P.ca_val.push_back(0.0);
+        }
         B.ca_tab_off = (long long)P.ca_tab.size();
         B.ca_lo = (long long)P.ca_col.size();
         for (int l = 0; l < B.nlv; ++l) {
             const int lo = lvp[l], w = lvp[l + 1] - lo;
-            int wl = 0;
-            for (int r = lo; r < lo + w; ++r) wl = std::max(wl, rp[r + 1] - rp[r]);
-            const long long off = (long long)P.ca_col.size() - B.ca_lo;
-            P.ca_tab.insert(P.ca_tab.end(), {lo, wl, (int)off});
-            P.ca_col.resize(P.ca_col.size() + (size_t)wl * w, -1);
-            P.ca_val.resize(P.ca_val.size() + (size_t)wl * w, 0.0);
-            for (int i = 0; i < w; ++i)
-                for (int j = 0; j < rp[lo + i + 1] - rp[lo + i]; ++j) {
-                    const size_t dst = (size_t)(B.ca_lo + off + (long long)j * w + i);
-                    P.ca_col[dst] = P.col_pool[rp[lo + i] + j];
-                    P.ca_val[dst] = P.val_pool[rp[lo + i] + j];
-                }
+            P.ca_tab.insert(P.ca_tab.end(), {lo, (int)((long long)lo * W), w, 0});
         }
-        P.ca_tab.push_back(B.m);
+        P.ca_tab.insert(P.ca_tab.end(), {B.m, (int)((long long)B.m * W), 0, 0});
+        P.ca_col.resize(P.ca_col.size() + (size_t)B.m * W, -1);
+        P.ca_val.resize(P.ca_val.size() + (size_t)B.m * W, 0.0);
+        for (int r = 0; r < B.m; ++r)
+            for (int j = 0; j < rp[r + 1] - rp[r]; ++j) {
+                const size_t dst = (size_t)(B.ca_lo + (long long)r * W + j);
+                P.ca_col[dst] = P.col_pool[rp[r] + j];
+                P.ca_val[dst] = P.val_pool[rp[r] + j];
+            }
         B.ca_hi = (long long)P.ca_col.size();
     }
     if (P.ell_col.size() > (size_t)0x7fffffff || P.ca_col.size() > (size_t)0x7fffffff) {

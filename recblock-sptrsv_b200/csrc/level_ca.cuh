@@ -11,9 +11,11 @@
 // is on chip when the level comes up.  A thread only reads what it copied
 // itself (cp.async.wait_group), so staging needs no extra synchronisation.
 //
-// Layout (host-built, per level l): rows [lo_l, lo_l + w_l), ELL width W_l,
-// entries column-major at off_l: column of entry j of row lo_l+i at
-// col[off_l + j*w_l + i] (padding -1), so a level's loads are coalesced.
+// Layout (host-built): per level l a table entry {lo, off, w, 0}: rows
+// [lo, lo + w) of the block; the block's ELL width W (1, 2 or 4) is fixed,
+// entry j of row lo+i at col/val[off + i*W + j] (row-major, padding column
+// -1), so a thread stages its row's columns and values with one or two
+// 4-16 byte copies and the level's loads are coalesced.
 // Dependencies within the last XW rows come from the window; older ones
 // from x in global memory (written by this CTA before an earlier barrier).
 #pragma once
@@ -24,15 +26,15 @@ namespace rbs {
 
 constexpr int CA_ROWS = 1024;  // rows per level (= threads)
 constexpr int CA_XW = 4096;    // x window (rows)
-constexpr int CA_TAB = 6144;   // ints of the level table staged in shared memory (3 per level)
+constexpr int CA_TAB = 6144;   // ints of the level table staged in shared memory (4 per level)
 
 struct CaDesc {
-    const int *col;   // level-ELL columns (block-local), padding -1
+    const int *col;   // row-major level-ELL columns (block-local), padding -1
     const void *val;  // level-ELL values
     const void *inv;  // inverse diagonal of the block's rows
     const void *b;    // right-hand side of the block's rows
     void *x;          // solution of the block's rows
-    const int *lvl;   // per level: lo, W, off  (3 ints), plus lo of the end (nlv*3 + 1 ints)
+    const int *lvl;   // per level: lo, off, w, 0 (4 ints), then {m, 0, 0, 0}
     int m, nlv, pad0, pad1;
 };
 
@@ -54,6 +56,10 @@ __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
                  : "memory");
 }
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -63,6 +69,18 @@ template <typename VT>
 __device__ __forceinline__ void cp_async_v(VT *dst, const VT *src) {
     if (sizeof(VT) == 8) cp_async8(dst, src);
     else cp_async4(dst, src);
+}
+// `bytes` (4, 8, 16 or 32) contiguous bytes, both ends aligned to min(bytes, 16)
+template <int BYTES>
+__device__ __forceinline__ void cp_async_n(void *dst, const void *src) {
+    if constexpr (BYTES == 4) cp_async4(dst, src);
+    else if constexpr (BYTES == 8) cp_async8(dst, src);
+    else if constexpr (BYTES == 16) cp_async16(dst, src);
+    else {
+        static_assert(BYTES == 32, "row segment of 4, 8, 16 or 32 bytes");
+        cp_async16(dst, src);
+        cp_async16(static_cast<char *>(dst) + 16, static_cast<const char *>(src) + 16);
+    }
 }
 
 template <typename VT, int W, int S>
@@ -77,30 +95,28 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
     VT *xs = reinterpret_cast<VT *>(sm + Lay::xw_off);
     int *tab = reinterpret_cast<int *>(sm + Lay::tab_off);
     const int tid = threadIdx.x;
-    const int ntab = 3 * d.nlv + 1;
+    const int ntab = 4 * (d.nlv + 1);
     const bool in_smem = ntab <= CA_TAB;
     if (in_smem)
         for (int i = tid; i < ntab; i += blockDim.x) tab[i] = d.lvl[i];
     __syncthreads();
-    const int *lt = in_smem ? tab : d.lvl;
+    const int4 *lt = reinterpret_cast<const int4 *>(in_smem ? tab : d.lvl);
 
     // stage the row data of level l for this thread (one commit group per level)
     auto stage = [&](int l) {
         if (l < d.nlv) {
-            const int lo = lt[3 * l], wl = lt[3 * l + 1], off = lt[3 * l + 2];
-            const int w = lt[3 * l + 3] - lo;  // rows of the level
-            if (tid < w) {
+            const int4 e = lt[l];  // lo, off, w
+            if (tid < e.z) {
                 unsigned char *st = sm + (size_t)(l % S) * Lay::stage_bytes;
                 int *cs = reinterpret_cast<int *>(st);
                 VT *vs = reinterpret_cast<VT *>(st + Lay::col_bytes);
                 VT *is = reinterpret_cast<VT *>(st + Lay::col_bytes + Lay::val_bytes);
                 VT *bs = is + CA_ROWS;
-                for (int j = 0; j < wl; ++j) {
-                    cp_async4(cs + j * CA_ROWS + tid, d.col + off + (long long)j * w + tid);
-                    cp_async_v<VT>(vs + j * CA_ROWS + tid, valp + off + (long long)j * w + tid);
-                }
-                cp_async_v<VT>(is + tid, invp + lo + tid);
-                cp_async_v<VT>(bs + tid, bp + lo + tid);
+                const long long o = (long long)e.y + (long long)tid * W;
+                cp_async_n<4 * W>(cs + tid * W, d.col + o);
+                cp_async_n<(int)sizeof(VT) * W>(vs + tid * W, valp + o);
+                cp_async_v<VT>(is + tid, invp + e.x + tid);
+                cp_async_v<VT>(bs + tid, bp + e.x + tid);
             }
         }
         cp_async_commit();
@@ -108,27 +124,25 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
 
 #pragma unroll 1
     for (int l = 0; l < S - 1; ++l) stage(l);
+    int lo = 0;
 #pragma unroll 1
     for (int l = 0; l < d.nlv; ++l) {
         stage(l + S - 1);             // its stage held level l-1, finished at the last barrier
         cp_async_wait<S - 1>();       // this thread's copies of level l have landed
-        const int lo = lt[3 * l], wl = lt[3 * l + 1];
-        const int hi = lt[3 * l + 3];
+        const int hi = lt[l + 1].x;
         if (tid < hi - lo) {
             const unsigned char *st = sm + (size_t)(l % S) * Lay::stage_bytes;
-            const int *cs = reinterpret_cast<const int *>(st);
-            const VT *vs = reinterpret_cast<const VT *>(st + Lay::col_bytes);
+            const int *cs = reinterpret_cast<const int *>(st) + tid * W;
+            const VT *vs = reinterpret_cast<const VT *>(st + Lay::col_bytes) + tid * W;
             const VT *is = reinterpret_cast<const VT *>(st + Lay::col_bytes + Lay::val_bytes);
             const VT *bs = is + CA_ROWS;
             VT sum = 0;
 #pragma unroll
             for (int j = 0; j < W; ++j) {
-                if (j < wl) {
-                    const int c = cs[j * CA_ROWS + tid];
-                    if (c >= 0) {
-                        const VT xv = c >= hi - CA_XW ? xs[c & (CA_XW - 1)] : x[c];
-                        sum += vs[j * CA_ROWS + tid] * xv;
-                    }
+                const int c = cs[j];
+                if (c >= 0) {
+                    const VT xv = c >= hi - CA_XW ? xs[c & (CA_XW - 1)] : x[c];
+                    sum += vs[j] * xv;
                 }
             }
             const int r = lo + tid;
@@ -136,6 +150,7 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
             xs[r & (CA_XW - 1)] = xv;
             x[r] = xv;
         }
+        lo = hi;
         __syncthreads();
     }
     cp_async_wait<0>();
