@@ -1070,6 +1070,23 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
         iv = {LC_XW, LC_NB, LC_D, LC_RMAX, LC_T, LC_RING, LC_FMAX, LC_HDR_INTS};
         return RBS_OK;
     }
+    if (name == "ca_tab") return put(P.ca_tab);
+    if (name == "ca_col") return put(P.ca_col);
+    if (name == "ca_val") {
+        is_double = true;
+        dv = P.ca_val;
+        return RBS_OK;
+    }
+    if (name == "ca_block") {  // per block: table offset, first entry, ELL width (-1: no level-ELL layout)
+        iv.assign(3 * sum, -1);
+        for (int b = 0; b < sum; ++b)
+            if (P.blocks[b].ca_ok) {
+                iv[3 * b] = (int)P.blocks[b].ca_tab_off;
+                iv[3 * b + 1] = (int)P.blocks[b].ca_lo;
+                iv[3 * b + 2] = P.blocks[b].ca_w;
+            }
+        return RBS_OK;
+    }
     if (name == "lc_tab") return put(P.lc_tab);
     if (name == "lc_segs") return put(P.lc_segs);
     if (name == "lc_rec64" || name == "lc_rec32") {  // 16-byte-aligned words, returned as int32

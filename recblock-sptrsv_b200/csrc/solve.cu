@@ -320,6 +320,7 @@ int ca_descs(Plan &P, CaDesc *&out, std::string &err) {
     out = dd;
     int rc;
     if ((rc = ca_attr<VT, 1, 4>(err)) || (rc = ca_attr<VT, 2, 4>(err)) || (rc = ca_attr<VT, 4, 2>(err))) return rc;
+
     return RBS_OK;
 }
 
@@ -482,12 +483,14 @@ int launch_blocks(Plan &P, std::string &err) {
                                                                    Pools<VT>::lcrec(D), sizeof(VT) == 4 ? 1 : 0, bb,
                                                                    xx, D.lc_queue + ti, D.status, limit);
                 } else if (K == 1 && B.lvl_var == LVL_CA && B.ca_ok) {
+                    // one thread per row of the widest level: no idle warps at the barriers
+                    const int nt = std::min(1024, std::max(32, (B.maxwidth + 31) / 32 * 32));
                     if (B.ca_w == 1)
-                        k_tri_level_ca<VT, 1, 4><<<1, 1024, CaLayout<VT, 1, 4>::total, st>>>(cdescs + cti);
+                        k_tri_level_ca<VT, 1, 4><<<1, nt, CaLayout<VT, 1, 4>::total, st>>>(cdescs + cti);
                     else if (B.ca_w == 2)
-                        k_tri_level_ca<VT, 2, 4><<<1, 1024, CaLayout<VT, 2, 4>::total, st>>>(cdescs + cti);
+                        k_tri_level_ca<VT, 2, 4><<<1, nt, CaLayout<VT, 2, 4>::total, st>>>(cdescs + cti);
                     else
-                        k_tri_level_ca<VT, 4, 2><<<1, 1024, CaLayout<VT, 4, 2>::total, st>>>(cdescs + cti);
+                        k_tri_level_ca<VT, 4, 2><<<1, nt, CaLayout<VT, 4, 2>::total, st>>>(cdescs + cti);
                 } else if (K == 1 && B.lvl_var == LVL_CSF && B.ell_ok) {
                     k_tri_cta_syncfree<VT><<<1, 1024, CsfLayout<VT>::total, st>>>(edescs + eti, D.status, limit);
                 } else {

@@ -226,7 +226,7 @@ class Plan:
     def export(self, name: str) -> np.ndarray:
         cnt = ctypes.c_longlong()
         _check(lib.rbs_plan_export(self._h, name.encode(), None, 0, ctypes.byref(cnt)))
-        dt = np.float64 if name in ("recblock_Val", "block_bytes", "ell_val", "inv_diag", "analyse_ms") else np.int32
+        dt = np.float64 if name in ("recblock_Val", "block_bytes", "ell_val", "inv_diag", "analyse_ms", "ca_val") else np.int32
         out = np.empty(max(cnt.value, 1), dtype=dt)
         _check(lib.rbs_plan_export(self._h, name.encode(), out.ctypes.data_as(ctypes.c_void_p), cnt.value,
                                    ctypes.byref(cnt)))
