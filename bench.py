@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-sweep", action="store_true", help="skip the structure/variant side measurements")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-system batched measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
+    ap.add_argument("--case", default="c1a", choices=["c1a", "c1b", "c1c", "c2r", "c0"],
+                    help="structure of the timed solve (profiling runs; the benchmark line is c1a)")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, side measurements and the CPU baseline "
                                                                "(short runs for profilers)")
     return ap.parse_args()
@@ -578,7 +580,7 @@ def run_ours(args):
         return float(t.item())
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    sysm = make_system("c1a", rbs.FORWARD)
+    sysm = make_system(args.case, rbs.FORWARD)
     plan = rbs.analyse(sysm["cp"], sysm["ri"], sysm["cv"], substitution=rbs.FORWARD, lv=-1,
                        opts=rbs.options(max_rhs=32))
     info = plan.info()
@@ -622,7 +624,7 @@ def run_ours(args):
     if args.no_extras:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "solves/s", "ms_per_step": ms_per_step,
-                              "roofline": roofline, "note": "--no-extras run (profiling)"}))
+                              "case": args.case, "roofline": roofline, "note": "--no-extras run (profiling)"}))
         if world > 1:
             dist.destroy_process_group()
         return
@@ -650,7 +652,8 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded stand-in for SuiteSparse inputs)",
-        "config": {"workload": WORKLOAD, "global_batch": world, "parallelism": f"replicas{world}",
+        "config": {"workload": WORKLOAD if args.case == "c1a" else args.case, "global_batch": world,
+                   "parallelism": f"replicas{world}",
                    "l2": "flushed before every timed solve (256 MB write)", "lv": info.lv,
                    "kernels": {rbs.KERNEL_NAMES[i]: info.kernels[i] for i in range(7) if info.kernels[i]}},
         "gb_per_s": useful / (ms_per_step / 1000) / 1e9,
