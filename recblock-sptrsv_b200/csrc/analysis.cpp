@@ -436,6 +436,10 @@ static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &le
     }
 }
 
+int host_bfs_levels(const int *cp, const int *ri, int m, std::vector<int> &levelPtr, std::vector<int> &item) {
+    return bfs_levels(cp, ri, m, levelPtr, item);
+}
+
 int auto_lv(int m, int device_id) {
     // main.cu:245-254: smallest li >= 1 with m / 2^(li+1) below the wave size
     int li;
@@ -1061,9 +1065,9 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
         }
         return put(name == "reordered_colptr" ? ncp : nri);
     }
-    if (name == "analyse_ms") {  // total analysis, of which on the device
+    if (name == "analyse_ms") {  // total analysis, of which on the device, level search on the device (1/0)
         is_double = true;
-        dv = {P.analyse_ms, P.device_analyse_ms};
+        dv = {P.analyse_ms, P.device_analyse_ms, (double)P.device_bfs};
         return RBS_OK;
     }
     if (name == "lc_consts") {  // the layout constants the records were built for

@@ -39,9 +39,14 @@ namespace rbs {
 namespace {
 
 constexpr int BFS_T = 1024;
-constexpr int BFS_MAXF = 8192;  // widest level the single-CTA kernel takes
+constexpr int BFS_MAXF = 4096;   // widest level the single-CTA kernel takes (rows)
+constexpr int BFS_EMAX = 16384;  // and column entries
+constexpr int BFS_SMEM = (BFS_MAXF + 1 + 2 * BFS_EMAX) * 4;
 
-enum { BFS_DONE = 1, BFS_BIG = 2, BFS_STUCK = 3 };
+enum { BFS_DONE = 1, BFS_BIG = 2, BFS_STUCK = 3, BFS_PAUSED = 4 };
+constexpr int BFS_PAUSE = 2048;        // levels per launch of the single-CTA kernel
+constexpr int BFS_NARROW = 16;         // mean rows per level below which ...
+constexpr int BFS_HOST_ROWS = 65536;   // ... and with more rows than this left, the host takes over
 enum { VAL_PTR = 1, VAL_NODIAG, VAL_DIAGPOS, VAL_ZERODIAG, VAL_OUTSIDE, VAL_DUPDIAG, VAL_INDEX };
 
 #define DCK(call)                                                                    \
@@ -114,88 +119,122 @@ __global__ void k_root_scatter(const int *__restrict__ flag, const int *__restri
         if (flag[i]) item[pos[i]] = i;
 }
 
-// Narrow levels: one CTA walks level after level until the graph is done,
-// a level is wider than maxf, or a level is empty (no progress).  deg, key
-// and item are read with ld.global.cg: other threads of this CTA changed them
-// through L2 (atomics, st.global.cg) since the last barrier.
+// Block-wide exclusive scan of v[0, n) in place (n <= BFS_EMAX), returns the
+// total; every thread of the CTA calls it.
+__device__ int block_exclusive_scan(int *v, int n, int *wsum) {
+    const int tid = threadIdx.x;
+    const int per = (n + BFS_T - 1) / BFS_T;
+    const int a = min(n, tid * per), z = min(n, a + per);
+    int run = 0;
+    for (int t = a; t < z; ++t) run += v[t];
+    int incl = run;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((tid & 31) >= o) incl += u;
+    }
+    if ((tid & 31) == 31) wsum[tid >> 5] = incl;
+    __syncthreads();
+    if (tid < 32) {
+        int w = tid < BFS_T / 32 ? wsum[tid] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, w, o);
+            if (tid >= o) w += u;
+        }
+        if (tid < BFS_T / 32) wsum[tid] = w;
+    }
+    __syncthreads();
+    int base = incl - run + ((tid >> 5) ? wsum[(tid >> 5) - 1] : 0);
+    const int total = wsum[BFS_T / 32 - 1];
+    for (int t = a; t < z; ++t) {
+        const int c = v[t];
+        v[t] = base;
+        base += c;
+    }
+    __syncthreads();
+    return total;
+}
+
+// Narrow levels: one CTA walks level after level until the graph is done, a
+// level has more than BFS_MAXF rows or BFS_EMAX column entries, maxlev
+// levels were done in this launch, or a level is empty (no progress).  The
+// level's (parent, entry) pairs are spread over all threads: the parents'
+// column lengths are scanned, every thread takes entries and finds its
+// parent by binary search.  deg, key and item are read with ld.global.cg:
+// other threads of this CTA changed them through L2 (atomics,
+// st.global.cg) since the last barrier.
 __global__ void __launch_bounds__(BFS_T) k_bfs_small(const int *__restrict__ cp, const int *__restrict__ ri, int n,
-                                                   int *deg, int *key, int *item, int *lptr, int *meta, int maxf) {
-    __shared__ int cnt[BFS_MAXF];
+                                                   int *deg, int *key, int *item, int *lptr, int *meta, int maxlev) {
+    extern __shared__ int bfs_sm[];
+    int *cst = bfs_sm;                  // [BFS_MAXF + 1] column starts of the level's parents
+    int *ent = cst + BFS_MAXF + 1;      // [BFS_EMAX] row of each entry (-1: diagonal / not a child)
+    int *pos = ent + BFS_EMAX;          // [BFS_EMAX] child flags, then their scan
     __shared__ int wsum[BFS_T / 32];
     const int tid = threadIdx.x;
     int nl = meta[0];
     int lo = lptr[nl - 1], hi = lptr[nl];
-    int status = 0;
+    int status = 0, done_here = 0;
     for (;;) {
         if (hi >= n) { status = BFS_DONE; break; }
         const int f = hi - lo;
         if (f == 0) { status = BFS_STUCK; break; }
-        if (f > maxf) { status = BFS_BIG; break; }
-        // expand
+        if (f > BFS_MAXF) { status = BFS_BIG; break; }
+        if (done_here >= maxlev) { status = BFS_PAUSED; break; }
         for (int t = tid; t < f; t += BFS_T) {
             const int p = __ldcg(item + lo + t);
-            for (int k = cp[p]; k < cp[p + 1]; ++k) {
-                const int r = ri[k];
-                if (r == p) continue;
-                atomicMax(key + r, lo + t);
+            cst[t] = cp[p + 1] - cp[p];
+        }
+        __syncthreads();
+        const int E = block_exclusive_scan(cst, f, wsum);
+        if (E > BFS_EMAX) { status = BFS_BIG; break; }
+        if (tid == 0) cst[f] = E;
+        __syncthreads();
+        // expand: every entry decrements its row and raises the row's key
+        for (int e = tid; e < E; e += BFS_T) {
+            int a = 0, z = f;  // parent t: cst[t] <= e < cst[t+1]
+            while (z - a > 1) {
+                const int mid = (a + z) >> 1;
+                if (cst[mid] <= e) a = mid;
+                else z = mid;
+            }
+            const int p = __ldcg(item + lo + a);
+            const int r = ri[cp[p] + (e - cst[a])];
+            if (r == p) {
+                ent[e] = -1;
+                __stcg(deg + p, 0);  // expanded: never a child again
+            } else {
+                ent[e] = r;
+                atomicMax(key + r, lo + a);
                 atomicSub(deg + r, 1);
             }
-            __stcg(deg + p, 0);  // expanded: never a child again
         }
         __syncthreads();
-        // count children per parent
-        for (int t = tid; t < f; t += BFS_T) {
-            const int p = __ldcg(item + lo + t);
-            int c = 0;
-            for (int k = cp[p]; k < cp[p + 1]; ++k) {
-                const int r = ri[k];
-                if (r != p && __ldcg(deg + r) == 1 && __ldcg(key + r) == lo + t) ++c;
+        // an entry is a child link when its row reached deg 1 and its parent
+        // is the one with the row's key (the last in serial order)
+        for (int e = tid; e < E; e += BFS_T) {
+            const int r = ent[e];
+            int flag = 0;
+            if (r >= 0 && __ldcg(deg + r) == 1) {
+                int a = 0, z = f;
+                while (z - a > 1) {
+                    const int mid = (a + z) >> 1;
+                    if (cst[mid] <= e) a = mid;
+                    else z = mid;
+                }
+                flag = __ldcg(key + r) == lo + a;
             }
-            cnt[t] = c;
+            pos[e] = flag;
         }
         __syncthreads();
-        // exclusive scan of cnt[0, f): each thread a contiguous run
-        const int per = (f + BFS_T - 1) / BFS_T;
-        const int a = min(f, tid * per), z = min(f, a + per);
-        int run = 0;
-        for (int t = a; t < z; ++t) run += cnt[t];
-        int incl = run;  // inclusive scan of runs across the CTA
-        for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, incl, o);
-            if ((tid & 31) >= o) incl += v;
-        }
-        if ((tid & 31) == 31) wsum[tid >> 5] = incl;
-        __syncthreads();
-        if (tid < 32) {
-            int w = tid < BFS_T / 32 ? wsum[tid] : 0;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_up_sync(0xffffffffu, w, o);
-                if (tid >= o) w += v;
-            }
-            if (tid < BFS_T / 32) wsum[tid] = w;
-        }
-        __syncthreads();
-        int base = incl - run + ((tid >> 5) ? wsum[(tid >> 5) - 1] : 0);
-        const int total = wsum[BFS_T / 32 - 1];
-        for (int t = a; t < z; ++t) {
-            const int c = cnt[t];
-            cnt[t] = base;
-            base += c;
-        }
-        __syncthreads();
-        // write children in parent order, each parent's in column order
-        for (int t = tid; t < f; t += BFS_T) {
-            const int p = __ldcg(item + lo + t);
-            int o = hi + cnt[t];
-            for (int k = cp[p]; k < cp[p + 1]; ++k) {
-                const int r = ri[k];
-                if (r != p && __ldcg(deg + r) == 1 && __ldcg(key + r) == lo + t) __stcg(item + o++, r);
-            }
-        }
+        // children in (parent, column) order = entry order
+        for (int e = tid; e < E; e += BFS_T) ent[e] = pos[e] ? ent[e] : -1;
+        const int total = block_exclusive_scan(pos, E, wsum);
+        for (int e = tid; e < E; e += BFS_T)
+            if (ent[e] >= 0) __stcg(item + hi + pos[e], ent[e]);
         __syncthreads();
         lo = hi;
         hi += total;
         ++nl;
+        ++done_here;
         if (tid == 0) lptr[nl] = hi;
     }
     if (tid == 0) {
@@ -472,8 +511,10 @@ int device_analyse(Plan &P, const int *d_ptr, const int *d_idx, const double *d_
         DCK(cudaStreamSynchronize(st));
     }
     int nl = 0;
+    P.device_bfs = 1;
+    DCK(cudaFuncSetAttribute(k_bfs_small, cudaFuncAttributeMaxDynamicSharedMemorySize, BFS_SMEM));
     for (;;) {
-        k_bfs_small<<<1, BFS_T, 0, st>>>(cp, ri, n, deg, key, item, lptr, meta, BFS_MAXF);
+        k_bfs_small<<<1, BFS_T, BFS_SMEM, st>>>(cp, ri, n, deg, key, item, lptr, meta, BFS_PAUSE);
         int hm[2];
         DCK(cudaMemcpyAsync(hm, meta, sizeof(hm), cudaMemcpyDeviceToHost, st));
         DCK(cudaStreamSynchronize(st));
@@ -482,6 +523,32 @@ int device_analyse(Plan &P, const int *d_ptr, const int *d_idx, const double *d_
         if (hm[1] == BFS_STUCK) {
             err = "rbs_analyse: level search stuck (dependency cycle)";
             return RBS_ERR_STRUCTURE;
+        }
+        if (hm[1] == BFS_PAUSED) {
+            // a chain-like graph (levels of a few rows each) costs a few L2 round
+            // trips per level here and far less in the host's serial search:
+            // hand the level search to the host (same order, bit for bit)
+            int done_rows = 0;
+            DCK(cudaMemcpyAsync(&done_rows, lptr + nl, sizeof(int), cudaMemcpyDeviceToHost, st));
+            DCK(cudaStreamSynchronize(st));
+            if ((long long)done_rows < (long long)BFS_NARROW * nl && n - done_rows > BFS_HOST_ROWS) {
+                std::vector<int> hcp((size_t)n + 1), hri((size_t)nnz), hptr, hitem;
+                DCK(cudaMemcpyAsync(hcp.data(), cp, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToHost, st));
+                DCK(cudaMemcpyAsync(hri.data(), ri, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToHost, st));
+                DCK(cudaStreamSynchronize(st));
+                const int hl = host_bfs_levels(hcp.data(), hri.data(), n, hptr, hitem);
+                if (hl < 0) {
+                    err = "rbs_analyse: level search stuck (dependency cycle)";
+                    return RBS_ERR_STRUCTURE;
+                }
+                DCK(cudaMemcpyAsync(item, hitem.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st));
+                DCK(cudaMemcpyAsync(lptr, hptr.data(), sizeof(int) * ((size_t)hl + 1), cudaMemcpyHostToDevice, st));
+                DCK(cudaStreamSynchronize(st));
+                nl = hl;
+                P.device_bfs = 0;
+                break;
+            }
+            continue;
         }
         // one wide level with grid-wide kernels
         int lh[2];

@@ -81,6 +81,7 @@ struct Plan {
     rbs_options opt{};
     double analyse_ms = 0;
     double device_analyse_ms = 0;  // part of analyse_ms spent in the device analysis (0: host analysis)
+    int device_bfs = 0;            // 1: the level search itself ran on the device
 
     // inputs kept for the reference-format export (CSC, caller's entry order)
     std::vector<int> in_cp, in_ri;
@@ -132,6 +133,9 @@ int auto_lv(int m, int device_id);
 // CSR on the device (fills in_*, bfs_*, nlevel, label, perm, full_*, dev_reorder_*)
 int device_analyse(Plan &P, const int *d_ptr, const int *d_idx, const double *d_val, int n, int nnz, int fmt,
                    int substitution, std::string &err);
+// analysis.cpp: findlevel's breadth-first search on the host (levelPtr, levelItem;
+// returns the level count or -1 when stuck)
+int host_bfs_levels(const int *cp, const int *ri, int m, std::vector<int> &levelPtr, std::vector<int> &item);
 // analysis.cpp: the layout steps after the level sets, from the fields
 // device_analyse filled
 int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, const rbs_options &opt, std::string &err,

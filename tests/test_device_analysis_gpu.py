@@ -59,6 +59,9 @@ def test_device_analysis_matches_host_at_size(cuda, name, sub):
     for k in ("levelItem", "levelPtr", "perm", "blk_nnz", "method", "nlv", "kernel", "reordered_colptr",
               "reordered_rowidx", "recblock_Ptr", "recblock_Index"):
         np.testing.assert_array_equal(dev.export(k), host.export(k), err_msg=f"{name}: {k}")
+    # the level search ran on the device, except for the chain (one row per
+    # level), which it hands to the host after a few thousand levels
+    assert dev.export("analyse_ms")[2] == (0 if name.startswith("chain") else 1)
     # and the plan built from the device analysis solves
     n = len(A[0]) - 1
     arp, aci, ava = (rp, ci, va) if sub == rbs.FORWARD else oracle.transpose(*A)
