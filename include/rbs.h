@@ -194,6 +194,16 @@ int rbs_plan_export(const rbs_plan *plan, const char *name, void *dst, long long
 
 int rbs_plan_free(rbs_plan *plan);
 
+/* Plan serialisation (no counterpart in the reference, which repeats its
+ * analysis in every process): rbs_plan_save writes the analysis -- level
+ * order, labels, block bounds, kernel choice and every execution layout --
+ * to a file; rbs_plan_load reads it back and, unless opt->host_only, builds
+ * the device state, with no level search, partition or kernel timing.
+ * opt may be NULL (defaults).  A file from another build is rejected
+ * (RBS_ERR_ARG). */
+int rbs_plan_save(const rbs_plan *plan, const char *path);
+int rbs_plan_load(const char *path, const rbs_options *opt, rbs_plan **plan);
+
 /* Per-block device timing (no counterpart in the reference, which times the
  * whole walk with gettimeofday, recblocking_calculate.h:45,164-165).  When
  * enabled, every FP64/FP32 solve records CUDA events around each block's

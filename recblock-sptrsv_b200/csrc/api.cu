@@ -322,6 +322,54 @@ int rbs_plan_block_times(const rbs_plan *plan, double *ms, double *bytes, long l
     return RBS_OK;
 }
 
+int rbs_plan_save(const rbs_plan *plan, const char *path) {
+    if (!plan || !path) return fail(RBS_ERR_ARG, "rbs_plan_save: NULL argument");
+    std::string err;
+    int rc = rbs::plan_save(plan->p, path, err);
+    if (rc) return fail(rc, err);
+    return RBS_OK;
+}
+
+int rbs_plan_load(const char *path, const rbs_options *opt, rbs_plan **plan) {
+    if (!plan || !path) return fail(RBS_ERR_ARG, "rbs_plan_load: NULL argument");
+    *plan = nullptr;
+    rbs_plan *P = new (std::nothrow) rbs_plan();
+    if (!P) return fail(RBS_ERR_NOMEM, "rbs_plan_load: out of host memory");
+    std::string err;
+    int rc;
+    try {
+        rc = rbs::plan_load(P->p, path, err);
+        if (rc == RBS_OK) {
+            // run-time options from the caller; the analysis from the file
+            rbs_options o = P->p.opt;
+            if (opt) {
+                o.device = opt->device;
+                o.host_only = opt->host_only;
+                o.max_rhs = opt->max_rhs < 1 ? 1 : opt->max_rhs;
+                o.mixed = opt->mixed;
+                if (opt->ir_tol > 0) o.ir_tol = opt->ir_tol;
+                if (opt->ir_max_iter > 0) o.ir_max_iter = opt->ir_max_iter;
+                if (opt->spin_limit > 0) o.spin_limit = opt->spin_limit;
+            } else {
+                o.host_only = 0;
+            }
+            P->p.opt = o;
+            if (!o.host_only) rc = rbs::device_build(P->p, err);
+        }
+    } catch (const std::bad_alloc &) {
+        rc = RBS_ERR_NOMEM;
+        err = "rbs_plan_load: out of host memory";
+    }
+    if (rc != RBS_OK) {
+        rbs::device_free(P->p);
+        delete P;
+        return fail(rc, err);
+    }
+    *plan = P;
+    set_error("");
+    return RBS_OK;
+}
+
 int rbs_plan_free(rbs_plan *plan) {
     if (!plan) return RBS_OK;
     rbs::device_free(plan->p);

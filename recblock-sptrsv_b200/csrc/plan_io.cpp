@@ -1,0 +1,165 @@
+// plan_io.cpp -- saving and loading an analysed plan (rbs_plan_save /
+// rbs_plan_load): a warm start for resident factors, e.g. a serving process
+// that restarts.  The file holds the plan's host side (scalars, options,
+// the reference-format inputs kept for export, level order, labels, the
+// execution blocks and every pool) in a versioned binary layout of this
+// build; the device state is rebuilt from it on load.
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "rbs.h"
+#include "rbs_internal.h"
+
+namespace rbs {
+
+namespace {
+
+constexpr char kMagic[8] = {'R', 'B', 'S', 'P', 'L', 'A', 'N', '1'};
+
+struct Writer {
+    FILE *f;
+    bool ok = true;
+    template <typename T>
+    void pod(const T &v) {
+        ok = ok && std::fwrite(&v, sizeof(T), 1, f) == 1;
+    }
+    template <typename T>
+    void vec(const std::vector<T> &v) {
+        const uint64_t n = v.size();
+        pod(n);
+        if (n) ok = ok && std::fwrite(v.data(), sizeof(T), n, f) == n;
+    }
+};
+
+struct Reader {
+    FILE *f;
+    bool ok = true;
+    template <typename T>
+    void pod(T &v) {
+        ok = ok && std::fread(&v, sizeof(T), 1, f) == 1;
+    }
+    template <typename T>
+    void vec(std::vector<T> &v) {
+        uint64_t n = 0;
+        pod(n);
+        if (!ok || n > (1ull << 40) / sizeof(T)) {
+            ok = false;
+            return;
+        }
+        v.resize((size_t)n);
+        if (n) ok = ok && std::fread(v.data(), sizeof(T), n, f) == n;
+    }
+};
+
+// One list of every plan field, used in both directions.
+template <typename IO>
+void fields(IO &io, Plan &P) {
+    io.pod(P.n);
+    io.pod(P.nnz);
+    io.pod(P.lv);
+    io.pod(P.sub);
+    io.pod(P.nlevel);
+    io.pod(P.sum_block);
+    io.pod(P.step);
+    io.pod(P.opt);
+    io.pod(P.analyse_ms);
+    io.pod(P.device_analyse_ms);
+    io.pod(P.device_bfs);
+    io.vec(P.in_cp);
+    io.vec(P.in_ri);
+    io.vec(P.in_va);
+    io.vec(P.bfs_item);
+    io.vec(P.bfs_ptr);
+    io.vec(P.label);
+    io.vec(P.perm);
+    io.vec(P.blocks);
+    io.vec(P.rp_pool);
+    io.vec(P.col_pool);
+    io.vec(P.lvl_pool);
+    io.vec(P.map_pool);
+    io.vec(P.rows_pool);
+    io.vec(P.val_pool);
+    io.vec(P.inv_diag);
+    io.vec(P.band_coef);
+    io.vec(P.band_inv);
+    io.vec(P.ell_col);
+    io.vec(P.ell_val);
+    io.vec(P.ell_chunks);
+    io.vec(P.ca_tab);
+    io.vec(P.ca_col);
+    io.vec(P.ca_val);
+    io.vec(P.lc_rec64);
+    io.vec(P.lc_rec32);
+    io.vec(P.lc_tab);
+    io.vec(P.lc_segs);
+    io.vec(P.seg_rows);
+    io.vec(P.dev_reorder_cp);
+    io.vec(P.dev_reorder_ri);
+    io.vec(P.full_rp);
+    io.vec(P.full_col);
+    io.vec(P.full_val);
+}
+
+// layout signature: a file is read only by a build with the same record sizes
+uint64_t layout_signature() {
+    return ((uint64_t)sizeof(ExecBlock) << 32) ^ ((uint64_t)sizeof(rbs_options) << 16) ^ (uint64_t)sizeof(Plan);
+}
+
+}  // namespace
+
+int plan_save(const Plan &P, const char *path, std::string &err) {
+    FILE *f = std::fopen(path, "wb");
+    if (!f) {
+        err = std::string("rbs_plan_save: cannot open ") + path;
+        return RBS_ERR_ARG;
+    }
+    Writer w{f};
+    w.ok = std::fwrite(kMagic, 1, sizeof(kMagic), f) == sizeof(kMagic);
+    w.pod(layout_signature());
+    fields(w, const_cast<Plan &>(P));
+    const bool ok = w.ok && std::fclose(f) == 0;
+    if (!ok) {
+        err = std::string("rbs_plan_save: write failed: ") + path;
+        return RBS_ERR_ARG;
+    }
+    return RBS_OK;
+}
+
+int plan_load(Plan &P, const char *path, std::string &err) {
+    FILE *f = std::fopen(path, "rb");
+    if (!f) {
+        err = std::string("rbs_plan_load: cannot open ") + path;
+        return RBS_ERR_ARG;
+    }
+    char magic[8] = {0};
+    Reader r{f};
+    r.ok = std::fread(magic, 1, sizeof(magic), f) == sizeof(magic) && std::memcmp(magic, kMagic, sizeof(kMagic)) == 0;
+    uint64_t sig = 0;
+    r.pod(sig);
+    if (!r.ok || sig != layout_signature()) {
+        std::fclose(f);
+        err = std::string("rbs_plan_load: not a plan file of this build: ") + path;
+        return RBS_ERR_ARG;
+    }
+    fields(r, P);
+    std::fclose(f);
+    if (!r.ok) {
+        err = std::string("rbs_plan_load: truncated or corrupt plan file: ") + path;
+        return RBS_ERR_ARG;
+    }
+    // consistency of the sizes the executor relies on
+    const bool sane = P.n > 0 && P.nnz >= P.n && P.sum_block == (int)P.blocks.size() && P.sum_block == 2 * (1 << P.lv) - 1 &&
+                      P.perm.size() == (size_t)P.n && P.full_rp.size() == (size_t)P.n + 1 &&
+                      P.full_col.size() == (size_t)P.nnz && P.inv_diag.size() == (size_t)P.n;
+    if (!sane) {
+        err = std::string("rbs_plan_load: inconsistent plan file: ") + path;
+        return RBS_ERR_ARG;
+    }
+    P.dev = nullptr;
+    return RBS_OK;
+}
+
+}  // namespace rbs

@@ -109,6 +109,7 @@ EXPORTS = [
     "rbs_gen_lower_csr", "rbs_gen_uniform", "rbs_gen_free", "rbs_plan_profile", "rbs_plan_block_times",
     "rbs_sptrsv_csr_noalloc", "rbs_batch_analyse", "rbs_server_create", "rbs_server_add_factor",
     "rbs_server_submit", "rbs_server_wait", "rbs_server_stats_get", "rbs_server_reset_stats", "rbs_server_destroy",
+    "rbs_plan_save", "rbs_plan_load",
 ]
 
 
@@ -138,6 +139,8 @@ def _load():
     lib.rbs_plan_info_get.argtypes = [P, ctypes.POINTER(PlanInfo)]
     lib.rbs_plan_export.argtypes = [P, ctypes.c_char_p, P, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
     lib.rbs_plan_free.argtypes = [P]
+    lib.rbs_plan_save.argtypes = [P, ctypes.c_char_p]
+    lib.rbs_plan_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(Options), ctypes.POINTER(P)]
     lib.rbs_last_error.restype = ctypes.c_char_p
     lib.rbs_auto_lv.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.recblocking_solver_cuda.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_int,
@@ -272,6 +275,10 @@ class Plan:
         _check(lib.rbs_plan_block_times(self._h, _dp(ms), _dp(by), ctypes.byref(solves), nb))
         return ms, by, solves.value
 
+    def save(self, path: str):
+        """rbs_plan_save: the analysis to a file."""
+        _check(lib.rbs_plan_save(self._h, str(path).encode()))
+
     def set_stream(self, stream_ptr: int | None):
         _check(lib.rbs_plan_set_stream(self._h, ctypes.c_void_p(stream_ptr) if stream_ptr else None))
 
@@ -350,6 +357,15 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def load_plan(path: str, opts: Options | None = None) -> Plan:
+    """rbs_plan_load: a saved analysis, device state rebuilt unless opts.host_only."""
+    h = ctypes.c_void_p()
+    _check(lib.rbs_plan_load(str(path).encode(), ctypes.byref(opts) if opts is not None else None, ctypes.byref(h)))
+    n = PlanInfo()
+    _check(lib.rbs_plan_info_get(h, ctypes.byref(n)))
+    return Plan(h, n.n)
 
 
 def analyse_device(ptr, idx, val, n: int, nnz: int, substitution: int = FORWARD, lv: int = -1,
