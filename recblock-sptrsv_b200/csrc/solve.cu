@@ -718,9 +718,11 @@ int device_build(Plan &P, std::string &err) {
     if ((rc = upload(D, D.band_coef, P.band_coef, err))) return rc;
     if ((rc = upload(D, D.band_inv, P.band_inv, err))) return rc;
     {
+        // every triangle with a band layout may run the band scan (the tuner
+        // switches kernels after this point), so size for all of them
         size_t maps = 1, states = 1;
         for (const ExecBlock &B : P.blocks)
-            if (B.tri && B.kernel == RBS_K_BANDSCAN) {
+            if (B.tri && B.band_w > 0) {
                 maps = std::max(maps, (size_t)B.band_nch * (B.band_w * B.band_w + B.band_w));
                 states = std::max(states, (size_t)B.band_nch * B.band_w);
             }

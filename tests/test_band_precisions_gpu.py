@@ -1,0 +1,36 @@
+"""Band-scan triangles in every precision: chosen by the cost model on a
+long chain, and by the tuner on a short one (the tuner picks kernels after
+the device state exists, so the band-scan scratch must already fit)."""
+import numpy as np
+import pytest
+
+import rbs
+from _util import rel_err
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n,select", [(200000, rbs.SELECT_AUTO), (1489, rbs.SELECT_TUNE), (20000, rbs.SELECT_TUNE)])
+@pytest.mark.parametrize("sub", [rbs.FORWARD, rbs.BACKWARD])
+def test_band_scan_precisions(cuda, n, select, sub):
+    import torch
+    rp, ci, va = rbs.gen_lower_csr(rbs.GEN_CHAIN, n=n, chain_bw=4, seed=n + 3)
+    if sub == rbs.FORWARD:
+        A, (arp, aci, ava) = oracle.transpose(rp, ci, va), (rp, ci, va)
+    else:
+        A, (arp, aci, ava) = (rp, ci, va), oracle.transpose(rp, ci, va)
+    plan = rbs.analyse(*A, substitution=sub, lv=-1 if n > 10000 else 0, opts=rbs.options(select=select, max_rhs=4))
+    assert (plan.export("kernel") == rbs.K_BANDSCAN).any()
+    k = 4
+    X = np.stack([rbs.gen_uniform(20 + c, n) for c in range(k)])
+    B = np.stack([oracle.spmv_csr(arp, aci, ava, X[c]) for c in range(k)])
+    Xo = np.stack([oracle.sptrsv_csr(arp, aci, ava, sub, B[c]) for c in range(k)])
+    for kk in (1, k):
+        dB = torch.tensor(B[:kk], device=cuda).reshape(-1)
+        for prec, tol in ((rbs.PREC_FP64, 1e-12), (rbs.PREC_FP32, 1e-4), (rbs.PREC_MIXED, 1e-12)):
+            dX = torch.empty_like(dB)
+            plan.solve(dB, dX, k=kk, prec=prec)
+            got = dX.cpu().numpy().reshape(kk, n)
+            for c in range(kk):
+                assert rel_err(got[c], Xo[c]) <= tol, (kk, prec, c)
