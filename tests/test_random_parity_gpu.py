@@ -64,3 +64,37 @@ def test_random_parity(cuda, seed):
         got = dX.cpu().numpy().reshape(k, n)
         for c in range(k):
             assert rel_err(got[c], Xo[c]) <= tol, (prec, c)
+
+
+@pytest.mark.parametrize("seed", range(10))
+def test_random_batch_parity(cuda, seed):
+    # many systems in one plan (one CTA per system in the level-chunk kernel,
+    # or whatever the selection picks for the block-diagonal triangle)
+    import torch
+    rng = np.random.default_rng(5000 + seed)
+    count = int(rng.integers(2, 12))
+    systems = [random_system(100 * seed + i) for i in range(count)]
+    sub = int(rng.integers(0, 2))
+    select = SELECTS[seed % 3]
+    inputs, csrs = [], []
+    for rp, ci, va in systems:
+        if sub == rbs.FORWARD:
+            inputs.append(oracle.transpose(rp, ci, va))
+            csrs.append((rp, ci, va))
+        else:
+            inputs.append((rp, ci, va))
+            csrs.append(oracle.transpose(rp, ci, va))
+    plan, offs = rbs.batch_analyse(inputs, substitution=sub, opts=rbs.options(select=select))
+    bs, xs = [], []
+    for i, (arp, aci, ava) in enumerate(csrs):
+        n = len(arp) - 1
+        b = oracle.spmv_csr(arp, aci, ava, rbs.gen_uniform(700 + i, n))
+        bs.append(b)
+        xs.append(oracle.sptrsv_csr(arp, aci, ava, sub, b))
+    dB = torch.tensor(np.concatenate(bs), device=cuda)
+    for prec, tol in ((rbs.PREC_FP64, 1e-12), (rbs.PREC_MIXED, 1e-12), (rbs.PREC_FP32, 1e-4)):
+        dX = torch.empty_like(dB)
+        plan.solve(dB, dX, prec=prec)
+        X = dX.cpu().numpy()
+        for i in range(count):
+            assert rel_err(X[offs[i]:offs[i + 1]], xs[i]) <= tol, (prec, i)
