@@ -320,6 +320,58 @@ def side_analysis(dev, args):
     return out
 
 
+def side_ilu0(dev, args):
+    """ILU(0) of the full 2D 5-point Laplacian pattern on a 1024 x 1024 grid
+    (both triangles, U(-1,1) values, dominant diagonal) on the device, and
+    one preconditioner apply z = U^-1 L^-1 b through this library's plans."""
+    import scipy.sparse as sp
+    import torch
+
+    import rbs
+
+    rp, ci, va = rbs.gen_lower_csr(rbs.GEN_LAPLACE2D, grid=1024, seed=401)
+    n = len(rp) - 1
+    S = sp.tril(sp.csr_matrix((va, ci, rp), shape=(n, n)), k=-1).tocsr()
+    T = S.T.tocsr()
+    T.data = np.random.default_rng(402).uniform(-1, 1, T.nnz)
+    off = (S + T).tocsr()
+    A = (off + sp.diags(1.0 + np.asarray(abs(off).sum(axis=1)).ravel())).tocsr()
+    A.sort_indices()
+    d = [torch.tensor(a, device=dev) for a in (A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data)]
+    dlu = torch.empty_like(d[2])
+    rbs.ilu0_device(d[0], d[1], d[2], dlu)  # first call loads the kernels
+    times = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rbs.ilu0_device(d[0], d[1], d[2], dlu)
+        times.append(time.perf_counter() - t0)
+    lu = dlu.cpu().numpy()
+    # split into L (unit diagonal written out) and U, plans for both
+    rows = np.repeat(np.arange(n), np.diff(A.indptr))
+    low = A.indices < rows
+    Lm = (sp.csr_matrix((lu[low], A.indices[low], np.r_[0, np.cumsum(np.bincount(rows[low], minlength=n))]),
+                        shape=(n, n)) + sp.identity(n, format="csr")).tocsr()
+    Um = sp.csr_matrix((lu[~low], A.indices[~low], np.r_[0, np.cumsum(np.bincount(rows[~low], minlength=n))]),
+                       shape=(n, n))
+    Lm.sort_indices()
+    Um.sort_indices()
+    Lp = rbs.analyse(Lm.indptr.astype(np.int32), Lm.indices.astype(np.int32), Lm.data, substitution=rbs.FORWARD,
+                     lv=-1, fmt=rbs.FMT_CSR)
+    Up = rbs.analyse(Um.indptr.astype(np.int32), Um.indices.astype(np.int32), Um.data, substitution=rbs.BACKWARD,
+                     lv=-1, fmt=rbs.FMT_CSR)
+    db = torch.tensor(rbs.gen_uniform(403, n), device=dev)
+    y, z = torch.empty_like(db), torch.empty_like(db)
+    apply_ms = []
+    for _ in range(5):
+        a = Lp.solve(db, y).ms
+        apply_ms.append(a + Up.solve(y, z).ms)
+    return {"n": n, "nnz": int(A.nnz), "factor_ms": 1000 * float(np.median(times)),
+            "apply_ms": float(np.median(apply_ms[1:])),
+            "apply_kernels": {"L": rbs.KERNEL_NAMES[int(np.bincount(Lp.export("kernel")).argmax())],
+                              "U": rbs.KERNEL_NAMES[int(np.bincount(Up.export("kernel")).argmax())]}}
+
+
 def side_mixed(dev, flush, args):
     """FP32 sweeps + FP64 refinement against the plain FP64 solve on the
     2D-Laplacian factor, the power-law factor and the n = 4M Poisson(10)
@@ -685,6 +737,7 @@ def run_ours(args):
         line["sweep_config1"] = side_structures(dev, flush, args)
         line["config2_mixed"] = side_mixed(dev, flush, args)
         line["analysis_host_vs_device"] = side_analysis(dev, args)
+        line["ilu0_laplace2d_1024"] = side_ilu0(dev, args)
     if not args.no_batch and world == 1:
         line["config3_batched_512"] = side_batched(dev, args)
     if not args.no_serve and world == 1:

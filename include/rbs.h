@@ -194,6 +194,18 @@ int rbs_plan_export(const rbs_plan *plan, const char *name, void *dst, long long
 
 int rbs_plan_free(rbs_plan *plan);
 
+/* ILU(0) of a square CSR matrix on the device (no counterpart in the
+ * reference, which solves with factors it is given): d_lu receives, in A's
+ * pattern, the strict lower part of L (unit diagonal implied) and U (on and
+ * above the diagonal).  Columns must ascend in every row and every row must
+ * hold its diagonal (RBS_ERR_STRUCTURE otherwise, and on a zero pivot).  The
+ * factor is the serial row-wise IKJ result bit for bit.  L and U then go to
+ * rbs_analyse as RBS_FMT_CSR triangles (L with its unit diagonal written
+ * out, RBS_FORWARD; U, RBS_BACKWARD).  Uses opt->device and
+ * opt->spin_limit; allocates O(n) scratch; returns when done. */
+int rbs_ilu0_device(const int *d_rowptr, const int *d_colidx, const double *d_val, int n, int nnz, double *d_lu,
+                    const rbs_options *opt);
+
 /* Plan serialisation (no counterpart in the reference, which repeats its
  * analysis in every process): rbs_plan_save writes the analysis -- level
  * order, labels, block bounds, kernel choice and every execution layout --

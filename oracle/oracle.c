@@ -552,3 +552,45 @@ void orc_spmv_csr(int n, const int *rowptr, const int *colidx, const double *val
         y[i] = acc;
     }
 }
+
+int orc_ilu0_csr(int n, const int *rowptr, const int *colidx, const double *val, double *lu) {
+    int *diag = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    for (int k = 0; k < rowptr[n]; ++k) lu[k] = val[k];
+    for (int i = 0; i < n; ++i) {
+        diag[i] = -1;
+        for (int p = rowptr[i]; p < rowptr[i + 1]; ++p)
+            if (colidx[p] == i) diag[i] = p;
+        if (diag[i] < 0) {
+            free(diag);
+            return -1;
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        for (int p = rowptr[i]; p < diag[i]; ++p) {
+            const int k = colidx[p];
+            const double piv = lu[diag[k]];
+            if (piv == 0.0) {
+                free(diag);
+                return -2;
+            }
+            const double a = lu[p] / piv;
+            lu[p] = a;
+            /* a_ij -= a_ik * a_kj for j > k present in both rows (both sorted) */
+            int t = diag[k] + 1;
+            for (int q = p + 1; q < rowptr[i + 1]; ++q) {
+                const int j = colidx[q];
+                while (t < rowptr[k + 1] && colidx[t] < j) ++t;
+                if (t < rowptr[k + 1] && colidx[t] == j) {
+                    volatile double prod = a * lu[t];
+                    lu[q] = lu[q] - prod;
+                }
+            }
+        }
+        if (lu[diag[i]] == 0.0) {
+            free(diag);
+            return -2;
+        }
+    }
+    free(diag);
+    return 0;
+}

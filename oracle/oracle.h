@@ -84,6 +84,14 @@ int orc_auto_lv(int m, int device_id);
 
 /* Serial FP64 substitution on CSR.  lower: x_i = (b_i - sum_{j<i} L_ij x_j)/L_ii
  * for i ascending; upper: descending.  Returns -1 on a zero/missing diagonal. */
+/* ILU(0) of a square CSR matrix (columns ascending, diagonal present in
+ * every row), row-wise IKJ order restricted to the pattern: lu holds the
+ * strict lower part of L (unit diagonal implied) and U.  Not part of the
+ * reference (the factor producer its solver is meant for); every update is
+ * a separate multiply and subtract, rounded to nearest (no contraction).
+ * Returns -1 on a missing diagonal, -2 on a zero pivot. */
+int orc_ilu0_csr(int n, const int *rowptr, const int *colidx, const double *val, double *lu);
+
 int orc_sptrsv_csr(int n, const int *rowptr, const int *colidx, const double *val,
                    int substitution, const double *b, double *x);
 /* Same with Neumaier-compensated row sums (bounds the oracle's own rounding). */

@@ -48,6 +48,7 @@ lib.orc_blocks_free.argtypes = [ctypes.POINTER(Blocks)]
 lib.orc_sptrsv_csr.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, _dp, _dp]
 lib.orc_sptrsv_csr_compensated.argtypes = lib.orc_sptrsv_csr.argtypes
 lib.orc_spmv_csr.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp, _dp]
+lib.orc_ilu0_csr.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp]
 lib.orc_spmv_csr.restype = None
 lib.orc_transpose.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _ip, _ip, _dp]
 lib.orc_transpose.restype = None
@@ -160,6 +161,17 @@ def sptrsv_csr(rowptr, colidx, val, substitution, b, compensated=False):
             raise RuntimeError("oracle substitution: zero or missing diagonal")
         xs[c] = xc
     return xs.reshape(b.shape)
+
+
+def ilu0_csr(rowptr, colidx, val):
+    """ILU(0) values in the pattern of a CSR matrix (strict L below, U on and above the diagonal)."""
+    rp, ci, va = _i(rowptr), _i(colidx), _d(val)
+    lu = np.zeros(len(ci))
+    rc = lib.orc_ilu0_csr(len(rp) - 1, rp.ctypes.data_as(_ip), ci.ctypes.data_as(_ip), va.ctypes.data_as(_dp),
+                          lu.ctypes.data_as(_dp))
+    if rc != 0:
+        raise RuntimeError("oracle ILU(0): missing diagonal" if rc == -1 else "oracle ILU(0): zero pivot")
+    return lu
 
 
 def spmv_csr(rowptr, colidx, val, x):

@@ -141,6 +141,10 @@ int host_bfs_levels(const int *cp, const int *ri, int m, std::vector<int> &level
 int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, const rbs_options &opt, std::string &err,
                          const std::vector<int> *seg_rows = nullptr);
 
+// ilu0.cu: ILU(0) of a device CSR matrix into d_lu (A's pattern)
+int device_ilu0(const int *d_rp, const int *d_ci, const double *d_val, int n, int nnz, double *d_lu,
+                const rbs_options &opt, std::string &err);
+
 // plan_io.cpp: the plan's host side to and from a file
 int plan_save(const Plan &P, const char *path, std::string &err);
 int plan_load(Plan &P, const char *path, std::string &err);

@@ -109,7 +109,7 @@ EXPORTS = [
     "rbs_gen_lower_csr", "rbs_gen_uniform", "rbs_gen_free", "rbs_plan_profile", "rbs_plan_block_times",
     "rbs_sptrsv_csr_noalloc", "rbs_batch_analyse", "rbs_server_create", "rbs_server_add_factor",
     "rbs_server_submit", "rbs_server_wait", "rbs_server_stats_get", "rbs_server_reset_stats", "rbs_server_destroy",
-    "rbs_plan_save", "rbs_plan_load",
+    "rbs_plan_save", "rbs_plan_load", "rbs_ilu0_device",
 ]
 
 
@@ -140,6 +140,7 @@ def _load():
     lib.rbs_plan_export.argtypes = [P, ctypes.c_char_p, P, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
     lib.rbs_plan_free.argtypes = [P]
     lib.rbs_plan_save.argtypes = [P, ctypes.c_char_p]
+    lib.rbs_ilu0_device.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, P, ctypes.POINTER(Options)]
     lib.rbs_plan_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(Options), ctypes.POINTER(P)]
     lib.rbs_last_error.restype = ctypes.c_char_p
     lib.rbs_auto_lv.argtypes = [ctypes.c_int, ctypes.c_int]
@@ -357,6 +358,14 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def ilu0_device(d_rowptr, d_colidx, d_val, d_lu, opts: Options | None = None):
+    """rbs_ilu0_device on torch CUDA tensors: d_lu receives ILU(0) of the CSR matrix in its pattern."""
+    n = d_rowptr.numel() - 1
+    _check(lib.rbs_ilu0_device(ctypes.c_void_p(d_rowptr.data_ptr()), ctypes.c_void_p(d_colidx.data_ptr()),
+                               ctypes.c_void_p(d_val.data_ptr()), n, d_colidx.numel(),
+                               ctypes.c_void_p(d_lu.data_ptr()), ctypes.byref(opts) if opts is not None else None))
 
 
 def load_plan(path: str, opts: Options | None = None) -> Plan:
