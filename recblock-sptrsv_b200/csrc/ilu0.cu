@@ -6,15 +6,19 @@
 // Row-wise IKJ order restricted to A's pattern: for row i and each k < i in
 // the row (ascending), a_ik /= a_kk, then a_ij -= a_ik * a_kj for every j > k
 // present in both rows i and k.  Row i needs rows k < i of its lower part to
-// be final, so one warp takes one row at a time in ticket order (the
-// earliest unfinished row always has a warp: no deadlock whatever the grid)
-// and waits, bounded, on each dependency's completion flag (release/acquire).
+// be final, so one warp takes one row at a time in ticket order -- rows
+// sorted by dependency level (computed on the host from a copy of the
+// pattern), so the rows in flight span whole levels; the earliest
+// unfinished row always has a warp: no deadlock whatever the grid -- and
+// waits, bounded, on each dependency's completion flag (release/acquire).
 // Every product and difference is rounded separately (no contraction), and
 // a row's updates happen in the serial order, so the factor is bit-identical
 // to the serial IKJ algorithm.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
+#include <vector>
 
 #include "kernels.cuh"
 #include "rbs.h"
@@ -58,13 +62,15 @@ __global__ void k_ilu0_diag(const int *__restrict__ rp, const int *__restrict__ 
 }
 
 __global__ void k_ilu0(const int *__restrict__ rp, const int *__restrict__ ci, const int *__restrict__ diag,
-                       double *lu, int n, int *ticket, int *done, int *status, int *bad_row, long long limit) {
+                       const int *__restrict__ order, double *lu, int n, int *ticket, int *done, int *status,
+                       int *bad_row, long long limit) {
     const int lane = threadIdx.x & 31;
     for (;;) {
-        int i = 0;
-        if (lane == 0) i = atomicAdd(ticket, 1);
-        i = __shfl_sync(0xffffffffu, i, 0);
-        if (i >= n) return;
+        int t = 0;
+        if (lane == 0) t = atomicAdd(ticket, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= n) return;
+        const int i = order[t];
         const int s = rp[i], d = diag[i], e = rp[i + 1];
         for (int p = s; p < d; ++p) {
             const int k = ci[p];
@@ -152,8 +158,35 @@ int device_ilu0(const int *d_rp, const int *d_ci, const double *d_val, int n, in
             rc = RBS_ERR_STRUCTURE;
         }
     }
+    // rows in dependency-level order (level of row i = 1 + the largest level
+    // of the rows of its lower part; all of them precede i), ascending inside
+    // a level: the rows in flight at a time span whole levels, and every
+    // dependency of a row has an earlier ticket
+    int *order = nullptr;
     if (rc == RBS_OK) {
-        k_ilu0<<<sms * 4, 256, 0, st>>>(d_rp, d_ci, diag, d_lu, n, ticket, done, status, bad, opt.spin_limit);
+        std::vector<int> hrp((size_t)n + 1), hci((size_t)nnz), lvl((size_t)n, 0), ord((size_t)n);
+        bool ok = ck(cudaMemcpyAsync(hrp.data(), d_rp, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToHost, st), "memcpy") &&
+                  ck(cudaMemcpyAsync(hci.data(), d_ci, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToHost, st), "memcpy") &&
+                  ck(cudaStreamSynchronize(st), "sync");
+        if (ok) {
+            int nlev = 0;
+            for (int i = 0; i < n; ++i) {
+                int l = 0;
+                for (int p = hrp[(size_t)i]; p < hrp[(size_t)i + 1] && hci[(size_t)p] < i; ++p) l = std::max(l, lvl[(size_t)hci[(size_t)p]] + 1);
+                lvl[(size_t)i] = l;
+                nlev = std::max(nlev, l + 1);
+            }
+            std::vector<int> start((size_t)nlev + 1, 0);
+            for (int i = 0; i < n; ++i) start[(size_t)lvl[(size_t)i] + 1]++;
+            for (int l = 0; l < nlev; ++l) start[(size_t)l + 1] += start[(size_t)l];
+            for (int i = 0; i < n; ++i) ord[(size_t)start[(size_t)lvl[(size_t)i]]++] = i;
+            ok = ck(cudaMalloc(&order, sizeof(int) * (size_t)n), "cudaMalloc") &&
+                 ck(cudaMemcpyAsync(order, ord.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st), "memcpy");
+        }
+        if (!ok) rc = RBS_ERR_CUDA;
+    }
+    if (rc == RBS_OK) {
+        k_ilu0<<<sms * 4, 256, 0, st>>>(d_rp, d_ci, diag, order, d_lu, n, ticket, done, status, bad, opt.spin_limit);
         if (!ck(cudaGetLastError(), "launch") ||
             !ck(cudaMemcpyAsync(h, ticket, sizeof(h), cudaMemcpyDeviceToHost, st), "memcpy") ||
             !ck(cudaStreamSynchronize(st), "sync"))
@@ -166,6 +199,7 @@ int device_ilu0(const int *d_rp, const int *d_ci, const double *d_val, int n, in
             rc = RBS_ERR_STRUCTURE;
         }
     }
+    if (order) cudaFree(order);
     if (scratch) cudaFree(scratch);
     if (st) cudaStreamDestroy(st);
     return rc;
