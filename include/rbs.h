@@ -206,6 +206,60 @@ int rbs_plan_free(rbs_plan *plan);
 int rbs_ilu0_device(const int *d_rowptr, const int *d_colidx, const double *d_val, int n, int nnz, double *d_lu,
                     const rbs_options *opt);
 
+/* ---- Matrix Market input on the device --------------------------------
+ * Replaces mmio_info + mmio_data (mmio_highlevel.h:7-296) and the driver's
+ * triangle extraction and CSR->CSC transposition (main.cu:151-236,
+ * tranpose.h:7-54).  The host reads the banner and size line and streams the
+ * entry bytes to the device, which tokenizes them, converts the numbers,
+ * mirrors symmetric / Hermitian entries (diagonal once; skew-symmetric files
+ * are read as general, as mmio_data does) and builds the CSR.
+ *   - CSR layout as mmio_data's: rows ascending, file order inside a row,
+ *     each mirrored entry placed as if it followed its entry in the file.
+ *   - Values carry the bits fscanf("%lg") gives (correctly rounded; tokens
+ *     outside the device's exact window go to the host's strtod, counted in
+ *     host_values); integer fields convert from C ints; pattern -> 1.0;
+ *     complex -> the real part.
+ *   - Errors instead of the reference's undefined behaviour: a truncated or
+ *     malformed entry (RBS_ERR_ARG), an index outside [1, m] x [1, n]
+ *     (RBS_ERR_STRUCTURE), array storage or an unknown field
+ *     (RBS_ERR_UNSUPPORTED); the message names the first bad entry.
+ * The handle holds the CSR in HBM (opt->device; opt may be NULL). */
+#define RBS_MTX_REAL 0
+#define RBS_MTX_INTEGER 1
+#define RBS_MTX_PATTERN 2
+#define RBS_MTX_COMPLEX 3
+typedef struct rbs_mtx rbs_mtx;
+typedef struct rbs_mtx_info {
+    int m, n;
+    long long nnz_file;   /* entries in the file (the size line's count) */
+    long long nnz;        /* entries after symmetric expansion (mmio_data's nnz) */
+    long long nnz_lower;  /* strictly lower entries of the expanded matrix */
+    long long nnz_upper;  /* strictly upper entries */
+    int field;            /* RBS_MTX_* */
+    int symmetric;        /* 1: symmetric or Hermitian file, mirrored */
+    long long host_values;  /* values converted by the host's strtod */
+    double read_ms;       /* header + file bytes into HBM */
+    double parse_ms;      /* tokens, numbers, expansion and CSR on the device */
+} rbs_mtx_info;
+int rbs_mtx_read(const char *path, const rbs_options *opt, rbs_mtx **mtx);
+/* the same from a file image in host memory */
+int rbs_mtx_read_buffer(const void *bytes, long long len, const rbs_options *opt, rbs_mtx **mtx);
+int rbs_mtx_info_get(const rbs_mtx *mtx, rbs_mtx_info *info);
+/* A's CSR into caller device arrays: rowptr[m+1], colidx[nnz], val[nnz] */
+int rbs_mtx_csr(const rbs_mtx *mtx, int *d_rowptr, int *d_colidx, double *d_val);
+/* main.cu:157-198 (+ tranpose.h for RBS_FMT_CSC): the square matrix's
+ * strictly lower (RBS_FORWARD) or upper (RBS_BACKWARD) entries with a unit
+ * diagonal, the diagonal last (forward) or first (backward) in each row of
+ * the CSR; RBS_FMT_CSC gives that CSR's stable transposition, the layout
+ * rbs_analyse / recblocking_solver_cuda take.  Strict entry number r, in the
+ * CSR's row-major order, takes d_strict_val[r] when d_strict_val is not
+ * NULL (main.cu draws these with rand()), else A's value.  Output sizes:
+ * m+1 pointers, m + nnz_lower (forward) or m + nnz_upper entries.  A
+ * non-square matrix is RBS_ERR_STRUCTURE. */
+int rbs_mtx_triangle(const rbs_mtx *mtx, int substitution, int fmt, const double *d_strict_val, int *d_ptr,
+                     int *d_idx, double *d_val);
+int rbs_mtx_free(rbs_mtx *mtx);
+
 /* Plan serialisation (no counterpart in the reference, which repeats its
  * analysis in every process): rbs_plan_save writes the analysis -- level
  * order, labels, block bounds, kernel choice and every execution layout --

@@ -10,6 +10,8 @@
 #include "oracle.h"
 
 #include <math.h>
+#include <ctype.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -593,4 +595,144 @@ int orc_ilu0_csr(int n, const int *rowptr, const int *colidx, const double *val,
     }
     free(diag);
     return 0;
+}
+
+/* ---- Matrix Market input (mmio_highlevel.h:137-296) -------------------- */
+
+void orc_free(void *p) { free(p); }
+
+int orc_mtx_read(const char *path, int *m, int *n, int *nnz, int *field, int *symmetric, int **rowptr,
+                 int **colidx, double **val) {
+    FILE *f = fopen(path, "r");
+    if (!f) return -1;
+    char line[1025], w[5][64];
+    /* mm_read_banner (mmio.h:254-331): five tokens, banner prefix, lower-cased words */
+    if (!fgets(line, sizeof line, f) ||
+        sscanf(line, "%63s %63s %63s %63s %63s", w[0], w[1], w[2], w[3], w[4]) != 5 ||
+        strncmp(w[0], "%%MatrixMarket", 14) != 0) {
+        fclose(f);
+        return -2;
+    }
+    for (int k = 1; k < 5; ++k)
+        for (char *q = w[k]; *q; ++q) *q = (char)tolower((unsigned char)*q);
+    if (strcmp(w[1], "matrix") || strcmp(w[2], "coordinate")) {
+        fclose(f);
+        return strcmp(w[1], "matrix") ? -2 : -3;
+    }
+    int fld = !strcmp(w[3], "real") ? 0 : !strcmp(w[3], "integer") ? 1 : !strcmp(w[3], "pattern") ? 2
+            : !strcmp(w[3], "complex") ? 3 : -1;
+    if (fld < 0) {
+        fclose(f);
+        return -3;
+    }
+    int sym = !strcmp(w[4], "symmetric") || !strcmp(w[4], "hermitian");
+    /* mm_read_mtx_crd_size (mmio.h:339-367): skip '%' lines, then M N nz */
+    int M = 0, N = 0, NZ = 0;
+    do {
+        if (!fgets(line, sizeof line, f)) {
+            fclose(f);
+            return -4;
+        }
+    } while (line[0] == '%');
+    if (sscanf(line, "%d %d %d", &M, &N, &NZ) != 3) {
+        int got;
+        do {
+            got = fscanf(f, "%d %d %d", &M, &N, &NZ);
+            if (got == EOF) {
+                fclose(f);
+                return -4;
+            }
+        } while (got != 3);
+    }
+    /* entries in file order (mmio_highlevel.h:182-216), 0-based */
+    int *I = (int *)malloc(sizeof(int) * (size_t)(NZ > 0 ? NZ : 1));
+    int *J = (int *)malloc(sizeof(int) * (size_t)(NZ > 0 ? NZ : 1));
+    double *V = (double *)malloc(sizeof(double) * (size_t)(NZ > 0 ? NZ : 1));
+    int rc = 0;
+    for (int k = 0; k < NZ && !rc; ++k) {
+        int i = 0, j = 0, iv = 0;
+        double re = 1.0, im = 0.0;
+        int want = fld == 2 ? 2 : fld == 3 ? 4 : 3, got;
+        if (fld == 0) got = fscanf(f, "%d %d %lg", &i, &j, &re);
+        else if (fld == 1) {
+            got = fscanf(f, "%d %d %d", &i, &j, &iv);
+            re = iv;
+        } else if (fld == 2) got = fscanf(f, "%d %d", &i, &j);
+        else got = fscanf(f, "%d %d %lg %lg", &i, &j, &re, &im);
+        if (got != want) rc = -5;
+        else if (i < 1 || i > M || j < 1 || j > N) rc = -6;
+        I[k] = i - 1;
+        J[k] = j - 1;
+        V[k] = re;
+    }
+    fclose(f);
+    if (rc) {
+        free(I);
+        free(J);
+        free(V);
+        return rc;
+    }
+    /* mmio_highlevel.h:218-290: row counts (mirrors included), scan, and
+     * placement in file order, the mirrored entry right after its entry */
+    int *ptr = (int *)calloc((size_t)M + 1, sizeof(int));
+    for (int k = 0; k < NZ; ++k) {
+        ptr[I[k] + 1]++;
+        if (sym && I[k] != J[k]) ptr[J[k] + 1]++;
+    }
+    for (int r = 0; r < M; ++r) ptr[r + 1] += ptr[r];
+    int total = ptr[M];
+    int *ci = (int *)malloc(sizeof(int) * (size_t)(total > 0 ? total : 1));
+    double *cv = (double *)malloc(sizeof(double) * (size_t)(total > 0 ? total : 1));
+    int *fill = (int *)malloc(sizeof(int) * (size_t)(M > 0 ? M : 1));
+    for (int r = 0; r < M; ++r) fill[r] = ptr[r];
+    for (int k = 0; k < NZ; ++k) {
+        int d = fill[I[k]]++;
+        ci[d] = J[k];
+        cv[d] = V[k];
+        if (sym && I[k] != J[k]) {
+            d = fill[J[k]]++;
+            ci[d] = I[k];
+            cv[d] = V[k];
+        }
+    }
+    free(fill);
+    free(I);
+    free(J);
+    free(V);
+    *m = M;
+    *n = N;
+    *nnz = total;
+    *field = fld;
+    *symmetric = sym;
+    *rowptr = ptr;
+    *colidx = ci;
+    *val = cv;
+    return 0;
+}
+
+int orc_tri_extract(int m, const int *rowptr, const int *colidx, const double *val, int substitution,
+                    const double *strict_val, int *trowptr, int *tcolidx, double *tval) {
+    /* main.cu:157-198 */
+    int p = 0, r = 0;
+    trowptr[0] = 0;
+    for (int i = 0; i < m; ++i) {
+        if (substitution == ORC_BACKWARD) {
+            tcolidx[p] = i;
+            tval[p++] = 1.0;
+        }
+        for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+            const int c = colidx[k];
+            if (substitution == ORC_FORWARD ? c < i : c > i) {
+                tcolidx[p] = c;
+                tval[p++] = strict_val ? strict_val[r] : val[k];
+                ++r;
+            }
+        }
+        if (substitution == ORC_FORWARD) {
+            tcolidx[p] = i;
+            tval[p++] = 1.0;
+        }
+        trowptr[i + 1] = p;
+    }
+    return p;
 }

@@ -104,6 +104,27 @@ int orc_sptrsv_csr_multi(int n, const int *rowptr, const int *colidx, const doub
 void orc_spmv_csr(int n, const int *rowptr, const int *colidx, const double *val,
                   const double *x, double *y);
 
+/* mmio_highlevel.h:137-296 (mmio_data, with mm_read_banner and
+ * mm_read_mtx_crd_size, mmio.h:254-367): a Matrix Market coordinate file
+ * into CSR.  fscanf reads the entries ("%d %d %lg" and the other fields'
+ * forms); symmetric and Hermitian files add the mirrored entry (diagonal
+ * once); rows ascending, file order inside a row.  The arrays are malloc'd
+ * (free with orc_free).  Returns 0, or -1 cannot open, -2 bad banner,
+ * -3 not coordinate / unknown field, -4 bad size line, -5 truncated or
+ * malformed entry, -6 index out of range (the reference does not check
+ * these two). */
+int orc_mtx_read(const char *path, int *m, int *n, int *nnz, int *field, int *symmetric, int **rowptr,
+                 int **colidx, double **val);
+void orc_free(void *p);
+
+/* main.cu:157-198: the unit-diagonal triangle of a square CSR: strictly
+ * lower (forward; diagonal last in the row) or upper (backward; diagonal
+ * first) entries in A's order; strict entry r takes strict_val[r] when
+ * strict_val is not NULL, else A's value.  Output arrays sized m+1 and
+ * m + (strict entries); returns the entry count. */
+int orc_tri_extract(int m, const int *rowptr, const int *colidx, const double *val, int substitution,
+                    const double *strict_val, int *trowptr, int *tcolidx, double *tval);
+
 #ifdef __cplusplus
 }
 #endif

@@ -53,6 +53,12 @@ lib.orc_spmv_csr.restype = None
 lib.orc_transpose.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _ip, _ip, _dp]
 lib.orc_transpose.restype = None
 lib.orc_auto_lv.argtypes = [ctypes.c_int, ctypes.c_int]
+lib.orc_mtx_read.argtypes = [ctypes.c_char_p] + [_ip] * 5 + [ctypes.POINTER(_ip), ctypes.POINTER(_ip),
+                                                          ctypes.POINTER(_dp)]
+lib.orc_free.argtypes = [ctypes.c_void_p]
+lib.orc_free.restype = None
+lib.orc_tri_extract.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, _dp, _ip, _ip, _dp]
+MTX_REF_DUMP = os.path.join(_HERE, "_ref", "mtx_dump")
 
 
 def _i(a):
@@ -207,3 +213,57 @@ def run_reference_dump(colptr, rowidx, val, substitution, lv, workdir):
         res[name] = np.frombuffer(data, dt, cnt, pos).copy()
         pos += cnt * np.dtype(dt).itemsize
     return res
+
+
+MTX_ERRORS = {-1: "cannot open", -2: "bad banner", -3: "not coordinate or unknown field", -4: "bad size line",
+              -5: "truncated or malformed entry", -6: "index out of range"}
+
+
+def mtx_read(path):
+    """Matrix Market file -> CSR the way mmio_data does (mmio_highlevel.h:137-296).
+
+    Returns dict(m, n, field, symmetric, rowptr, colidx, val); raises
+    RuntimeError with the oracle's error code."""
+    m, n, nnz, fld, sym = (ctypes.c_int() for _ in range(5))
+    rp, ci, va = _ip(), _ip(), _dp()
+    rc = lib.orc_mtx_read(os.fsencode(path), ctypes.byref(m), ctypes.byref(n), ctypes.byref(nnz), ctypes.byref(fld),
+                          ctypes.byref(sym), ctypes.byref(rp), ctypes.byref(ci), ctypes.byref(va))
+    if rc != 0:
+        raise RuntimeError(f"oracle mtx_read: {MTX_ERRORS.get(rc, rc)}", rc)
+    try:
+        out = dict(m=m.value, n=n.value, field=fld.value, symmetric=sym.value,
+                   rowptr=np.ctypeslib.as_array(rp, (m.value + 1,)).copy(),
+                   colidx=np.ctypeslib.as_array(ci, (max(nnz.value, 1),))[: nnz.value].copy(),
+                   val=np.ctypeslib.as_array(va, (max(nnz.value, 1),))[: nnz.value].copy())
+    finally:
+        for p in (rp, ci, va):
+            lib.orc_free(ctypes.cast(p, ctypes.c_void_p))
+    return out
+
+
+def tri_extract(rowptr, colidx, val, substitution, strict_val=None):
+    """main.cu:157-198: unit-diagonal strictly lower (forward) / upper (backward) triangle of a square CSR."""
+    rp, ci, va = _i(rowptr), _i(colidx), _d(val)
+    m = len(rp) - 1
+    cap = m + len(ci)
+    tp = np.zeros(m + 1, np.int32)
+    ti = np.zeros(max(cap, 1), np.int32)
+    tv = np.zeros(max(cap, 1), np.float64)
+    sv = None if strict_val is None else _d(strict_val)
+    cnt = lib.orc_tri_extract(m, rp.ctypes.data_as(_ip), ci.ctypes.data_as(_ip), va.ctypes.data_as(_dp), substitution,
+                              None if sv is None else sv.ctypes.data_as(_dp), tp.ctypes.data_as(_ip),
+                              ti.ctypes.data_as(_ip), tv.ctypes.data_as(_dp))
+    return tp, ti[:cnt].copy(), tv[:cnt].copy()
+
+
+def run_reference_mtx(path):
+    """The reference's own mmio_info + mmio_data (oracle/_ref/mtx_dump) on a file."""
+    out = subprocess.run([MTX_REF_DUMP, path], check=True, capture_output=True).stdout
+    m, n, nnz, sym = np.frombuffer(out, np.int32, 4, 0)
+    pos = 16
+    rp = np.frombuffer(out, np.int32, m + 1, pos).copy()
+    pos += 4 * (m + 1)
+    ci = np.frombuffer(out, np.int32, nnz, pos).copy()
+    pos += 4 * nnz
+    va = np.frombuffer(out, np.float64, nnz, pos).copy()
+    return dict(m=int(m), n=int(n), symmetric=int(sym), rowptr=rp, colidx=ci, val=va)

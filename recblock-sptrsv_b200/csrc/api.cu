@@ -4,6 +4,7 @@
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -334,6 +335,85 @@ int rbs_ilu0_device(const int *d_rowptr, const int *d_colidx, const double *d_va
     const int rc = rbs::device_ilu0(d_rowptr, d_colidx, d_val, n, nnz, d_lu, o, err);
     if (rc) return fail(rc, err);
     set_error("");
+    return RBS_OK;
+}
+
+struct rbs_mtx {
+    rbs::DeviceMtx m;
+};
+
+static int mtx_open(const char *path, const void *bytes, long long len, const rbs_options *opt, rbs_mtx **mtx) {
+    if (!mtx) return fail(RBS_ERR_ARG, "rbs_mtx_read: mtx is NULL");
+    *mtx = nullptr;
+    rbs_options o;
+    rbs_options_default(&o);
+    if (opt) o = *opt;
+    rbs_mtx *h = new (std::nothrow) rbs_mtx;
+    if (!h) return fail(RBS_ERR_NOMEM, "rbs_mtx_read: out of host memory");
+    std::string err;
+    const int rc = rbs::mtx_read(path, bytes, len, o, h->m, err);
+    if (rc) {
+        delete h;
+        return fail(rc, err);
+    }
+    *mtx = h;
+    set_error("");
+    return RBS_OK;
+}
+
+int rbs_mtx_read(const char *path, const rbs_options *opt, rbs_mtx **mtx) {
+    if (!path) return fail(RBS_ERR_ARG, "rbs_mtx_read: path is NULL");
+    return mtx_open(path, nullptr, 0, opt, mtx);
+}
+
+int rbs_mtx_read_buffer(const void *bytes, long long len, const rbs_options *opt, rbs_mtx **mtx) {
+    if ((!bytes && len) || len < 0) return fail(RBS_ERR_ARG, "rbs_mtx_read_buffer: bad buffer");
+    return mtx_open(nullptr, bytes, len, opt, mtx);
+}
+
+int rbs_mtx_info_get(const rbs_mtx *mtx, rbs_mtx_info *info) {
+    if (!mtx || !info) return fail(RBS_ERR_ARG, "rbs_mtx_info_get: NULL argument");
+    const rbs::DeviceMtx &M = mtx->m;
+    info->m = M.m;
+    info->n = M.n;
+    info->nnz_file = M.nnz_file;
+    info->nnz = M.nnz;
+    info->nnz_lower = M.nnz_lower;
+    info->nnz_upper = M.nnz_upper;
+    info->field = M.field;
+    info->symmetric = M.symmetric;
+    info->host_values = M.host_values;
+    info->read_ms = M.read_ms;
+    info->parse_ms = M.parse_ms;
+    return RBS_OK;
+}
+
+int rbs_mtx_csr(const rbs_mtx *mtx, int *d_rowptr, int *d_colidx, double *d_val) {
+    if (!mtx || !d_rowptr || ((!d_colidx || !d_val) && mtx->m.nnz))
+        return fail(RBS_ERR_ARG, "rbs_mtx_csr: NULL argument");
+    std::string err;
+    const int rc = rbs::mtx_csr(mtx->m, d_rowptr, d_colidx, d_val, err);
+    if (rc) return fail(rc, err);
+    return RBS_OK;
+}
+
+int rbs_mtx_triangle(const rbs_mtx *mtx, int substitution, int fmt, const double *d_strict_val, int *d_ptr,
+                     int *d_idx, double *d_val) {
+    if (!mtx || !d_ptr || !d_idx || !d_val) return fail(RBS_ERR_ARG, "rbs_mtx_triangle: NULL argument");
+    if (substitution != RBS_FORWARD && substitution != RBS_BACKWARD)
+        return fail(RBS_ERR_ARG, "rbs_mtx_triangle: substitution must be RBS_FORWARD or RBS_BACKWARD");
+    if (fmt != RBS_FMT_CSC && fmt != RBS_FMT_CSR)
+        return fail(RBS_ERR_ARG, "rbs_mtx_triangle: fmt must be RBS_FMT_CSC or RBS_FMT_CSR");
+    std::string err;
+    const int rc = rbs::mtx_triangle(mtx->m, substitution, fmt, d_strict_val, d_ptr, d_idx, d_val, err);
+    if (rc) return fail(rc, err);
+    return RBS_OK;
+}
+
+int rbs_mtx_free(rbs_mtx *mtx) {
+    if (!mtx) return RBS_OK;
+    rbs::mtx_free(mtx->m);
+    delete mtx;
     return RBS_OK;
 }
 

@@ -145,6 +145,25 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
 int device_ilu0(const int *d_rp, const int *d_ci, const double *d_val, int n, int nnz, double *d_lu,
                 const rbs_options &opt, std::string &err);
 
+// mtx.cu: a Matrix Market coordinate file parsed on the device into CSR
+// (mmio_data's layout: rows ascending, file order inside a row, symmetric
+// files mirrored); rowof holds the row of every entry
+struct DeviceMtx {
+    int m = 0, n = 0, field = 0, symmetric = 0, device = 0;
+    long long nnz_file = 0, nnz = 0, nnz_lower = 0, nnz_upper = 0, host_values = 0;
+    double read_ms = 0, parse_ms = 0;
+    int *rowptr = nullptr, *colidx = nullptr, *rowof = nullptr;
+    double *val = nullptr;
+};
+// path != NULL: read the file; else parse bytes[0, len) from host memory
+int mtx_read(const char *path, const void *bytes, long long len, const rbs_options &opt, DeviceMtx &M,
+             std::string &err);
+int mtx_csr(const DeviceMtx &M, int *d_rowptr, int *d_colidx, double *d_val, std::string &err);
+// the unit-diagonal triangle of main.cu:157-198 in CSR or CSC (fmt)
+int mtx_triangle(const DeviceMtx &M, int substitution, int fmt, const double *d_strict, int *d_ptr, int *d_idx,
+                 double *d_val, std::string &err);
+void mtx_free(DeviceMtx &M);
+
 // plan_io.cpp: the plan's host side to and from a file
 int plan_save(const Plan &P, const char *path, std::string &err);
 int plan_load(Plan &P, const char *path, std::string &err);

@@ -109,8 +109,18 @@ EXPORTS = [
     "rbs_gen_lower_csr", "rbs_gen_uniform", "rbs_gen_free", "rbs_plan_profile", "rbs_plan_block_times",
     "rbs_sptrsv_csr_noalloc", "rbs_batch_analyse", "rbs_server_create", "rbs_server_add_factor",
     "rbs_server_submit", "rbs_server_wait", "rbs_server_stats_get", "rbs_server_reset_stats", "rbs_server_destroy",
-    "rbs_plan_save", "rbs_plan_load", "rbs_ilu0_device",
+    "rbs_plan_save", "rbs_plan_load", "rbs_ilu0_device", "rbs_mtx_read", "rbs_mtx_read_buffer", "rbs_mtx_info_get",
+    "rbs_mtx_csr", "rbs_mtx_triangle", "rbs_mtx_free",
 ]
+
+MTX_REAL, MTX_INTEGER, MTX_PATTERN, MTX_COMPLEX = range(4)
+
+
+class MtxInfo(ctypes.Structure):
+    _fields_ = [("m", ctypes.c_int), ("n", ctypes.c_int), ("nnz_file", ctypes.c_longlong),
+                ("nnz", ctypes.c_longlong), ("nnz_lower", ctypes.c_longlong), ("nnz_upper", ctypes.c_longlong),
+                ("field", ctypes.c_int), ("symmetric", ctypes.c_int), ("host_values", ctypes.c_longlong),
+                ("read_ms", ctypes.c_double), ("parse_ms", ctypes.c_double)]
 
 
 class RbsError(RuntimeError):
@@ -142,6 +152,12 @@ def _load():
     lib.rbs_plan_save.argtypes = [P, ctypes.c_char_p]
     lib.rbs_ilu0_device.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, P, ctypes.POINTER(Options)]
     lib.rbs_plan_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(Options), ctypes.POINTER(P)]
+    lib.rbs_mtx_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(Options), ctypes.POINTER(P)]
+    lib.rbs_mtx_read_buffer.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.POINTER(Options), ctypes.POINTER(P)]
+    lib.rbs_mtx_info_get.argtypes = [P, ctypes.POINTER(MtxInfo)]
+    lib.rbs_mtx_csr.argtypes = [P, P, P, P]
+    lib.rbs_mtx_triangle.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P, P]
+    lib.rbs_mtx_free.argtypes = [P]
     lib.rbs_last_error.restype = ctypes.c_char_p
     lib.rbs_auto_lv.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.recblocking_solver_cuda.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_int,
@@ -366,6 +382,64 @@ def ilu0_device(d_rowptr, d_colidx, d_val, d_lu, opts: Options | None = None):
     _check(lib.rbs_ilu0_device(ctypes.c_void_p(d_rowptr.data_ptr()), ctypes.c_void_p(d_colidx.data_ptr()),
                                ctypes.c_void_p(d_val.data_ptr()), n, d_colidx.numel(),
                                ctypes.c_void_p(d_lu.data_ptr()), ctypes.byref(opts) if opts is not None else None))
+
+
+class Mtx:
+    """A Matrix Market file parsed on the device (rbs_mtx_*): A's CSR in HBM,
+    exported to torch tensors, and the triangle main.cu builds from it."""
+
+    def __init__(self, h):
+        self._h = h
+        self.info = MtxInfo()
+        _check(lib.rbs_mtx_info_get(h, ctypes.byref(self.info)))
+
+    def csr(self, device="cuda"):
+        import torch
+        i = self.info
+        rp = torch.empty(i.m + 1, dtype=torch.int32, device=device)
+        ci = torch.empty(max(i.nnz, 1), dtype=torch.int32, device=device)
+        va = torch.empty(max(i.nnz, 1), dtype=torch.float64, device=device)
+        _check(lib.rbs_mtx_csr(self._h, ctypes.c_void_p(rp.data_ptr()), ctypes.c_void_p(ci.data_ptr()),
+                               ctypes.c_void_p(va.data_ptr())))
+        return rp, ci[: i.nnz], va[: i.nnz]
+
+    def triangle(self, substitution: int = FORWARD, fmt: int = FMT_CSC, strict_val=None, device="cuda"):
+        """Unit-diagonal strictly lower (FORWARD) / upper (BACKWARD) triangle
+        as (ptr, idx, val) torch tensors in CSC or CSR; strict_val: optional
+        device tensor of the strict entries' values in row-major order."""
+        import torch
+        i = self.info
+        cnt = i.m + (i.nnz_lower if substitution == FORWARD else i.nnz_upper)
+        ptr = torch.empty(i.m + 1, dtype=torch.int32, device=device)
+        idx = torch.empty(max(cnt, 1), dtype=torch.int32, device=device)
+        val = torch.empty(max(cnt, 1), dtype=torch.float64, device=device)
+        sv = None if strict_val is None else ctypes.c_void_p(strict_val.data_ptr())
+        _check(lib.rbs_mtx_triangle(self._h, substitution, fmt, sv, ctypes.c_void_p(ptr.data_ptr()),
+                                    ctypes.c_void_p(idx.data_ptr()), ctypes.c_void_p(val.data_ptr())))
+        return ptr, idx[:cnt], val[:cnt]
+
+    def close(self):
+        if getattr(self, "_h", None) and lib is not None:
+            lib.rbs_mtx_free(self._h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def mtx_read(path: str, opts: Options | None = None) -> Mtx:
+    """rbs_mtx_read: parse a Matrix Market file on the device."""
+    h = ctypes.c_void_p()
+    _check(lib.rbs_mtx_read(os.fsencode(str(path)), ctypes.byref(opts) if opts is not None else None, ctypes.byref(h)))
+    return Mtx(h)
+
+
+def mtx_read_buffer(data: bytes, opts: Options | None = None) -> Mtx:
+    """rbs_mtx_read_buffer: parse a Matrix Market file image held in host memory."""
+    h = ctypes.c_void_p()
+    _check(lib.rbs_mtx_read_buffer(data, len(data), ctypes.byref(opts) if opts is not None else None,
+                                   ctypes.byref(h)))
+    return Mtx(h)
 
 
 def load_plan(path: str, opts: Options | None = None) -> Plan:
