@@ -372,6 +372,70 @@ def side_ilu0(dev, args):
                               "U": rbs.KERNEL_NAMES[int(np.bincount(Up.export("kernel")).argmax())]}}
 
 
+def side_mtx(dev, args):
+    """Matrix Market input (main.cu:120-236's steps): the 2D 5-point
+    Laplacian pattern on a 1024 x 1024 grid in symmetric storage with
+    U(-1,1) values written %.17g, read and expanded to CSR on the device
+    (rbs_mtx_read), then cut into the forward triangle's CSC
+    (rbs_mtx_triangle).  CPU side: the reference's own mmio_info +
+    mmio_data (oracle/_ref/mtx_dump when built, else the oracle's reader),
+    then the oracle's triangle extraction and transposition.  The file is
+    in the page cache for both sides."""
+    import tempfile
+
+    import torch
+
+    import rbs
+    from oracle import oracle
+
+    rp, ci, _ = rbs.gen_lower_csr(rbs.GEN_LAPLACE2D, grid=1024, seed=77)
+    va = rbs.gen_uniform(78, len(ci))
+    n = len(rp) - 1
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "laplace2d_1024.mtx")
+        rbs.mtx_write(path, rp, ci, va, symmetric=True)
+        size = os.path.getsize(path)
+        M = rbs.mtx_read(path)  # first call: page cache, kernels, pinned staging
+        M.triangle(rbs.FORWARD, rbs.FMT_CSC)
+        reads, parses, tris, totals = [], [], [], []
+        for _ in range(5):
+            del M
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            M = rbs.mtx_read(path)
+            t1 = time.perf_counter()
+            p, x, v = M.triangle(rbs.FORWARD, rbs.FMT_CSC)
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            reads.append(M.info.read_ms)
+            parses.append(M.info.parse_ms)
+            tris.append(1000 * (t2 - t1))
+            totals.append(1000 * (t2 - t0))
+        ref_ms = oracle.reference_mtx_ms(path)
+        t0 = time.perf_counter()
+        o = oracle.mtx_read(path)
+        t1 = time.perf_counter()
+        tp, ti, tv = oracle.tri_extract(o["rowptr"], o["colidx"], o["val"], rbs.FORWARD)
+        cp, cr, cv = oracle.transpose(tp, ti, tv)
+        t2 = time.perf_counter()
+        drp, dci, dva = M.csr()
+        same = bool(np.array_equal(drp.cpu().numpy(), o["rowptr"]) and np.array_equal(dci.cpu().numpy(), o["colidx"])
+                    and np.array_equal(dva.cpu().numpy().view(np.uint64), o["val"].view(np.uint64))
+                    and np.array_equal(p.cpu().numpy(), cp) and np.array_equal(x.cpu().numpy(), cr)
+                    and np.array_equal(v.cpu().numpy().view(np.uint64), cv.view(np.uint64)))
+        read_cpu_ms = ref_ms if ref_ms is not None else 1000 * (t1 - t0)
+        cpu_total = read_cpu_ms + 1000 * (t2 - t1)
+        gpu_total = float(np.median(totals))
+        return {"file_mb": size / 1e6, "entries_file": int(M.info.nnz_file), "entries_csr": int(M.info.nnz), "n": n,
+                "device_ms": {"read_to_hbm": float(np.median(reads)), "parse_to_csr": float(np.median(parses)),
+                              "triangle_csc": float(np.median(tris)), "total": gpu_total},
+                "file_gb_per_s": size / (gpu_total * 1e6), "host_values": int(M.info.host_values),
+                "cpu_ms": {"read": read_cpu_ms,
+                           "read_by": "reference mmio_info + mmio_data" if ref_ms is not None else "oracle port",
+                           "extract_transpose": 1000 * (t2 - t1), "total": cpu_total},
+                "speedup_vs_cpu": cpu_total / gpu_total, "identical": same}
+
+
 def side_mixed(dev, flush, args):
     """FP32 sweeps + FP64 refinement against the plain FP64 solve on the
     2D-Laplacian factor, the power-law factor and the n = 4M Poisson(10)
@@ -738,6 +802,7 @@ def run_ours(args):
         line["config2_mixed"] = side_mixed(dev, flush, args)
         line["analysis_host_vs_device"] = side_analysis(dev, args)
         line["ilu0_laplace2d_1024"] = side_ilu0(dev, args)
+        line["mtx_ingest_laplace2d_1024"] = side_mtx(dev, args)
     if not args.no_batch and world == 1:
         line["config3_batched_512"] = side_batched(dev, args)
     if not args.no_serve and world == 1:

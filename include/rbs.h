@@ -259,6 +259,13 @@ int rbs_mtx_csr(const rbs_mtx *mtx, int *d_rowptr, int *d_colidx, double *d_val)
 int rbs_mtx_triangle(const rbs_mtx *mtx, int substitution, int fmt, const double *d_strict_val, int *d_ptr,
                      int *d_idx, double *d_val);
 int rbs_mtx_free(rbs_mtx *mtx);
+/* Matrix Market output (the reference's mm_write_banner /
+ * mm_write_mtx_crd_size, mmio.h): a host CSR written as a coordinate file,
+ * entries in row-major order, values with %.17g (read back bit for bit),
+ * "pattern" when val is NULL; symmetric != 0 writes only entries with
+ * column <= row under a "symmetric" banner. */
+int rbs_mtx_write(const char *path, int m, int n, const int *rowptr, const int *colidx, const double *val,
+                  int symmetric);
 
 /* Plan serialisation (no counterpart in the reference, which repeats its
  * analysis in every process): rbs_plan_save writes the analysis -- level

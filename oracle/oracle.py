@@ -267,3 +267,12 @@ def run_reference_mtx(path):
     pos += 4 * nnz
     va = np.frombuffer(out, np.float64, nnz, pos).copy()
     return dict(m=int(m), n=int(n), symmetric=int(sym), rowptr=rp, colidx=ci, val=va)
+
+
+def reference_mtx_ms(path):
+    """Wall milliseconds of the reference's own mmio_info + mmio_data on a
+    file (oracle/_ref/mtx_dump --time), or None when it was not built."""
+    if not os.path.exists(MTX_REF_DUMP):
+        return None
+    out = subprocess.run([MTX_REF_DUMP, "--time", path], check=True, capture_output=True, text=True).stdout
+    return float(out.strip())

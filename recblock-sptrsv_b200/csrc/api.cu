@@ -410,6 +410,16 @@ int rbs_mtx_triangle(const rbs_mtx *mtx, int substitution, int fmt, const double
     return RBS_OK;
 }
 
+int rbs_mtx_write(const char *path, int m, int n, const int *rowptr, const int *colidx, const double *val,
+                  int symmetric) {
+    if (!path || !rowptr || (!colidx && m > 0 && rowptr[m] > 0) || m < 0 || n < 0)
+        return fail(RBS_ERR_ARG, "rbs_mtx_write: bad arguments");
+    std::string err;
+    const int rc = rbs::mtx_write(path, m, n, rowptr, colidx, val, symmetric, err);
+    if (rc) return fail(rc, err);
+    return RBS_OK;
+}
+
 int rbs_mtx_free(rbs_mtx *mtx) {
     if (!mtx) return RBS_OK;
     rbs::mtx_free(mtx->m);

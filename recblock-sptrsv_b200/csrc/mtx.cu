@@ -69,15 +69,51 @@ constexpr int SLOT_TEXT = SLOT - 2;              // token characters held in a s
 
 enum { MTX_BAD_TOKEN = 1, MTX_OUT_OF_RANGE = 2 };
 
-struct Buf {  // temporaries of one call
+// Per-device stream-ordered pool for this module's device memory: after the
+// first file, allocations and frees cost microseconds instead of
+// cudaMalloc/cudaFree's milliseconds and device-wide synchronisation.  Up to
+// 4 GB stays reserved between calls; the rest returns to the device at the
+// next synchronisation.
+constexpr int MAX_DEV = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[MAX_DEV] = {};
+
+cudaError_t pool_for(int dev, cudaMemPool_t &pool) {
+    if (dev < 0 || dev >= MAX_DEV) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaError_t e = cudaMemPoolCreate(&g_pool[dev], &props);
+        if (e != cudaSuccess) {
+            g_pool[dev] = nullptr;
+            return e;
+        }
+        unsigned long long keep = 4ULL << 30;
+        e = cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) return e;
+    }
+    pool = g_pool[dev];
+    return cudaSuccess;
+}
+
+struct Buf {  // temporaries of one call, stream-ordered on st
+    cudaStream_t st = nullptr;
+    cudaMemPool_t pool = nullptr;
     std::vector<void *> ptrs;
     ~Buf() {
-        for (void *p : ptrs) cudaFree(p);
+        for (void *p : ptrs) cudaFreeAsync(p, st);
     }
     template <typename T>
     cudaError_t get(T *&p, size_t count) {
-        cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
-        if (e == cudaSuccess) ptrs.push_back(p);
+        void *q = nullptr;
+        cudaError_t e = cudaMallocFromPoolAsync(&q, std::max<size_t>(count, 1) * sizeof(T), pool, st);
+        if (e == cudaSuccess) {
+            ptrs.push_back(q);
+            p = static_cast<T *>(q);
+        }
         return e;
     }
 };
@@ -95,22 +131,23 @@ int grid_for(long long n, int threads, int sms) {
 
 // ---------------------------------------------------------------- kernels
 
-// bit j set: byte p0 + j starts a token (bytes at or beyond len count as space)
+// bit j of the result: byte j of w is a C-locale space (' ', \t..\r)
+__device__ __forceinline__ unsigned space4(unsigned w) {
+    const unsigned sp = __vcmpeq4(w, 0x20202020u) | __vcmpltu4(__vsub4(w, 0x09090909u), 0x05050505u);
+    // 0x00/0xFF bytes -> 4 bits: the top bit of byte j lands on bit 28 + j
+    return ((sp & 0x80808080u) * 0x00204081u) >> 28;
+}
+
+// bit j set: byte p0 + j starts a token.  The buffer is padded with spaces
+// to whole tiles, so bytes at or beyond len are spaces already.
 __device__ __forceinline__ unsigned start_mask(const unsigned char *__restrict__ s, long long len, long long p0) {
     if (p0 >= len) return 0;
-    bool prev_space = p0 == 0 || mtxp::is_space(s[p0 - 1]);
+    const unsigned prev_space = (p0 == 0 || mtxp::is_space(s[p0 - 1])) ? 1u : 0u;
     const uint4 a = *reinterpret_cast<const uint4 *>(s + p0);
     const uint4 b = *reinterpret_cast<const uint4 *>(s + p0 + 16);
-    const unsigned w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-    unsigned mask = 0;
-#pragma unroll
-    for (int j = 0; j < 32; ++j) {
-        const unsigned char c = (unsigned char)(w[j >> 2] >> (8 * (j & 3)));
-        const bool sp = p0 + j >= len || mtxp::is_space(c);
-        if (!sp && prev_space) mask |= 1u << j;
-        prev_space = sp;
-    }
-    return mask;
+    const unsigned sp = space4(a.x) | space4(a.y) << 4 | space4(a.z) << 8 | space4(a.w) << 12 | space4(b.x) << 16 |
+                        space4(b.y) << 20 | space4(b.z) << 24 | space4(b.w) << 28;
+    return ~sp & ((sp << 1) | prev_space);
 }
 
 __global__ void __launch_bounds__(TOK_T) k_tok_count(const unsigned char *__restrict__ s, long long len,
@@ -132,12 +169,18 @@ __global__ void __launch_bounds__(TOK_T) k_tok_mark(const unsigned char *__restr
     __shared__ typename S::TempStorage tmp;
     int before = 0;
     S(tmp).ExclusiveSum(__popc(mask), before);
-    long long t = tile_off[blockIdx.x] + before;
-    while (mask) {
+    if (!mask) return;
+    const long long t = tile_off[blockIdx.x] + before;
+    long long q = t / tpe;  // entry of this thread's first token
+    int r = (int)(t - q * tpe);  // its place inside the entry
+    while (mask && q < nz) {
         const int j = __ffs(mask) - 1;
         mask &= mask - 1;
-        if (t % tpe == 0 && t / tpe < nz) entry_pos[t / tpe] = p0 + j;
-        ++t;
+        if (r == 0) entry_pos[q] = p0 + j;
+        if (++r == tpe) {
+            r = 0;
+            ++q;
+        }
     }
 }
 
@@ -146,48 +189,70 @@ __device__ __forceinline__ long long skip_space(const unsigned char *s, long lon
     return p;
 }
 
-// one entry per thread: 0-based row and column, value, the mirror flag of
-// symmetric files, and the value token's offset when the host converts it
-__global__ void k_entries(const unsigned char *__restrict__ s, long long len, const long long *__restrict__ entry_pos,
-                          long long nz, int field, int symmetric, int m, int n, int *row, int *col, double *val,
-                          int *mirror, unsigned char *host_flag, long long *vpos, int *status,
-                          unsigned long long *bad_entry) {
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nz;
-         e += (long long)gridDim.x * blockDim.x) {
-        long long p = entry_pos[e], end = p;
-        int r = 0, c = 0, fl = 0, hf = 0;
-        double v = 1.0;
-        if (mtxp::parse_int(s, len, p, r, end) != mtxp::PARSE_OK) {
-            fl = MTX_BAD_TOKEN;
-        } else {
-            p = skip_space(s, len, end);
-            if (mtxp::parse_int(s, len, p, c, end) != mtxp::PARSE_OK) {
-                fl = MTX_BAD_TOKEN;
-            } else if (field == RBS_MTX_REAL || field == RBS_MTX_COMPLEX) {
-                p = skip_space(s, len, end);
-                if (mtxp::parse_real(s, len, p, v, end) != mtxp::PARSE_OK) {
-                    hf = 1;
-                    vpos[e] = p;
-                    v = 0.0;
-                }
-            } else if (field == RBS_MTX_INTEGER) {
-                p = skip_space(s, len, end);
-                int iv = 0;
-                if (mtxp::parse_int(s, len, p, iv, end) != mtxp::PARSE_OK) fl = MTX_BAD_TOKEN;
-                v = (double)iv;
-            }
-        }
-        if (!fl && (r < 1 || r > m || c < 1 || c > n)) fl = MTX_OUT_OF_RANGE;
-        if (fl) {
-            atomicOr(status, fl);
-            atomicMin(bad_entry, (unsigned long long)e);
-        }
-        row[e] = r - 1;
-        col[e] = c - 1;
-        val[e] = v;
-        mirror[e] = (symmetric && r != c) ? 1 : 0;
-        host_flag[e] = (unsigned char)hf;
+constexpr int ENT_T = 256;          // entries per CTA
+constexpr int ENT_SMEM = 24576;     // bytes of their text staged in shared memory
+
+// One entry per thread: 0-based row and column, value, the mirror flag of
+// symmetric files, and the value token's offset when the host converts it.
+// A CTA's 256 consecutive entries occupy one contiguous stretch of text,
+// loaded into shared memory with 16-byte coalesced loads (parsed from global
+// memory instead when the stretch is longer than the buffer).
+__global__ void __launch_bounds__(ENT_T) k_entries(const unsigned char *__restrict__ s, long long len,
+                                                   const long long *__restrict__ entry_pos, long long nz, int field,
+                                                   int symmetric, int m, int n, int *row, int *col, double *val,
+                                                   int *mirror, unsigned char *host_flag, long long *vpos,
+                                                   int *status, unsigned long long *bad_entry) {
+    __shared__ __align__(16) unsigned char text[ENT_SMEM];
+    const long long e0 = (long long)blockIdx.x * ENT_T;
+    const long long e = e0 + threadIdx.x;
+    const long long last = e0 + ENT_T < nz ? e0 + ENT_T : nz;
+    const long long start = entry_pos[e0] & ~15LL;  // the buffer base is 256-byte aligned
+    const long long stop = last < nz ? entry_pos[last] : len;
+    const long long wlen = stop - start;
+    const bool staged = wlen <= ENT_SMEM;
+    if (staged) {
+        // up to 15 bytes past stop: inside the tile-padded buffer
+        const int nvec = (int)((wlen + 15) >> 4);
+        const uint4 *src = reinterpret_cast<const uint4 *>(s + start);
+        for (int i = threadIdx.x; i < nvec; i += ENT_T) reinterpret_cast<uint4 *>(text)[i] = src[i];
     }
+    __syncthreads();
+    if (e >= nz) return;
+    const unsigned char *b = staged ? text : s + start;
+    const long long blen = staged ? wlen : len - start;
+    long long p = entry_pos[e] - start, end = p;
+    int r = 0, c = 0, fl = 0, hf = 0;
+    double v = 1.0;
+    if (mtxp::parse_int(b, blen, p, r, end) != mtxp::PARSE_OK) {
+        fl = MTX_BAD_TOKEN;
+    } else {
+        p = skip_space(b, blen, end);
+        if (mtxp::parse_int(b, blen, p, c, end) != mtxp::PARSE_OK) {
+            fl = MTX_BAD_TOKEN;
+        } else if (field == RBS_MTX_REAL || field == RBS_MTX_COMPLEX) {
+            p = skip_space(b, blen, end);
+            if (mtxp::parse_real(b, blen, p, v, end) != mtxp::PARSE_OK) {
+                hf = 1;
+                vpos[e] = start + p;
+                v = 0.0;
+            }
+        } else if (field == RBS_MTX_INTEGER) {
+            p = skip_space(b, blen, end);
+            int iv = 0;
+            if (mtxp::parse_int(b, blen, p, iv, end) != mtxp::PARSE_OK) fl = MTX_BAD_TOKEN;
+            v = (double)iv;
+        }
+    }
+    if (!fl && (r < 1 || r > m || c < 1 || c > n)) fl = MTX_OUT_OF_RANGE;
+    if (fl) {
+        atomicOr(status, fl);
+        atomicMin(bad_entry, (unsigned long long)e);
+    }
+    row[e] = r - 1;
+    col[e] = c - 1;
+    val[e] = v;
+    mirror[e] = (symmetric && r != c) ? 1 : 0;
+    host_flag[e] = (unsigned char)hf;
 }
 
 // the value tokens the host converts, one slot each: text (NUL-terminated,
@@ -428,6 +493,23 @@ struct Source {
     }
 };
 
+// one chunk read by several host threads (page-cache copies scale with
+// threads; the device copy of the previous chunk runs meanwhile)
+bool read_parallel(const Source &src, long long off, long long n, unsigned char *dst) {
+    const int P = n >= (4LL << 20) ? (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency())) : 1;
+    if (P == 1) return src.read(off, n, dst);
+    std::vector<char> ok((size_t)P, 1);
+    std::vector<std::thread> th;
+    for (int t = 0; t < P; ++t) {
+        const long long lo = n * t / P, hi = n * (t + 1) / P;
+        th.emplace_back([&, t, lo, hi] { ok[(size_t)t] = src.read(off + lo, hi - lo, dst + lo); });
+    }
+    for (auto &x : th) x.join();
+    for (char c : ok)
+        if (!c) return false;
+    return true;
+}
+
 // process-wide pinned staging ring (one reader at a time)
 std::mutex g_ring_mu;
 unsigned char *g_ring[NRING] = {nullptr, nullptr, nullptr};
@@ -497,6 +579,8 @@ int read_impl(const Source &src, const rbs_options &opt, DeviceMtx &M, std::stri
         }
     } sg{st};
     Buf buf;
+    buf.st = st;
+    MCK(pool_for(dev, buf.pool));
 
     // entry bytes to HBM, padded with spaces to whole tiles
     const long long len = src.size - h.data_off;
@@ -512,7 +596,7 @@ int read_impl(const Source &src, const rbs_options &opt, DeviceMtx &M, std::stri
         for (long long off = 0; off < len; off += CHUNK, k = (k + 1) % NRING) {
             const long long nb = std::min(CHUNK, len - off);
             if (used[k]) MCK(cudaEventSynchronize(g_ring_ev[k]));
-            if (!src.read(h.data_off + off, nb, g_ring[k])) {
+            if (!read_parallel(src, h.data_off + off, nb, g_ring[k])) {
                 err = "Matrix Market reader: read error";
                 cudaStreamSynchronize(st);
                 return RBS_ERR_ARG;
@@ -577,7 +661,8 @@ int read_impl(const Source &src, const rbs_options &opt, DeviceMtx &M, std::stri
     MCK(cudaMemsetAsync(bad, 0xff, sizeof(unsigned long long), st));
     MCK(cudaMemsetAsync(mir + nz, 0, sizeof(int), st));
     if (nz) {
-        k_entries<<<grid_for(nz, 256, sms), 256, 0, st>>>(ds, len, entry_pos, nz, h.field, h.symmetric, h.m, h.n,
+        k_entries<<<(unsigned)((nz + ENT_T - 1) / ENT_T), ENT_T, 0, st>>>(ds, len, entry_pos, nz, h.field,
+                                                                         h.symmetric, h.m, h.n,
                                                           row, col, v, mir, hflag, vpos, status, bad);
         MCK(cudaGetLastError());
     }
@@ -700,10 +785,14 @@ int read_impl(const Source &src, const rbs_options &opt, DeviceMtx &M, std::stri
     MCK(buf.get(codes, (size_t)cnt));
     unsigned *scodes = nullptr;
     MCK(buf.get(scodes, (size_t)cnt));
-    MCK(cudaMalloc(&M.rowptr, sizeof(int) * ((size_t)h.m + 1)));
-    MCK(cudaMalloc(&M.colidx, sizeof(int) * std::max<size_t>((size_t)cnt, 1)));
-    MCK(cudaMalloc(&M.rowof, sizeof(int) * std::max<size_t>((size_t)cnt, 1)));
-    MCK(cudaMalloc(&M.val, sizeof(double) * std::max<size_t>((size_t)cnt, 1)));
+    // the handle's arrays come from the same pool (freed by mtx_free)
+    MCK(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&M.rowptr), sizeof(int) * ((size_t)h.m + 1), buf.pool, st));
+    MCK(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&M.colidx), sizeof(int) * std::max<size_t>((size_t)cnt, 1),
+                                buf.pool, st));
+    MCK(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&M.rowof), sizeof(int) * std::max<size_t>((size_t)cnt, 1),
+                                buf.pool, st));
+    MCK(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&M.val), sizeof(double) * std::max<size_t>((size_t)cnt, 1),
+                                buf.pool, st));
     unsigned long long *lu = nullptr;
     MCK(buf.get(lu, 2));
     MCK(cudaMemsetAsync(lu, 0, sizeof(unsigned long long) * 2, st));
@@ -733,10 +822,14 @@ int read_impl(const Source &src, const rbs_options &opt, DeviceMtx &M, std::stri
 }  // namespace
 
 void mtx_free(DeviceMtx &M) {
-    cudaFree(M.rowptr);
-    cudaFree(M.colidx);
-    cudaFree(M.rowof);
-    cudaFree(M.val);
+    if (!M.rowptr && !M.colidx && !M.rowof && !M.val) return;
+    int old = 0;
+    cudaGetDevice(&old);
+    cudaSetDevice(M.device);
+    for (void *p : {(void *)M.rowptr, (void *)M.colidx, (void *)M.rowof, (void *)M.val})
+        if (p) cudaFreeAsync(p, nullptr);
+    cudaStreamSynchronize(nullptr);
+    cudaSetDevice(old);
     M.rowptr = M.colidx = M.rowof = nullptr;
     M.val = nullptr;
 }
@@ -765,6 +858,48 @@ int mtx_read(const char *path, const void *bytes, long long len, const rbs_optio
     if (src.fd >= 0) close(src.fd);
     if (rc) mtx_free(M);
     return rc;
+}
+
+int mtx_write(const char *path, int m, int n, const int *rp, const int *ci, const double *val, int symmetric,
+              std::string &err) {
+    // rows in parallel into per-thread text, then written in row order
+    const int nth = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+    std::vector<std::string> part((size_t)nth);
+    long long total = 0;
+    for (int i = 0; i < m; ++i)
+        for (int k = rp[i]; k < rp[i + 1]; ++k) total += !symmetric || ci[k] <= i;
+    auto work = [&](int t) {
+        const int lo = (int)((long long)m * t / nth), hi = (int)((long long)m * (t + 1) / nth);
+        std::string &o = part[(size_t)t];
+        o.reserve((size_t)(rp[hi] - rp[lo]) * 36);
+        char line[96];
+        for (int i = lo; i < hi; ++i)
+            for (int k = rp[i]; k < rp[i + 1]; ++k) {
+                if (symmetric && ci[k] > i) continue;
+                const int len = val ? snprintf(line, sizeof line, "%d %d %.17g\n", i + 1, ci[k] + 1, val[k])
+                                    : snprintf(line, sizeof line, "%d %d\n", i + 1, ci[k] + 1);
+                o.append(line, (size_t)len);
+            }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nth; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto &x : th) x.join();
+    FILE *f = fopen(path, "wb");
+    if (!f) {
+        err = std::string("Matrix Market writer: cannot create ") + path;
+        return RBS_ERR_ARG;
+    }
+    fprintf(f, "%%%%MatrixMarket matrix coordinate %s %s\n%d %d %lld\n", val ? "real" : "pattern",
+            symmetric ? "symmetric" : "general", m, n, total);
+    bool ok = true;
+    for (const auto &o : part) ok = ok && fwrite(o.data(), 1, o.size(), f) == o.size();
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) {
+        err = std::string("Matrix Market writer: write error on ") + path;
+        return RBS_ERR_ARG;
+    }
+    return RBS_OK;
 }
 
 int mtx_csr(const DeviceMtx &M, int *d_rowptr, int *d_colidx, double *d_val, std::string &err) {
@@ -803,6 +938,8 @@ int mtx_triangle(const DeviceMtx &M, int substitution, int fmt, const double *d_
         }
     } sg{st};
     Buf buf;
+    buf.st = st;
+    MCK(pool_for(M.device, buf.pool));
     int *flag = nullptr, *srank = nullptr;
     MCK(buf.get(flag, (size_t)cnt + 1));
     MCK(buf.get(srank, (size_t)cnt + 1));

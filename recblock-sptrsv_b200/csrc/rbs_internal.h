@@ -163,6 +163,8 @@ int mtx_csr(const DeviceMtx &M, int *d_rowptr, int *d_colidx, double *d_val, std
 int mtx_triangle(const DeviceMtx &M, int substitution, int fmt, const double *d_strict, int *d_ptr, int *d_idx,
                  double *d_val, std::string &err);
 void mtx_free(DeviceMtx &M);
+int mtx_write(const char *path, int m, int n, const int *rp, const int *ci, const double *val, int symmetric,
+              std::string &err);
 
 // plan_io.cpp: the plan's host side to and from a file
 int plan_save(const Plan &P, const char *path, std::string &err);

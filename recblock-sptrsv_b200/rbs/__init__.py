@@ -110,7 +110,7 @@ EXPORTS = [
     "rbs_sptrsv_csr_noalloc", "rbs_batch_analyse", "rbs_server_create", "rbs_server_add_factor",
     "rbs_server_submit", "rbs_server_wait", "rbs_server_stats_get", "rbs_server_reset_stats", "rbs_server_destroy",
     "rbs_plan_save", "rbs_plan_load", "rbs_ilu0_device", "rbs_mtx_read", "rbs_mtx_read_buffer", "rbs_mtx_info_get",
-    "rbs_mtx_csr", "rbs_mtx_triangle", "rbs_mtx_free",
+    "rbs_mtx_csr", "rbs_mtx_triangle", "rbs_mtx_free", "rbs_mtx_write",
 ]
 
 MTX_REAL, MTX_INTEGER, MTX_PATTERN, MTX_COMPLEX = range(4)
@@ -158,6 +158,7 @@ def _load():
     lib.rbs_mtx_csr.argtypes = [P, P, P, P]
     lib.rbs_mtx_triangle.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P, P]
     lib.rbs_mtx_free.argtypes = [P]
+    lib.rbs_mtx_write.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ip, ip, dp, ctypes.c_int]
     lib.rbs_last_error.restype = ctypes.c_char_p
     lib.rbs_auto_lv.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.recblocking_solver_cuda.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_int,
@@ -440,6 +441,17 @@ def mtx_read_buffer(data: bytes, opts: Options | None = None) -> Mtx:
     _check(lib.rbs_mtx_read_buffer(data, len(data), ctypes.byref(opts) if opts is not None else None,
                                    ctypes.byref(h)))
     return Mtx(h)
+
+
+def mtx_write(path: str, rowptr: np.ndarray, colidx: np.ndarray, val: np.ndarray | None, ncols: int | None = None,
+              symmetric: bool = False):
+    """rbs_mtx_write: a host CSR as a Matrix Market coordinate file (%.17g values)."""
+    rp = np.ascontiguousarray(rowptr, np.int32)
+    ci = np.ascontiguousarray(colidx, np.int32)
+    m = len(rp) - 1
+    va = None if val is None else np.ascontiguousarray(val, np.float64)
+    _check(lib.rbs_mtx_write(os.fsencode(str(path)), m, m if ncols is None else ncols, _ip(rp), _ip(ci),
+                             None if va is None else _dp(va), int(bool(symmetric))))
 
 
 def load_plan(path: str, opts: Options | None = None) -> Plan:
