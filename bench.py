@@ -436,6 +436,45 @@ def side_mtx(dev, args):
                 "speedup_vs_cpu": cpu_total / gpu_total, "identical": same}
 
 
+def side_ic0(dev, args):
+    """IC(0) of the 2D 5-point Laplacian on a 1024 x 1024 grid given as its
+    lower triangle (U(-1,1) off-diagonal values, dominant diagonal) on the
+    device, and one preconditioner apply z = L^-T L^-1 b: L through a CSR
+    forward plan, L^T through the same arrays read as CSC (backward)."""
+    import scipy.sparse as sp
+    import torch
+
+    import rbs
+
+    rp, ci, va = rbs.gen_lower_csr(rbs.GEN_LAPLACE2D, grid=1024, seed=411)
+    n = len(rp) - 1
+    S = sp.tril(sp.csr_matrix((va, ci, rp), shape=(n, n)), k=-1).tocsr()
+    S = sp.csr_matrix((np.random.default_rng(412).uniform(-1, 1, S.nnz), S.indices, S.indptr), shape=(n, n))
+    Lo = (S + sp.diags(1.0 + np.asarray(abs(S + S.T).sum(axis=1)).ravel())).tocsr()
+    Lo.sort_indices()
+    h = (Lo.indptr.astype(np.int32), Lo.indices.astype(np.int32), Lo.data)
+    d = [torch.tensor(a, device=dev) for a in h]
+    dl = torch.empty_like(d[2])
+    rbs.ic0_device(d[0], d[1], d[2], dl)  # first call loads the kernels
+    times = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rbs.ic0_device(d[0], d[1], d[2], dl)
+        times.append(time.perf_counter() - t0)
+    l = dl.cpu().numpy()
+    Lp = rbs.analyse(h[0], h[1], l, substitution=rbs.FORWARD, lv=-1, fmt=rbs.FMT_CSR)
+    Ltp = rbs.analyse(h[0], h[1], l, substitution=rbs.BACKWARD, lv=-1, fmt=rbs.FMT_CSC)
+    db = torch.tensor(rbs.gen_uniform(413, n), device=dev)
+    y, z = torch.empty_like(db), torch.empty_like(db)
+    apply_ms = []
+    for _ in range(5):
+        a = Lp.solve(db, y).ms
+        apply_ms.append(a + Ltp.solve(y, z).ms)
+    return {"n": n, "nnz_lower": int(Lo.nnz), "factor_ms": 1000 * float(np.median(times)),
+            "apply_ms": float(np.median(apply_ms[1:]))}
+
+
 def side_mixed(dev, flush, args):
     """FP32 sweeps + FP64 refinement against the plain FP64 solve on the
     2D-Laplacian factor, the power-law factor and the n = 4M Poisson(10)
@@ -802,6 +841,7 @@ def run_ours(args):
         line["config2_mixed"] = side_mixed(dev, flush, args)
         line["analysis_host_vs_device"] = side_analysis(dev, args)
         line["ilu0_laplace2d_1024"] = side_ilu0(dev, args)
+        line["ic0_laplace2d_1024"] = side_ic0(dev, args)
         line["mtx_ingest_laplace2d_1024"] = side_mtx(dev, args)
     if not args.no_batch and world == 1:
         line["config3_batched_512"] = side_batched(dev, args)

@@ -206,6 +206,19 @@ int rbs_plan_free(rbs_plan *plan);
 int rbs_ilu0_device(const int *d_rowptr, const int *d_colidx, const double *d_val, int n, int nnz, double *d_lu,
                     const rbs_options *opt);
 
+/* IC(0) (incomplete Cholesky, zero fill) of a symmetric positive definite
+ * matrix on the device (no counterpart in the reference): input is A's
+ * lower triangle as CSR, columns ascending and the diagonal last in every
+ * row; d_l receives L in that pattern (L L^T equals A on it).  The factor is
+ * the serial row algorithm (l_ik = (a_ik - sum_{j<k} l_ij l_kj) / l_kk, then
+ * l_ii = sqrt(a_ii - sum_j l_ij^2), ascending columns, separately rounded
+ * products) bit for bit.  RBS_ERR_STRUCTURE for a bad pattern or a pivot
+ * <= 0.  The preconditioner apply needs one plan for L (RBS_FMT_CSR,
+ * RBS_FORWARD) and one for L^T, which is the same arrays read as CSC
+ * (RBS_FMT_CSC, RBS_BACKWARD): no transpose is formed. */
+int rbs_ic0_device(const int *d_rowptr, const int *d_colidx, const double *d_val, int n, int nnz, double *d_l,
+                   const rbs_options *opt);
+
 /* ---- Matrix Market input on the device --------------------------------
  * Replaces mmio_info + mmio_data (mmio_highlevel.h:7-296) and the driver's
  * triangle extraction and CSR->CSC transposition (main.cu:151-236,

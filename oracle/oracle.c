@@ -597,6 +597,49 @@ int orc_ilu0_csr(int n, const int *rowptr, const int *colidx, const double *val,
     return 0;
 }
 
+int orc_ic0_csr(int n, const int *rowptr, const int *colidx, const double *val, double *l) {
+    /* lower triangle, columns ascending, diagonal last in every row */
+    for (int i = 0; i < n; ++i) {
+        const int b = rowptr[i], e = rowptr[i + 1];
+        if (e <= b || colidx[e - 1] != i) return -1;
+        for (int p = b; p + 1 < e; ++p)
+            if (colidx[p] >= colidx[p + 1] || colidx[p] < 0) return -1;
+    }
+    for (int k = 0; k < rowptr[n]; ++k) l[k] = val[k];
+    int bad = 0;
+    for (int i = 0; i < n; ++i) {
+        const int b = rowptr[i], d = rowptr[i + 1] - 1;
+        for (int p = b; p < d; ++p) {
+            /* l_ik = (a_ik - sum_{j<k} l_ij l_kj) / l_kk, j ascending over both rows */
+            const int k = colidx[p], kd = rowptr[k + 1] - 1;
+            double s = l[p];
+            int qi = b, qk = rowptr[k];
+            while (qi < p && qk < kd) {
+                if (colidx[qi] == colidx[qk]) {
+                    volatile double prod = l[qi] * l[qk];
+                    s = s - prod;
+                    ++qi;
+                    ++qk;
+                } else if (colidx[qi] < colidx[qk]) {
+                    ++qi;
+                } else {
+                    ++qk;
+                }
+            }
+            l[p] = s / l[kd];
+        }
+        /* l_ii = sqrt(a_ii - sum_j l_ij^2), j ascending */
+        double s = l[d];
+        for (int p = b; p < d; ++p) {
+            volatile double prod = l[p] * l[p];
+            s = s - prod;
+        }
+        if (!(s > 0.0) && !bad) bad = 1;
+        l[d] = s > 0.0 ? sqrt(s) : s;
+    }
+    return bad ? -2 : 0;
+}
+
 /* ---- Matrix Market input (mmio_highlevel.h:137-296) -------------------- */
 
 void orc_free(void *p) { free(p); }

@@ -104,6 +104,16 @@ int orc_sptrsv_csr_multi(int n, const int *rowptr, const int *colidx, const doub
 void orc_spmv_csr(int n, const int *rowptr, const int *colidx, const double *val,
                   const double *x, double *y);
 
+/* IC(0): incomplete Cholesky with zero fill of an SPD matrix given as its
+ * lower triangle (CSR, columns ascending, diagonal last in every row);
+ * l receives L in that pattern with L L^T matching A on it.  Row by row,
+ * l_ik = (a_ik - sum_{j<k} l_ij l_kj) / l_kk over the columns shared by rows
+ * i and k in ascending order, then l_ii = sqrt(a_ii - sum_j l_ij^2); every
+ * product rounded on its own.  Returns 0, -1 bad structure, -2 a pivot
+ * <= 0 (not positive definite on the pattern; l_ii is left as the
+ * non-positive value). */
+int orc_ic0_csr(int n, const int *rowptr, const int *colidx, const double *val, double *l);
+
 /* mmio_highlevel.h:137-296 (mmio_data, with mm_read_banner and
  * mm_read_mtx_crd_size, mmio.h:254-367): a Matrix Market coordinate file
  * into CSR.  fscanf reads the entries ("%d %d %lg" and the other fields'

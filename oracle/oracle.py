@@ -49,6 +49,7 @@ lib.orc_sptrsv_csr.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, _dp, _
 lib.orc_sptrsv_csr_compensated.argtypes = lib.orc_sptrsv_csr.argtypes
 lib.orc_spmv_csr.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp, _dp]
 lib.orc_ilu0_csr.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp]
+lib.orc_ic0_csr.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp]
 lib.orc_spmv_csr.restype = None
 lib.orc_transpose.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _ip, _ip, _dp]
 lib.orc_transpose.restype = None
@@ -178,6 +179,17 @@ def ilu0_csr(rowptr, colidx, val):
     if rc != 0:
         raise RuntimeError("oracle ILU(0): missing diagonal" if rc == -1 else "oracle ILU(0): zero pivot")
     return lu
+
+
+def ic0_csr(rowptr, colidx, val):
+    """IC(0) of an SPD matrix given as its lower-triangle CSR (diagonal last): L in that pattern."""
+    rp, ci, va = _i(rowptr), _i(colidx), _d(val)
+    out = np.zeros(len(ci))
+    rc = lib.orc_ic0_csr(len(rp) - 1, rp.ctypes.data_as(_ip), ci.ctypes.data_as(_ip), va.ctypes.data_as(_dp),
+                         out.ctypes.data_as(_dp))
+    if rc != 0:
+        raise RuntimeError("oracle IC(0): bad structure" if rc == -1 else "oracle IC(0): pivot <= 0", rc)
+    return out
 
 
 def spmv_csr(rowptr, colidx, val, x):

@@ -427,6 +427,21 @@ int rbs_mtx_free(rbs_mtx *mtx) {
     return RBS_OK;
 }
 
+int rbs_ic0_device(const int *d_rowptr, const int *d_colidx, const double *d_val, int n, int nnz, double *d_l,
+                   const rbs_options *opt) {
+    if (!d_rowptr || !d_colidx || !d_val || !d_l || n <= 0 || nnz < n)
+        return fail(RBS_ERR_ARG, "rbs_ic0_device: need n > 0, nnz >= n and non-null arrays");
+    rbs_options o;
+    rbs_options_default(&o);
+    if (opt) o = *opt;
+    if (o.spin_limit <= 0) o.spin_limit = 1LL << 22;
+    std::string err;
+    const int rc = rbs::device_ic0(d_rowptr, d_colidx, d_val, n, nnz, d_l, o, err);
+    if (rc) return fail(rc, err);
+    set_error("");
+    return RBS_OK;
+}
+
 int rbs_plan_save(const rbs_plan *plan, const char *path) {
     if (!plan || !path) return fail(RBS_ERR_ARG, "rbs_plan_save: NULL argument");
     std::string err;

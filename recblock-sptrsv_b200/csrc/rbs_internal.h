@@ -144,6 +144,9 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
 // ilu0.cu: ILU(0) of a device CSR matrix into d_lu (A's pattern)
 int device_ilu0(const int *d_rp, const int *d_ci, const double *d_val, int n, int nnz, double *d_lu,
                 const rbs_options &opt, std::string &err);
+// ilu0.cu: IC(0) of an SPD matrix's lower-triangle CSR into d_l (its pattern)
+int device_ic0(const int *d_rp, const int *d_ci, const double *d_val, int n, int nnz, double *d_l,
+               const rbs_options &opt, std::string &err);
 
 // mtx.cu: a Matrix Market coordinate file parsed on the device into CSR
 // (mmio_data's layout: rows ascending, file order inside a row, symmetric

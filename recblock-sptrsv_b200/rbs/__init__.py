@@ -110,7 +110,7 @@ EXPORTS = [
     "rbs_sptrsv_csr_noalloc", "rbs_batch_analyse", "rbs_server_create", "rbs_server_add_factor",
     "rbs_server_submit", "rbs_server_wait", "rbs_server_stats_get", "rbs_server_reset_stats", "rbs_server_destroy",
     "rbs_plan_save", "rbs_plan_load", "rbs_ilu0_device", "rbs_mtx_read", "rbs_mtx_read_buffer", "rbs_mtx_info_get",
-    "rbs_mtx_csr", "rbs_mtx_triangle", "rbs_mtx_free", "rbs_mtx_write",
+    "rbs_mtx_csr", "rbs_mtx_triangle", "rbs_mtx_free", "rbs_mtx_write", "rbs_ic0_device",
 ]
 
 MTX_REAL, MTX_INTEGER, MTX_PATTERN, MTX_COMPLEX = range(4)
@@ -151,6 +151,7 @@ def _load():
     lib.rbs_plan_free.argtypes = [P]
     lib.rbs_plan_save.argtypes = [P, ctypes.c_char_p]
     lib.rbs_ilu0_device.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, P, ctypes.POINTER(Options)]
+    lib.rbs_ic0_device.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, P, ctypes.POINTER(Options)]
     lib.rbs_plan_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(Options), ctypes.POINTER(P)]
     lib.rbs_mtx_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(Options), ctypes.POINTER(P)]
     lib.rbs_mtx_read_buffer.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.POINTER(Options), ctypes.POINTER(P)]
@@ -452,6 +453,15 @@ def mtx_write(path: str, rowptr: np.ndarray, colidx: np.ndarray, val: np.ndarray
     va = None if val is None else np.ascontiguousarray(val, np.float64)
     _check(lib.rbs_mtx_write(os.fsencode(str(path)), m, m if ncols is None else ncols, _ip(rp), _ip(ci),
                              None if va is None else _dp(va), int(bool(symmetric))))
+
+
+def ic0_device(d_rowptr, d_colidx, d_val, d_l, opts: Options | None = None):
+    """rbs_ic0_device on torch CUDA tensors: d_l receives IC(0) of the SPD
+    matrix given as its lower-triangle CSR (diagonal last in every row)."""
+    n = d_rowptr.numel() - 1
+    _check(lib.rbs_ic0_device(ctypes.c_void_p(d_rowptr.data_ptr()), ctypes.c_void_p(d_colidx.data_ptr()),
+                              ctypes.c_void_p(d_val.data_ptr()), n, d_colidx.numel(),
+                              ctypes.c_void_p(d_l.data_ptr()), ctypes.byref(opts) if opts is not None else None))
 
 
 def load_plan(path: str, opts: Options | None = None) -> Plan:
