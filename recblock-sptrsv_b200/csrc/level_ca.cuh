@@ -20,6 +20,8 @@
 // from x in global memory (written by this CTA before an earlier barrier).
 #pragma once
 
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace rbs {
@@ -56,10 +58,6 @@ __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
                  : "memory");
 }
-__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
-}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -70,88 +68,127 @@ __device__ __forceinline__ void cp_async_v(VT *dst, const VT *src) {
     if (sizeof(VT) == 8) cp_async8(dst, src);
     else cp_async4(dst, src);
 }
-// `bytes` (4, 8, 16 or 32) contiguous bytes, both ends aligned to min(bytes, 16)
+__device__ __forceinline__ void cp_async_s4(unsigned dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_s8(unsigned dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_s16(unsigned dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+// `BYTES` (4, 8, 16 or 32) contiguous bytes to a shared-memory address
 template <int BYTES>
-__device__ __forceinline__ void cp_async_n(void *dst, const void *src) {
-    if constexpr (BYTES == 4) cp_async4(dst, src);
-    else if constexpr (BYTES == 8) cp_async8(dst, src);
-    else if constexpr (BYTES == 16) cp_async16(dst, src);
+__device__ __forceinline__ void cp_async_sn(unsigned dst, const void *src) {
+    if constexpr (BYTES == 4) cp_async_s4(dst, src);
+    else if constexpr (BYTES == 8) cp_async_s8(dst, src);
+    else if constexpr (BYTES == 16) cp_async_s16(dst, src);
     else {
         static_assert(BYTES == 32, "row segment of 4, 8, 16 or 32 bytes");
-        cp_async16(dst, src);
-        cp_async16(static_cast<char *>(dst) + 16, static_cast<const char *>(src) + 16);
+        cp_async_s16(dst, src);
+        cp_async_s16(dst + 16, static_cast<const char *>(src) + 16);
     }
 }
 
+template <typename T, int N>
+struct alignas(sizeof(T) * N) Vec {
+    T v[N];
+};
+
+// The level loop is unrolled by the stage count S, so every stage address
+// is a compile-time offset from per-thread bases computed once.
 template <typename VT, int W, int S>
 __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict__ descs) {
     using Lay = CaLayout<VT, W, S>;
+    static_assert(S == 2 || S == 4, "stage count 2 or 4");
     extern __shared__ __align__(128) unsigned char sm[];
     const CaDesc d = descs[blockIdx.x];
-    const VT *__restrict__ valp = (const VT *)d.val;
-    const VT *__restrict__ invp = (const VT *)d.inv;
-    const VT *__restrict__ bp = (const VT *)d.b;
     VT *x = (VT *)d.x;
     VT *xs = reinterpret_cast<VT *>(sm + Lay::xw_off);
     int *tab = reinterpret_cast<int *>(sm + Lay::tab_off);
     const int tid = threadIdx.x;
-    const int ntab = 4 * (d.nlv + 1);
+    const int nlv = d.nlv;
+    const int ntab = 4 * (nlv + 1);
     const bool in_smem = ntab <= CA_TAB;
     if (in_smem)
         for (int i = tid; i < ntab; i += blockDim.x) tab[i] = d.lvl[i];
     __syncthreads();
     const int4 *lt = reinterpret_cast<const int4 *>(in_smem ? tab : d.lvl);
 
-    // stage the row data of level l for this thread (one commit group per level)
-    auto stage = [&](int l) {
-        if (l < d.nlv) {
+    // this thread's source rows and stage-0 slots
+    const int *colp = d.col + tid * W;
+    const VT *valp = (const VT *)d.val + tid * W;
+    const VT *inv_t = (const VT *)d.inv + tid;
+    const VT *b_t = (const VT *)d.b + tid;
+    const unsigned s0 = (unsigned)__cvta_generic_to_shared(sm);
+    const unsigned s_col = s0 + tid * W * 4;
+    const unsigned s_val = s0 + (unsigned)Lay::col_bytes + tid * W * (unsigned)sizeof(VT);
+    const unsigned s_inv = s0 + (unsigned)(Lay::col_bytes + Lay::val_bytes) + tid * (unsigned)sizeof(VT);
+    const unsigned s_b = s_inv + CA_ROWS * (unsigned)sizeof(VT);
+
+    // stage the row data of level l into slot U (= l % S) for this thread,
+    // one commit group per level
+    auto stage = [&](int l, auto slot) {
+        constexpr unsigned off = decltype(slot)::value * (unsigned)Lay::stage_bytes;
+        if (l < nlv) {
             const int4 e = lt[l];  // lo, off, w
             if (tid < e.z) {
-                unsigned char *st = sm + (size_t)(l % S) * Lay::stage_bytes;
-                int *cs = reinterpret_cast<int *>(st);
-                VT *vs = reinterpret_cast<VT *>(st + Lay::col_bytes);
-                VT *is = reinterpret_cast<VT *>(st + Lay::col_bytes + Lay::val_bytes);
-                VT *bs = is + CA_ROWS;
-                const long long o = (long long)e.y + (long long)tid * W;
-                cp_async_n<4 * W>(cs + tid * W, d.col + o);
-                cp_async_n<(int)sizeof(VT) * W>(vs + tid * W, valp + o);
-                cp_async_v<VT>(is + tid, invp + e.x + tid);
-                cp_async_v<VT>(bs + tid, bp + e.x + tid);
+                cp_async_sn<4 * W>(s_col + off, colp + e.y);
+                cp_async_sn<(int)sizeof(VT) * W>(s_val + off, valp + e.y);
+                cp_async_sn<(int)sizeof(VT)>(s_inv + off, inv_t + e.x);
+                cp_async_sn<(int)sizeof(VT)>(s_b + off, b_t + e.x);
             }
         }
         cp_async_commit();
     };
-
-#pragma unroll 1
-    for (int l = 0; l < S - 1; ++l) stage(l);
-    int lo = 0;
-#pragma unroll 1
-    for (int l = 0; l < d.nlv; ++l) {
-        stage(l + S - 1);             // its stage held level l-1, finished at the last barrier
-        cp_async_wait<S - 1>();       // this thread's copies of level l have landed
+    // solve level l from slot U: stage the level S-1 ahead into the slot
+    // freed at the last barrier, wait for this thread's copies of level l
+    auto level = [&](int l, int &lo, auto slot) {
+        constexpr int U = decltype(slot)::value;
+        stage(l + S - 1, std::integral_constant<int, (U + S - 1) % S>{});
+        cp_async_wait<S - 1>();
         const int hi = lt[l + 1].x;
         if (tid < hi - lo) {
-            const unsigned char *st = sm + (size_t)(l % S) * Lay::stage_bytes;
-            const int *cs = reinterpret_cast<const int *>(st) + tid * W;
-            const VT *vs = reinterpret_cast<const VT *>(st + Lay::col_bytes) + tid * W;
-            const VT *is = reinterpret_cast<const VT *>(st + Lay::col_bytes + Lay::val_bytes);
-            const VT *bs = is + CA_ROWS;
+            const unsigned char *st = sm + (size_t)U * Lay::stage_bytes;
+            const Vec<int, W> cs = reinterpret_cast<const Vec<int, W> *>(st)[tid];
+            const Vec<VT, W> vs = reinterpret_cast<const Vec<VT, W> *>(st + Lay::col_bytes)[tid];
+            const VT iv = reinterpret_cast<const VT *>(st + Lay::col_bytes + Lay::val_bytes)[tid];
+            const VT bv = reinterpret_cast<const VT *>(st + Lay::col_bytes + Lay::val_bytes)[CA_ROWS + tid];
             VT sum = 0;
 #pragma unroll
             for (int j = 0; j < W; ++j) {
-                const int c = cs[j];
+                const int c = cs.v[j];
                 if (c >= 0) {
                     const VT xv = c >= hi - CA_XW ? xs[c & (CA_XW - 1)] : x[c];
-                    sum += vs[j] * xv;
+                    sum += vs.v[j] * xv;
                 }
             }
             const int r = lo + tid;
-            const VT xv = finalize((bs[tid] - sum) * is[tid]);
+            const VT xv = finalize((bv - sum) * iv);
             xs[r & (CA_XW - 1)] = xv;
             x[r] = xv;
         }
         lo = hi;
         __syncthreads();
+    };
+
+    stage(0, std::integral_constant<int, 0>{});
+    if constexpr (S == 4) {
+        stage(1, std::integral_constant<int, 1>{});
+        stage(2, std::integral_constant<int, 2>{});
+    }
+    int lo = 0;
+#pragma unroll 1
+    for (int l = 0; l < nlv; l += S) {
+        level(l, lo, std::integral_constant<int, 0>{});
+        if (l + 1 >= nlv) break;
+        level(l + 1, lo, std::integral_constant<int, 1>{});
+        if constexpr (S == 4) {
+            if (l + 2 >= nlv) break;
+            level(l + 2, lo, std::integral_constant<int, 2>{});
+            if (l + 3 >= nlv) break;
+            level(l + 3, lo, std::integral_constant<int, 3>{});
+        }
     }
     cp_async_wait<0>();
 }
