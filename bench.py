@@ -53,6 +53,8 @@ def parse():
                     help="structure of the timed solve (profiling runs; the benchmark line is c1a)")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, side measurements and the CPU baseline "
                                                                "(short runs for profilers)")
+    ap.add_argument("--side", default=None, choices=sorted(SIDE_SECTIONS),
+                    help="run one side measurement alone on cuda:0 and print its JSON (no benchmark line)")
     return ap.parse_args()
 
 
@@ -861,8 +863,16 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# side measurements that take (device, args) and can run alone (--side)
+SIDE_SECTIONS = {"mtx": "side_mtx", "ic0": "side_ic0", "ilu0": "side_ilu0", "analysis": "side_analysis"}
+
+
 def main():
     args = parse()
+    if args.side:
+        import torch
+        print(json.dumps({args.side: globals()[SIDE_SECTIONS[args.side]](torch.device("cuda:0"), args)}))
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
