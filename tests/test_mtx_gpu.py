@@ -130,6 +130,41 @@ def test_device_reader_rejects_bad_entries(cuda, body, code):
     assert e.value.code == code, str(e.value)
 
 
+def test_long_and_out_of_window_tokens_go_through_the_host(cuda):
+    # values whose decimal exponent lies outside the device's exact window,
+    # one of them longer than a host slot (100 zeros after the point)
+    tiny = "0." + "0" * 100 + "123"
+    text = ("%%MatrixMarket matrix coordinate real general\n3 3 4\n"
+            f"1 1 {tiny}\n2 2 1e-200\n3 3 -2.5e+300\n3 1 0.5\n")
+    M = rbs.mtx_read_buffer(text.encode())
+    assert M.info.host_values == 3
+    _, _, va = M.csr()
+    # rows ascending, file order inside row 3: (3,3) then (3,1)
+    np.testing.assert_array_equal(bits(va.cpu().numpy()), bits(np.array([float(tiny), 1e-200, -2.5e300, 0.5])))
+
+
+@pytest.mark.parametrize("sym", [False, True])
+def test_write_read_round_trip_at_size(cuda, tmp_path, sym):
+    # rbs_mtx_write's %.17g values read back bit for bit; a symmetric file
+    # (lower triangle written) expands to L + L^T - diag(L)
+    rp, ci, _ = rbs.gen_lower_csr(rbs.GEN_LAPLACE2D, grid=1024, seed=61)
+    va = rbs.gen_uniform(62, len(ci)) * 10.0 ** np.random.default_rng(63).integers(-40, 40, len(ci))
+    path = str(tmp_path / "w.mtx")
+    rbs.mtx_write(path, rp, ci, va, symmetric=sym)
+    M = rbs.mtx_read(path)
+    if not sym:
+        check_csr(M, rp, ci, va)
+    else:
+        o = oracle.mtx_read(path)
+        check_csr(M, o["rowptr"], o["colidx"], o["val"])
+        # the lower part of every row, in file order, is the written row
+        drp, dci, dva = (t.cpu().numpy() for t in M.csr())
+        rows = np.repeat(np.arange(len(drp) - 1), np.diff(drp))
+        low = dci <= rows
+        np.testing.assert_array_equal(dci[low], ci)
+        np.testing.assert_array_equal(bits(dva[low]), bits(va))
+
+
 def test_triangle_needs_square(cuda):
     M = rbs.mtx_read(os.path.join(ROOT, "tests", "golden", "mtx", "rectangular.mtx"))
     with pytest.raises(rbs.RbsError) as e:
