@@ -615,7 +615,7 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
         B.band_off = -1;
         B.ell_ok = B.ell_nchunks = 0;
         B.ell_chunk_off = B.ell_lo = B.ell_hi = -1;
-        B.ca_ok = B.ca_w = 0;
+        B.ca_ok = B.ca_w = B.ca_win = 0;
         B.ca_tab_off = B.ca_lo = B.ca_hi = -1;
         B.lc_ok = B.lc_nseg = 0;
         B.lc_seg_off = -1;
@@ -944,6 +944,19 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
                 P.ca_val[dst] = P.val_pool[rp[r] + j];
             }
         B.ca_hi = (long long)P.ca_col.size();
+        // window-only blocks: every dependency of level l lies in
+        // [hi_l - CA_WINDOW_ROWS, lo_l); columns become window slots
+        bool win = true;
+        for (int l = 0; l < B.nlv && win; ++l)
+            for (int r = lvp[l]; r < lvp[l + 1] && win; ++r)
+                for (int j = 0; j < rp[r + 1] - rp[r]; ++j)
+                    if (P.col_pool[rp[r] + j] < lvp[l + 1] - CA_WINDOW_ROWS) win = false;
+        if (win) {
+            B.ca_win = 1;
+            for (long long e = B.ca_lo; e < B.ca_hi; ++e)
+                P.ca_col[(size_t)e] = P.ca_col[(size_t)e] < 0 ? CA_WINDOW_ROWS
+                                                             : (P.ca_col[(size_t)e] & (CA_WINDOW_ROWS - 1));
+        }
     }
     if (P.ell_col.size() > (size_t)0x7fffffff || P.ca_col.size() > (size_t)0x7fffffff) {
         err = "rbs_analyse: ELL pool too large";

@@ -23,11 +23,12 @@
 #include <type_traits>
 
 #include "kernels.cuh"
+#include "rbs_internal.h"
 
 namespace rbs {
 
-constexpr int CA_ROWS = 1024;  // rows per level (= threads)
-constexpr int CA_XW = 4096;    // x window (rows)
+constexpr int CA_ROWS = 1024;            // rows per level (= threads)
+constexpr int CA_XW = CA_WINDOW_ROWS;    // x window (rows), plus one always-zero slot
 constexpr int CA_TAB = 6144;   // ints of the level table staged in shared memory (4 per level)
 
 struct CaDesc {
@@ -46,7 +47,7 @@ struct CaLayout {
     static constexpr size_t val_bytes = (size_t)W * CA_ROWS * sizeof(VT);
     static constexpr size_t stage_bytes = col_bytes + val_bytes + 2 * CA_ROWS * sizeof(VT);
     static constexpr size_t xw_off = S * stage_bytes;
-    static constexpr size_t tab_off = xw_off + CA_XW * sizeof(VT);
+    static constexpr size_t tab_off = xw_off + (CA_XW + 16) * sizeof(VT);
     static constexpr size_t total = tab_off + CA_TAB * 4;
 };
 
@@ -97,7 +98,10 @@ struct alignas(sizeof(T) * N) Vec {
 
 // The level loop is unrolled by the stage count S, so every stage address
 // is a compile-time offset from per-thread bases computed once.
-template <typename VT, int W, int S>
+// WIN: the block's columns are window slots (every dependency within the
+// window; padding reads the zero slot), so a dependency is one shared-memory
+// load and an unconditional multiply-add.
+template <typename VT, int W, int S, bool WIN>
 __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict__ descs) {
     using Lay = CaLayout<VT, W, S>;
     static_assert(S == 2 || S == 4, "stage count 2 or 4");
@@ -112,6 +116,7 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
     const bool in_smem = ntab <= CA_TAB;
     if (in_smem)
         for (int i = tid; i < ntab; i += blockDim.x) tab[i] = d.lvl[i];
+    if (tid == 0) xs[CA_XW] = VT(0);
     __syncthreads();
     const int4 *lt = reinterpret_cast<const int4 *>(in_smem ? tab : d.lvl);
 
@@ -158,7 +163,9 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
 #pragma unroll
             for (int j = 0; j < W; ++j) {
                 const int c = cs.v[j];
-                if (c >= 0) {
+                if constexpr (WIN) {
+                    sum += vs.v[j] * xs[c];
+                } else if (c >= 0) {
                     const VT xv = c >= hi - CA_XW ? xs[c & (CA_XW - 1)] : x[c];
                     sum += vs.v[j] * xv;
                 }

@@ -56,8 +56,11 @@ struct ExecBlock {
     // band-scan triangles: W = power of two >= bandwidth, chunks of C rows
     int band_w, band_c, band_nch;
     long long band_off;  // coefficient pool offset (band_nch*band_c*band_w); inverse pool at band_off / band_w
-    // level triangles staged per thread with cp.async (level-ELL layout)
-    int ca_ok, ca_w;
+    // level triangles staged per thread with cp.async (level-ELL layout);
+    // ca_win: every dependency lies within the last CA_WINDOW_ROWS rows of
+    // its level's end, and columns are stored as window slots (padding ->
+    // the always-zero slot CA_WINDOW_ROWS)
+    int ca_ok, ca_w, ca_win;
     long long ca_tab_off;     // level table offset in ca_tab (3*nlv+1 ints)
     long long ca_lo, ca_hi;   // element range of the block in the level-ELL pools
     // single-CTA triangles in ELL chunks (CTA sync-free kernel)
@@ -70,6 +73,9 @@ struct ExecBlock {
     // which single-CTA level kernel runs a RBS_K_LEVEL triangle
     int lvl_var;              // LVL_* below
 };
+
+// rows of the shared-memory x window of the staged level kernel (power of 2)
+constexpr int CA_WINDOW_ROWS = 4096;
 
 // single-CTA level kernels of a RBS_K_LEVEL triangle
 enum { LVL_PLAIN = 0, LVL_CA = 1, LVL_CSF = 2, LVL_LC = 3 };

@@ -283,7 +283,9 @@ template <typename VT, int W, int S>
 int ca_attr(std::string &err) {
     static bool done = false;
     if (!done) {
-        CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)CaLayout<VT, W, S>::total));
+        CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)CaLayout<VT, W, S>::total));
         done = true;
     }
@@ -485,12 +487,18 @@ int launch_blocks(Plan &P, std::string &err) {
                 } else if (K == 1 && B.lvl_var == LVL_CA && B.ca_ok) {
                     // one thread per row of the widest level: no idle warps at the barriers
                     const int nt = std::min(1024, std::max(32, (B.maxwidth + 31) / 32 * 32));
-                    if (B.ca_w == 1)
-                        k_tri_level_ca<VT, 1, 4><<<1, nt, CaLayout<VT, 1, 4>::total, st>>>(cdescs + cti);
+                    if (B.ca_w == 1 && B.ca_win)
+                        k_tri_level_ca<VT, 1, 4, true><<<1, nt, CaLayout<VT, 1, 4>::total, st>>>(cdescs + cti);
+                    else if (B.ca_w == 1)
+                        k_tri_level_ca<VT, 1, 4, false><<<1, nt, CaLayout<VT, 1, 4>::total, st>>>(cdescs + cti);
+                    else if (B.ca_w == 2 && B.ca_win)
+                        k_tri_level_ca<VT, 2, 4, true><<<1, nt, CaLayout<VT, 2, 4>::total, st>>>(cdescs + cti);
                     else if (B.ca_w == 2)
-                        k_tri_level_ca<VT, 2, 4><<<1, nt, CaLayout<VT, 2, 4>::total, st>>>(cdescs + cti);
+                        k_tri_level_ca<VT, 2, 4, false><<<1, nt, CaLayout<VT, 2, 4>::total, st>>>(cdescs + cti);
+                    else if (B.ca_win)
+                        k_tri_level_ca<VT, 4, 2, true><<<1, nt, CaLayout<VT, 4, 2>::total, st>>>(cdescs + cti);
                     else
-                        k_tri_level_ca<VT, 4, 2><<<1, nt, CaLayout<VT, 4, 2>::total, st>>>(cdescs + cti);
+                        k_tri_level_ca<VT, 4, 2, false><<<1, nt, CaLayout<VT, 4, 2>::total, st>>>(cdescs + cti);
                 } else if (K == 1 && B.lvl_var == LVL_CSF && B.ell_ok) {
                     k_tri_cta_syncfree<VT><<<1, 1024, CsfLayout<VT>::total, st>>>(edescs + eti, D.status, limit);
                 } else {
