@@ -133,26 +133,32 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
 
     // stage the row data of level l into slot U (= l % S) for this thread,
     // one commit group per level
-    auto stage = [&](int l, auto slot) {
+    // e: the level's table entry {lo, off, w}
+    auto stage = [&](int l, const int4 &e, auto slot) {
         constexpr unsigned off = decltype(slot)::value * (unsigned)Lay::stage_bytes;
-        if (l < nlv) {
-            const int4 e = lt[l];  // lo, off, w
-            if (tid < e.z) {
-                cp_async_sn<4 * W>(s_col + off, colp + e.y);
-                cp_async_sn<(int)sizeof(VT) * W>(s_val + off, valp + e.y);
-                cp_async_sn<(int)sizeof(VT)>(s_inv + off, inv_t + e.x);
-                cp_async_sn<(int)sizeof(VT)>(s_b + off, b_t + e.x);
-            }
+        if (l < nlv && tid < e.z) {
+            cp_async_sn<4 * W>(s_col + off, colp + e.y);
+            cp_async_sn<(int)sizeof(VT) * W>(s_val + off, valp + e.y);
+            cp_async_sn<(int)sizeof(VT)>(s_inv + off, inv_t + e.x);
+            cp_async_sn<(int)sizeof(VT)>(s_b + off, b_t + e.x);
         }
         cp_async_commit();
     };
-    // solve level l from slot U: stage the level S-1 ahead into the slot
-    // freed at the last barrier, wait for this thread's copies of level l
+    // table entries of levels l .. l+S-1 in registers, entry of level l' in
+    // ent[l' % S] (compile-time indices in the unrolled loop)
+    int4 ent[S];
+#pragma unroll
+    for (int k = 0; k < S; ++k) ent[k] = lt[k < nlv ? k : nlv];
+    // solve level l from slot U: read the entry of level l+S a level early,
+    // stage level l+S-1 into the slot freed at the last barrier, wait for
+    // this thread's copies of level l
     auto level = [&](int l, int &lo, auto slot) {
         constexpr int U = decltype(slot)::value;
-        stage(l + S - 1, std::integral_constant<int, (U + S - 1) % S>{});
+        const int hi = ent[(U + 1) % S].x;
+        const int4 e_stage = ent[(U + S - 1) % S];
+        if (l + S <= nlv) ent[U] = lt[l + S];  // level l's own entry is no longer needed
+        stage(l + S - 1, e_stage, std::integral_constant<int, (U + S - 1) % S>{});
         cp_async_wait<S - 1>();
-        const int hi = lt[l + 1].x;
         if (tid < hi - lo) {
             const unsigned char *st = sm + (size_t)U * Lay::stage_bytes;
             const Vec<int, W> cs = reinterpret_cast<const Vec<int, W> *>(st)[tid];
@@ -179,10 +185,10 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
         __syncthreads();
     };
 
-    stage(0, std::integral_constant<int, 0>{});
+    stage(0, ent[0], std::integral_constant<int, 0>{});
     if constexpr (S == 4) {
-        stage(1, std::integral_constant<int, 1>{});
-        stage(2, std::integral_constant<int, 2>{});
+        stage(1, ent[1], std::integral_constant<int, 1>{});
+        stage(2, ent[2], std::integral_constant<int, 2>{});
     }
     int lo = 0;
 #pragma unroll 1
