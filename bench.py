@@ -305,13 +305,13 @@ def side_analysis(dev, args):
         host_s = time.perf_counter() - t0
         d = [torch.tensor(s2[k], device=dev) for k in ("cp", "ri", "cv")]
         times = []
-        for _ in range(2):  # the first call of a size also loads the kernels it needs
+        for _ in range(3):  # the first call of a size also loads the kernels it needs
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             pd = rbs.analyse_device(d[0], d[1], d[2], s2["n"], s2["nnz"], substitution=rbs.FORWARD, lv=-1,
                                     opts=rbs.options(host_only=1))
             times.append(time.perf_counter() - t0)
-        dev_s = times[-1]
+        dev_s = min(times[1:])
         same = bool((ph.export("levelItem") == pd.export("levelItem")).all() and
                     (ph.export("recblock_Index") == pd.export("recblock_Index")).all())
         out[kind] = {"n": s2["n"], "nnz": s2["nnz"], "nlevel": ph.info().nlevel,

@@ -343,16 +343,23 @@ __global__ void k_row_count(const int *__restrict__ rows, long long nnz, int *cn
         atomicAdd(cnt + rows[t], 1);
 }
 
-// device buffers of one analysis, freed on every path
+// device buffers of one analysis, stream-ordered on the analysis stream
+// from the per-device pool, freed on every path
 struct Buf {
+    cudaStream_t st = nullptr;
+    cudaMemPool_t pool = nullptr;
     std::vector<void *> ptrs;
     ~Buf() {
-        for (void *p : ptrs) cudaFree(p);
+        for (void *p : ptrs) cudaFreeAsync(p, st);
     }
     template <typename T>
     cudaError_t get(T *&p, size_t count) {
-        cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
-        if (e == cudaSuccess) ptrs.push_back(p);
+        void *q = nullptr;
+        cudaError_t e = cudaMallocFromPoolAsync(&q, std::max<size_t>(count, 1) * sizeof(T), pool, st);
+        if (e == cudaSuccess) {
+            ptrs.push_back(q);
+            p = static_cast<T *>(q);
+        }
         return e;
     }
 };
@@ -396,6 +403,12 @@ int device_analyse(Plan &P, const int *d_ptr, const int *d_idx, const double *d_
         ~StreamGuard() { cudaStreamDestroy(s); }
     } guard{st};
     Buf buf;
+    buf.st = st;
+    {
+        int dev = 0;
+        DCK(cudaGetDevice(&dev));
+        DCK(device_mem_pool(dev, buf.pool));
+    }
     const int fwd = substitution == RBS_FORWARD;
     const int TPB = 256;
     // 1. CSC input (a CSR input is transposed: stable sort of its entries by

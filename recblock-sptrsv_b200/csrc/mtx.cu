@@ -69,35 +69,7 @@ constexpr int SLOT_TEXT = SLOT - 2;              // token characters held in a s
 
 enum { MTX_BAD_TOKEN = 1, MTX_OUT_OF_RANGE = 2 };
 
-// Per-device stream-ordered pool for this module's device memory: after the
-// first file, allocations and frees cost microseconds instead of
-// cudaMalloc/cudaFree's milliseconds and device-wide synchronisation.  Up to
-// 4 GB stays reserved between calls; the rest returns to the device at the
-// next synchronisation.
-constexpr int MAX_DEV = 64;
-std::mutex g_pool_mu;
-cudaMemPool_t g_pool[MAX_DEV] = {};
-
-cudaError_t pool_for(int dev, cudaMemPool_t &pool) {
-    if (dev < 0 || dev >= MAX_DEV) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lk(g_pool_mu);
-    if (!g_pool[dev]) {
-        cudaMemPoolProps props = {};
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = dev;
-        cudaError_t e = cudaMemPoolCreate(&g_pool[dev], &props);
-        if (e != cudaSuccess) {
-            g_pool[dev] = nullptr;
-            return e;
-        }
-        unsigned long long keep = 4ULL << 30;
-        e = cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &keep);
-        if (e != cudaSuccess) return e;
-    }
-    pool = g_pool[dev];
-    return cudaSuccess;
-}
+cudaError_t pool_for(int dev, cudaMemPool_t &pool) { return device_mem_pool(dev, pool); }
 
 struct Buf {  // temporaries of one call, stream-ordered on st
     cudaStream_t st = nullptr;
@@ -820,6 +792,38 @@ int read_impl(const Source &src, const rbs_options &opt, DeviceMtx &M, std::stri
 }
 
 }  // namespace
+
+// Per-device stream-ordered pool for the temporaries of the Matrix Market
+// reader and the device analysis: after the first call, allocations and
+// frees cost microseconds instead of cudaMalloc/cudaFree's milliseconds and
+// device-wide synchronisation.  Up to 4 GB stays reserved between calls;
+// the rest returns to the device at the next synchronisation.
+namespace {
+constexpr int MAX_DEV = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[MAX_DEV] = {};
+}  // namespace
+
+cudaError_t device_mem_pool(int dev, cudaMemPool_t &pool) {
+    if (dev < 0 || dev >= MAX_DEV) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaError_t e = cudaMemPoolCreate(&g_pool[dev], &props);
+        if (e != cudaSuccess) {
+            g_pool[dev] = nullptr;
+            return e;
+        }
+        unsigned long long keep = 4ULL << 30;
+        e = cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) return e;
+    }
+    pool = g_pool[dev];
+    return cudaSuccess;
+}
 
 void mtx_free(DeviceMtx &M) {
     if (!M.rowptr && !M.colidx && !M.rowof && !M.val) return;

@@ -19,6 +19,7 @@
 // (rows run to m when t+lowbit(t) == 2^lv).
 #pragma once
 
+#include <cuda_runtime_api.h>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -153,6 +154,10 @@ int device_ilu0(const int *d_rp, const int *d_ci, const double *d_val, int n, in
 // ilu0.cu: IC(0) of an SPD matrix's lower-triangle CSR into d_l (its pattern)
 int device_ic0(const int *d_rp, const int *d_ci, const double *d_val, int n, int nnz, double *d_l,
                const rbs_options &opt, std::string &err);
+
+// mtx.cu: the per-device stream-ordered memory pool for temporaries
+// (allocate with cudaMallocFromPoolAsync, free with cudaFreeAsync)
+cudaError_t device_mem_pool(int dev, cudaMemPool_t &pool);
 
 // mtx.cu: a Matrix Market coordinate file parsed on the device into CSR
 // (mmio_data's layout: rows ascending, file order inside a row, symmetric
