@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -19,6 +20,19 @@
 #include "rbs_internal.h"
 
 namespace rbs {
+
+// Kernel attributes (the dynamic shared-memory limit) belong to a device
+// context: set them once per device, tracked by one bit per device.
+inline bool attr_done(const std::atomic<unsigned long long> &seen) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return (seen.load() >> (dev & 63)) & 1ULL;
+}
+inline void attr_mark(std::atomic<unsigned long long> &seen) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    seen.fetch_or(1ULL << (dev & 63));
+}
 
 struct DeviceState {
     int device = 0, num_sms = 148;
@@ -269,11 +283,11 @@ int ell_descs(Plan &P, CsfDesc *&out, std::string &err) {
     D.ell_cache[key] = dd;
     out = dd;
     if (!h.empty()) {
-        static bool attr = false;
-        if (!attr) {
+        static std::atomic<unsigned long long> attr{0};
+        if (!attr_done(attr)) {
             CK(cudaFuncSetAttribute(k_tri_cta_syncfree<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)CsfLayout<VT>::total));
-            attr = true;
+            attr_mark(attr);
         }
     }
     return RBS_OK;
@@ -281,13 +295,13 @@ int ell_descs(Plan &P, CsfDesc *&out, std::string &err) {
 
 template <typename VT, int W, int S>
 int ca_attr(std::string &err) {
-    static bool done = false;
-    if (!done) {
+    static std::atomic<unsigned long long> done{0};
+    if (!attr_done(done)) {
         CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)CaLayout<VT, W, S>::total));
         CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)CaLayout<VT, W, S>::total));
-        done = true;
+        attr_mark(done);
     }
     return RBS_OK;
 }
@@ -332,10 +346,10 @@ constexpr int lc_smem() {
 }
 template <typename VT>
 int lc_attr(std::string &err) {
-    static bool done = false;
-    if (!done) {
+    static std::atomic<unsigned long long> done{0};
+    if (!attr_done(done)) {
         CK(cudaFuncSetAttribute(k_tri_lc<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lc_smem<VT>()));
-        done = true;
+        attr_mark(done);
     }
     return RBS_OK;
 }
@@ -383,10 +397,10 @@ int run_band(Plan &P, const ExecBlock &B, const VT *bb, VT *xx, int K, std::stri
     VT *states = reinterpret_cast<VT *>(D.band_states);
     const int tpb = 256;
     const size_t smem = (size_t)tpb * (W * W + W) * sizeof(VT);
-    static bool attr_set = false;
-    if (!attr_set) {
+    static std::atomic<unsigned long long> attr_set{0};
+    if (!attr_done(attr_set)) {
         CK(cudaFuncSetAttribute(k_band_scan<VT, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
+        attr_mark(attr_set);
     }
     const int grid = (B.band_nch + 255) / 256;
     for (int c = 0; c < K; ++c) {
