@@ -242,10 +242,13 @@ static int device_factor(bool ic, const int *d_rp, const int *d_ci, const double
         !ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute"))
         return RBS_ERR_CUDA;
     cudaStream_t st = nullptr;
+    cudaMemPool_t pool = nullptr;  // the per-device stream-ordered pool (allocations on st)
     int *scratch = nullptr;  // diag[n], done[n], ticket, status, bad_row
     int rc = RBS_OK;
     if (!ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream") ||
-        !ck(cudaMalloc(&scratch, sizeof(int) * (2 * (size_t)n + 4)), "cudaMalloc"))
+        !ck(device_mem_pool(dev, pool), "memory pool") ||
+        !ck(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&scratch), sizeof(int) * (2 * (size_t)n + 4), pool, st),
+            "cudaMallocFromPoolAsync"))
         rc = RBS_ERR_CUDA;
     int *diag = scratch, *done = scratch + n, *ticket = scratch + 2 * (size_t)n, *status = ticket + 1,
         *bad = ticket + 2;
@@ -295,7 +298,8 @@ static int device_factor(bool ic, const int *d_rp, const int *d_ci, const double
             for (int i = 0; i < n; ++i) start[(size_t)lvl[(size_t)i] + 1]++;
             for (int l = 0; l < nlev; ++l) start[(size_t)l + 1] += start[(size_t)l];
             for (int i = 0; i < n; ++i) ord[(size_t)start[(size_t)lvl[(size_t)i]]++] = i;
-            ok = ck(cudaMalloc(&order, sizeof(int) * (size_t)n), "cudaMalloc") &&
+            ok = ck(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&order), sizeof(int) * (size_t)n, pool, st),
+                    "cudaMallocFromPoolAsync") &&
                  ck(cudaMemcpyAsync(order, ord.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st), "memcpy");
         }
         if (!ok) rc = RBS_ERR_CUDA;
@@ -319,9 +323,12 @@ static int device_factor(bool ic, const int *d_rp, const int *d_ci, const double
             rc = RBS_ERR_STRUCTURE;
         }
     }
-    if (order) cudaFree(order);
-    if (scratch) cudaFree(scratch);
-    if (st) cudaStreamDestroy(st);
+    if (order) cudaFreeAsync(order, st);
+    if (scratch) cudaFreeAsync(scratch, st);
+    if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
     return rc;
 }
 
