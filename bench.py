@@ -53,7 +53,7 @@ def parse():
                     help="structure of the timed solve (profiling runs; the benchmark line is c1a)")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, side measurements and the CPU baseline "
                                                                "(short runs for profilers)")
-    ap.add_argument("--side", default=None, choices=sorted(SIDE_SECTIONS),
+    ap.add_argument("--side", default=None, choices=["analysis", "batched", "ic0", "ilu0", "mtx", "serve"],
                     help="run one side measurement alone on cuda:0 and print its JSON (no benchmark line)")
     return ap.parse_args()
 
@@ -873,7 +873,8 @@ def run_ours(args):
 
 
 # side measurements that take (device, args) and can run alone (--side)
-SIDE_SECTIONS = {"mtx": "side_mtx", "ic0": "side_ic0", "ilu0": "side_ilu0", "analysis": "side_analysis"}
+SIDE_SECTIONS = {"mtx": "side_mtx", "ic0": "side_ic0", "ilu0": "side_ilu0", "analysis": "side_analysis",
+                 "batched": "side_batched", "serve": "side_serving"}
 
 
 def main():

@@ -121,14 +121,19 @@ struct Factor {
                     err = cudaGetErrorString(e);
                 }
             }
+            // results out of the staging buffer before the server lock: the
+            // copies (tens of MB) must not hold up the other factors' workers
+            if (rc == RBS_OK || rc == RBS_ERR_NOCONV) {
+                int off = 0;
+                for (auto &r : batch) {
+                    std::memcpy(r->x, hx + (size_t)off * n, sizeof(double) * (size_t)n * r->k);
+                    off += r->k;
+                }
+            }
             const auto now = Clock::now();
-            int off = 0;
             {
                 std::lock_guard<std::mutex> lk(srv->mu);
                 for (auto &r : batch) {
-                    if (rc == RBS_OK || rc == RBS_ERR_NOCONV)
-                        std::memcpy(r->x, hx + (size_t)off * n, sizeof(double) * (size_t)n * r->k);
-                    off += r->k;
                     r->status = rc;
                     r->error = err;
                     r->batch_k = k;
