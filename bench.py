@@ -714,7 +714,8 @@ def launches_per_solve(plan):
     import rbs
     kern = plan.export("kernel")
     lr = plan.export("longrow")
-    return 2 + int((kern != rbs.K_EMPTY).sum()) + int((lr > 0).sum())
+    mr = plan.export("medrow")
+    return 2 + int((kern != rbs.K_EMPTY).sum()) + int((lr > 0).sum()) + int((mr > 0).sum())
 
 
 def run_ours(args):

@@ -22,6 +22,7 @@ namespace rbs {
 namespace {
 
 constexpr int kLongRow = 2048;  // utils_spmv_cuda.h:9 LONGROW_THRESHOLD
+constexpr int kMedRow = 32;     // RBS_MEDROW (kernels.cuh)
 
 int lowbit(int t) { return t & -t; }
 
@@ -610,7 +611,8 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
         ExecBlock &B = P.blocks[b];
         B.index = b;
         B.tri = (b & 1) == 0;
-        B.rows_off = B.long_off = B.map_off = B.lvl_off = -1;
+        B.rows_off = B.long_off = B.med_off = B.map_off = B.lvl_off = -1;
+        B.medrows = 0;
         B.band_w = B.band_c = B.band_nch = 0;
         B.band_off = -1;
         B.ell_ok = B.ell_nchunks = 0;
@@ -774,6 +776,18 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
                 if (rowcnt[b][r] > kLongRow) P.rows_pool.push_back(pos);
                 ++pos;
             }
+        }
+        if (!B.tri && B.kernel == RBS_K_SPMV && B.group < 32 && B.lenmax > kMedRow) {
+            // single RHS: rows of kMedRow+1..kLongRow entries take a warp each
+            B.med_off = (long long)P.rows_pool.size();
+            int pos = 0;
+            for (int r = 0; r < B.m; ++r) {
+                if (dcsr && rowcnt[b][r] == 0) continue;
+                if (rowcnt[b][r] > kMedRow && rowcnt[b][r] <= kLongRow) P.rows_pool.push_back(pos);
+                ++pos;
+            }
+            B.medrows = (int)((long long)P.rows_pool.size() - B.med_off);
+            if (!B.medrows) B.med_off = -1;
         }
         if (wants_level(B, opt)) {
             B.lvl_off = (long long)P.lvl_pool.size();
@@ -999,7 +1013,7 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
     // geometry
     std::vector<int> loc_off(sum, 0), tmp_off(sum, 0), blk_m(sum), blk_n(sum), blk_nnz(sum);
     std::vector<int> stu(sum, -1), std_(sum, -1), sru(sum, -1), srd(sum, -1), srr(sum, -1), srl(sum, -1);
-    std::vector<int> method(sum), kernel(sum);
+    std::vector<int> method(sum), kernel(sum), medrow(sum);
     for (int b = 0; b < sum; ++b) {
         const ExecBlock &B = P.blocks[b];
         blk_m[b] = B.m;
@@ -1007,6 +1021,7 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
         blk_nnz[b] = B.nnz;
         method[b] = B.ref_method;
         kernel[b] = B.kernel;
+        medrow[b] = B.medrows;
         if (B.tri) {
             mirror(B.r0, B.r0 + B.m, stu[b], std_[b]);
             loc_off[b] = stu[b];
@@ -1031,6 +1046,7 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
     if (name == "subrec_left") return put(srl);
     if (name == "method") return put(method);
     if (name == "kernel") return put(kernel);
+    if (name == "medrow") return put(medrow);  // per block: rows of the single-RHS warp-per-row pass
     if (name == "perm") return put(P.perm);
     if (name == "levelItem") {
         // utils_reordering.h:189-197: reversed for backward

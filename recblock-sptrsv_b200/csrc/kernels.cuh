@@ -21,6 +21,7 @@ namespace rbs {
 #define RBS_SENT32 0xFFC0DEADu
 #define RBS_STATUS_TIMEOUT 1
 #define RBS_LONGROW 2048
+#define RBS_MEDROW 32  // squares, single RHS, lane group < 32: longer rows take a warp each
 
 template <typename VT> struct Sent;
 template <> struct Sent<double> {
@@ -298,7 +299,7 @@ template <typename VT, int K>
 __global__ void __launch_bounds__(256) k_spmv_sub(const int *__restrict__ rp, const int *__restrict__ col,
                                                   const VT *__restrict__ val, const int *__restrict__ rows,
                                                   int nrows, int G, const VT *__restrict__ x, VT *b,
-                                                  int skip_long) {
+                                                  int maxlen) {
     constexpr int R = K < 32 ? K : 32;
     constexpr int RPL = K / R;
     const int g = K == 1 ? G : R;
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(256) k_spmv_sub(const int *__restrict__ rp, co
             s = rp[i];
             e = rp[i + 1];
             row = rows ? rows[i] : (int)i;
-            if (skip_long && e - s > RBS_LONGROW) e = s;
+            if (e - s > maxlen) e = s;  // a longer row is another kernel's
         }
         if (K == 1) {
             VT sum = 0;
@@ -335,6 +336,30 @@ __global__ void __launch_bounds__(256) k_spmv_sub(const int *__restrict__ rp, co
 #pragma unroll
             for (int r = 0; r < RPL; ++r) b[o + r] -= acc[r];
         }
+    }
+}
+
+// Medium rows of a square whose lane group is narrow (single RHS): rows of
+// more than RBS_MEDROW entries, up to RBS_LONGROW, one warp each, summed in
+// a fixed shuffle order (deterministic) -- so a few long rows no longer
+// hold a narrow group for hundreds of serial steps.  `pos` lists positions
+// in the row pointer (the row for CSR, the list index for DCSR).
+template <typename VT>
+__global__ void __launch_bounds__(256) k_spmv_rows(const int *__restrict__ rp, const int *__restrict__ col,
+                                                   const VT *__restrict__ val, const int *__restrict__ rows,
+                                                   const int *__restrict__ pos, int npos,
+                                                   const VT *__restrict__ x, VT *b) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long t = warp; t < npos; t += nwarps) {
+        const int i = pos[t];
+        const int s = rp[i], e = rp[i + 1];
+        VT sum = 0;
+        for (int k = s + lane; k < e; k += 32) sum += val[k] * x[col[k]];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+        if (lane == 0) b[rows ? rows[i] : i] -= sum;
     }
 }
 

@@ -552,9 +552,15 @@ int launch_blocks(Plan &P, std::string &err) {
         } else if (B.kernel == RBS_K_SPMV) {
             const int g = K == 1 ? B.group : (K < 32 ? K : 32);
             const int *rows = B.rows_off >= 0 ? D.rows + B.rows_off : nullptr;
+            const bool med = K == 1 && B.medrows > 0;
+            const int maxlen = med ? RBS_MEDROW : B.longrows > 0 ? RBS_LONGROW : 0x7fffffff;
             k_spmv_sub<VT, K><<<grid_for((long long)B.nrows * g, 256, D.num_sms), 256, 0, st>>>(
                 D.rp + B.rp_off, D.col, val, rows, B.nrows, B.group, xw + (long long)B.c0 * K,
-                bw + (long long)B.r0 * K, B.longrows > 0);
+                bw + (long long)B.r0 * K, maxlen);
+            if (med)
+                k_spmv_rows<VT><<<grid_for((long long)B.medrows * 32, 256, D.num_sms), 256, 0, st>>>(
+                    D.rp + B.rp_off, D.col, val, rows, D.rows + B.med_off, B.medrows, xw + (long long)B.c0 * K,
+                    bw + (long long)B.r0 * K);
             if (B.longrows > 0)
                 k_spmv_long<VT, K><<<D.num_sms * 2, 256, 0, st>>>(D.rp + B.rp_off, D.col, val, rows,
                                                                   D.rows + B.long_off, B.longrows,
