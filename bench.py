@@ -53,7 +53,7 @@ def parse():
                     help="structure of the timed solve (profiling runs; the benchmark line is c1a)")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, side measurements and the CPU baseline "
                                                                "(short runs for profilers)")
-    ap.add_argument("--side", default=None, choices=["analysis", "batched", "ic0", "ilu0", "mtx", "serve"],
+    ap.add_argument("--side", default=None, choices=["analysis", "batched", "blocks", "ic0", "ilu0", "mtx", "serve"],
                     help="run one side measurement alone on cuda:0 and print its JSON (no benchmark line)")
     return ap.parse_args()
 
@@ -873,9 +873,38 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def side_blocks(dev, args):
+    """Per-block device time of the --case structure, forward and backward:
+    CUDA events around every block (eager launches), the ten slowest blocks
+    with their kernel, rows and entries, and the graph-replayed solve time."""
+    import torch
+
+    import rbs
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    out = {}
+    for sub, tag in ((rbs.FORWARD, "fwd"), (rbs.BACKWARD, "bwd")):
+        s = make_system(args.case, sub)
+        db = torch.tensor(s["b"], device=dev)
+        dx = torch.empty_like(db)
+        p = rbs.analyse(s["cp"], s["ri"], s["cv"], substitution=sub, lv=-1)
+        ms, _ = measure(p, db, dx, flush, 20)
+        p.profile(True)
+        timed_solves(p, db, dx, 10, flush)
+        bms, _, n = p.block_times()
+        p.profile(False)
+        kern, bm, bnnz = p.export("kernel"), p.export("blk_m"), p.export("blk_nnz")
+        top = np.argsort(-np.asarray(bms))[:10]
+        out[tag] = {"graph_ms": ms, "profiled_ms": float(sum(bms)) / max(n, 1),
+                    "blocks": [{"block": int(b), "kernel": rbs.KERNEL_NAMES[int(kern[b])], "rows": int(bm[b]),
+                                "entries": int(bnnz[b]), "ms": float(bms[b]) / max(n, 1)} for b in top]}
+        del p
+    return out
+
+
 # side measurements that take (device, args) and can run alone (--side)
 SIDE_SECTIONS = {"mtx": "side_mtx", "ic0": "side_ic0", "ilu0": "side_ilu0", "analysis": "side_analysis",
-                 "batched": "side_batched", "serve": "side_serving"}
+                 "batched": "side_batched", "serve": "side_serving", "blocks": "side_blocks"}
 
 
 def main():
