@@ -11,6 +11,13 @@ matrices the reference evaluates on (values U(-1,1), diagonal 1 + sum of
 write) before every timed solve: the factor (58.7 MB) fits in the 126 MB L2.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+  python bench.py --side analysis|batched|blocks|ic0|ilu0|mtx|serve [--case c1b]
+
+The headline value is timed on the block walk replayed from its CUDA graph;
+the roofline's per-kernel times come from a second pass of the same steps
+with CUDA events around every block.  Side measurements (multi-RHS, other
+structures, mixed precision, analysis, factors, Matrix Market input,
+batched systems, serving) follow on one GPU; --side runs one alone.
 
 N > 1 runs N independent replicas (the solve has no data-path collective:
 a triangular solve is one dependency chain), one process per GPU launched by
