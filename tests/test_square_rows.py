@@ -45,3 +45,28 @@ def test_square_medium_rows_listed(long_len, expect_rows):
     # the square's rows: 2 (or long_len) entries; rows of more than 2048
     # entries go to the long-row kernel instead
     assert med[1] == expect_rows
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("long_len", [40, 700, 2048, 3000])
+def test_square_with_long_rows_solves(cuda, long_len):
+    # the warp-per-row pass (and, past 2048 entries, the long-row kernel)
+    # against the serial oracle; the warp-per-row sum has a fixed order, so
+    # two solves agree bit for bit when no row is longer than 2048
+    import torch
+    from _util import rel_err
+    n = 8000
+    long_rows = {n // 2 + 3, n // 2 + 999, n - 2}
+    rp, ci, va = chain_with_long_rows(n, long_rows, long_len, 9)
+    cp, ri, cv = oracle.transpose(rp, ci, va)
+    plan = rbs.analyse(cp, ri, cv, substitution=rbs.FORWARD, lv=1)
+    assert plan.export("medrow")[1] == (3 if long_len <= 2048 else 0)
+    b = rbs.gen_uniform(10, n)
+    x_ref = oracle.sptrsv_csr(rp, ci, va, rbs.FORWARD, b)
+    db = torch.tensor(b, device=cuda)
+    x1, x2 = torch.empty_like(db), torch.empty_like(db)
+    plan.solve(db, x1)
+    plan.solve(db, x2)
+    assert rel_err(x1.cpu().numpy(), x_ref) <= 1e-12
+    if long_len <= 2048:
+        assert torch.equal(x1, x2)
