@@ -88,7 +88,7 @@ int pick_group(double avg) {
 
 // Kernel choice.  REFERENCE maps each reference method to this library's
 // kernel of the same kind; AUTO uses a latency/bandwidth cost model of the
-// B200 (constants measured with bench.py, see DESIGN notes in the repo).
+// B200 (constants measured on a B200 with bench.py).
 void select_kernel(ExecBlock &b, const rbs_options &opt, const std::vector<int> &lvl_sizes) {
     if (!b.tri) {
         if (b.nnz == 0) {

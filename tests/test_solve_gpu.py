@@ -1,5 +1,5 @@
 """Parity of the CUDA solve with the serial FP64 oracle (tolerance: relative
-2-norm error <= 1e-12, the bound the north-star metric states), through the
+2-norm error <= 1e-12, the bound of the solve metric), through the
 C ABI, on every golden case, both directions, every selection mode,
 multi-RHS and mixed precision."""
 import numpy as np
