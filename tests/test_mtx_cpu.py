@@ -113,3 +113,30 @@ def test_library_missing_file(tmp_path):
     with pytest.raises(rbs.RbsError) as e:
         rbs.mtx_read(str(tmp_path / "absent.mtx"))
     assert e.value.code == rbs.ERR_ARG
+
+
+@pytest.mark.parametrize("kind", ["general", "symmetric", "pattern"])
+def test_writer_round_trips_through_the_oracle_reader(tmp_path, kind):
+    # rbs_mtx_write is host code: %.17g values read back bit for bit by the
+    # reference-style reader; symmetric files hold the lower triangle
+    rp, ci, va = rbs.gen_lower_csr(rbs.GEN_ZIPF, n=3000, zipf_alpha=2.1, zipf_max=50, seed=21)
+    va = va * 10.0 ** np.random.default_rng(22).integers(-30, 30, len(va))
+    path = str(tmp_path / "w.mtx")
+    rbs.mtx_write(path, rp, ci, None if kind == "pattern" else va, symmetric=kind == "symmetric")
+    o = oracle.mtx_read(path)
+    n = len(rp) - 1
+    if kind == "general":
+        np.testing.assert_array_equal(o["rowptr"], rp)
+        np.testing.assert_array_equal(o["colidx"], ci)
+        np.testing.assert_array_equal(o["val"].view(np.uint64), va.view(np.uint64))
+    elif kind == "pattern":
+        assert o["field"] == 2
+        np.testing.assert_array_equal(o["colidx"], ci)
+        assert (o["val"] == 1.0).all()
+    else:
+        assert o["symmetric"] == 1
+        rows = np.repeat(np.arange(n), np.diff(o["rowptr"]))
+        low = o["colidx"] <= rows
+        np.testing.assert_array_equal(o["colidx"][low], ci)
+        np.testing.assert_array_equal(o["val"][low].view(np.uint64), va.view(np.uint64))
+        assert int((~low).sum()) == int((ci < np.repeat(np.arange(n), np.diff(rp))).sum())
