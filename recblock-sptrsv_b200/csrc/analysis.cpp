@@ -542,30 +542,24 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
         pos_of[orig] = i;
     }
 
-    // 4. processing-order CSR with columns ascending (two stable counting
-    //    sorts: by column, then by row)
+    // 4. processing-order CSR with columns ascending: rows counted, then the
+    //    columns walked in processing order (column perm[q] is processing
+    //    column q), each appending its entries to their rows -- the result
+    //    of a stable sort by column and then by row, in one pass
     {
-        std::vector<int> P_of((size_t)nnz), Q_of((size_t)nnz);
-        for (int c = 0; c < n; ++c)
-            for (int k = cp[c]; k < cp[c + 1]; ++k) {
-                P_of[k] = pos_of[ri[k]];
-                Q_of[k] = pos_of[c];
-            }
-        std::vector<int> byq((size_t)n + 1, 0), order1((size_t)nnz);
-        for (int k = 0; k < nnz; ++k) byq[(size_t)Q_of[k] + 1]++;
-        for (int q = 0; q < n; ++q) byq[(size_t)q + 1] += byq[q];
-        for (int k = 0; k < nnz; ++k) order1[byq[Q_of[k]]++] = k;
         P.full_rp.assign((size_t)n + 1, 0);
-        for (int k = 0; k < nnz; ++k) P.full_rp[(size_t)P_of[k] + 1]++;
+        for (int k = 0; k < nnz; ++k) P.full_rp[(size_t)pos_of[ri[k]] + 1]++;
         for (int p = 0; p < n; ++p) P.full_rp[(size_t)p + 1] += P.full_rp[p];
         std::vector<int> fill(P.full_rp.begin(), P.full_rp.end() - 1);
         P.full_col.resize((size_t)nnz);
         P.full_val.resize((size_t)nnz);
-        for (int t = 0; t < nnz; ++t) {
-            int k = order1[t];
-            int d = fill[P_of[k]]++;
-            P.full_col[d] = Q_of[k];
-            P.full_val[d] = va[k];
+        for (int q = 0; q < n; ++q) {
+            const int c = P.perm[q];
+            for (int k = cp[c]; k < cp[c + 1]; ++k) {
+                const int d = fill[pos_of[ri[k]]]++;
+                P.full_col[d] = q;
+                P.full_val[d] = va[k];
+            }
         }
     }
     P.analyse_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
