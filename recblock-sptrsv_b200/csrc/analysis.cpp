@@ -855,61 +855,6 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
             }
         }
     }
-    // 9. ELL chunks of single-CTA triangles (the CTA sync-free kernel,
-    //    cta_syncfree.cuh): chunks of <= 512 rows and <= 2048 ELL slots,
-    //    column-major inside a chunk, padding column -1
-    P.ell_col.clear();
-    P.ell_val.clear();
-    P.ell_chunks.clear();
-    constexpr int RMAX = 512, EMAX = 2048;
-    for (ExecBlock &B : P.blocks) {
-        if (!wants_level(B, opt)) continue;
-        const int *rp = P.rp_pool.data() + B.rp_off;
-        std::vector<int> cuts{0}, widths;
-        bool ok = true;
-        int w = 0, rows = 0;
-        for (int r = 0; r < B.m && ok; ++r) {
-            const int len = rp[r + 1] - rp[r];
-            if (len > EMAX) ok = false;
-            const int w2 = std::max(w, len);
-            if (rows == RMAX || (long long)(rows + 1) * w2 > EMAX) {
-                cuts.push_back(r);
-                widths.push_back(w);
-                w = len;
-                rows = 1;
-            } else {
-                w = w2;
-                ++rows;
-            }
-        }
-        if (!ok) continue;
-        cuts.push_back(B.m);
-        widths.push_back(w);
-        const int nch = (int)widths.size();
-        B.ell_ok = 1;
-        B.ell_nchunks = nch;
-        B.ell_chunk_off = (long long)P.ell_chunks.size() / 4;
-        B.ell_lo = (long long)P.ell_col.size();
-        for (int q = 0; q < nch; ++q) {
-            while (P.ell_col.size() % 4) {  // 16-byte aligned chunk starts
-                P.ell_col.push_back(-1);
-                P.ell_val.push_back(0.0);
-            }
-            const int R0 = cuts[q], R1 = cuts[q + 1], W = widths[q], R = R1 - R0;
-            const long long off = (long long)P.ell_col.size();
-            P.ell_chunks.insert(P.ell_chunks.end(), {R0, R1, W, (int)off});
-            P.ell_col.resize(P.ell_col.size() + (size_t)R * W, -1);
-            P.ell_val.resize(P.ell_val.size() + (size_t)R * W, 0.0);
-            for (int i = 0; i < R; ++i) {
-                const int r = R0 + i;
-                for (int j = 0; j < rp[r + 1] - rp[r]; ++j) {
-                    P.ell_col[(size_t)(off + (long long)j * R + i)] = P.col_pool[rp[r] + j];
-                    P.ell_val[(size_t)(off + (long long)j * R + i)] = P.val_pool[rp[r] + j];
-                }
-            }
-        }
-        B.ell_hi = (long long)P.ell_col.size();
-    }
     // 10. level-ELL layout of level triangles with narrow levels (<= 1024
     //     rows) and short rows (<= 4 entries): the cp.async-staged kernel
     //     (level_ca.cuh).  Per level a table entry {lo, off, w, 0}; the block's
@@ -966,13 +911,77 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
                                                              : (P.ca_col[(size_t)e] & (CA_WINDOW_ROWS - 1));
         }
     }
-    if (P.ell_col.size() > (size_t)0x7fffffff || P.ca_col.size() > (size_t)0x7fffffff) {
+    if (P.ca_col.size() > (size_t)0x7fffffff) {
         err = "rbs_analyse: ELL pool too large";
         return RBS_ERR_NOMEM;
     }
     // 11. level-chunk records (level_lc.cuh) and the level kernel of every
     //     level triangle
     build_lc(P, opt, level);
+    // 12. ELL chunks of single-CTA triangles (the CTA sync-free kernel,
+    //    cta_syncfree.cuh): chunks of <= 512 rows and <= 2048 ELL slots,
+    //    column-major inside a chunk, padding column -1; built after the
+    //    staged and chunk layouts, for the triangles that have neither (or,
+    //    when tuning, for every candidate)
+    P.ell_col.clear();
+    P.ell_val.clear();
+    P.ell_chunks.clear();
+    constexpr int RMAX = 512, EMAX = 2048;
+    for (ExecBlock &B : P.blocks) {
+        if (!wants_level(B, opt)) continue;
+        // only the kernel choice's fallback outside tuning: a triangle with a
+        // staged or chunk layout never runs this kernel then
+        if (opt.select != RBS_SELECT_TUNE && (B.ca_ok || B.lc_ok)) continue;
+        const int *rp = P.rp_pool.data() + B.rp_off;
+        std::vector<int> cuts{0}, widths;
+        bool ok = true;
+        int w = 0, rows = 0;
+        for (int r = 0; r < B.m && ok; ++r) {
+            const int len = rp[r + 1] - rp[r];
+            if (len > EMAX) ok = false;
+            const int w2 = std::max(w, len);
+            if (rows == RMAX || (long long)(rows + 1) * w2 > EMAX) {
+                cuts.push_back(r);
+                widths.push_back(w);
+                w = len;
+                rows = 1;
+            } else {
+                w = w2;
+                ++rows;
+            }
+        }
+        if (!ok) continue;
+        cuts.push_back(B.m);
+        widths.push_back(w);
+        const int nch = (int)widths.size();
+        B.ell_ok = 1;
+        B.ell_nchunks = nch;
+        B.ell_chunk_off = (long long)P.ell_chunks.size() / 4;
+        B.ell_lo = (long long)P.ell_col.size();
+        for (int q = 0; q < nch; ++q) {
+            while (P.ell_col.size() % 4) {  // 16-byte aligned chunk starts
+                P.ell_col.push_back(-1);
+                P.ell_val.push_back(0.0);
+            }
+            const int R0 = cuts[q], R1 = cuts[q + 1], W = widths[q], R = R1 - R0;
+            const long long off = (long long)P.ell_col.size();
+            P.ell_chunks.insert(P.ell_chunks.end(), {R0, R1, W, (int)off});
+            P.ell_col.resize(P.ell_col.size() + (size_t)R * W, -1);
+            P.ell_val.resize(P.ell_val.size() + (size_t)R * W, 0.0);
+            for (int i = 0; i < R; ++i) {
+                const int r = R0 + i;
+                for (int j = 0; j < rp[r + 1] - rp[r]; ++j) {
+                    P.ell_col[(size_t)(off + (long long)j * R + i)] = P.col_pool[rp[r] + j];
+                    P.ell_val[(size_t)(off + (long long)j * R + i)] = P.val_pool[rp[r] + j];
+                }
+            }
+        }
+        B.ell_hi = (long long)P.ell_col.size();
+    }
+    if (P.ell_col.size() > (size_t)0x7fffffff) {
+        err = "rbs_analyse: ELL pool too large";
+        return RBS_ERR_NOMEM;
+    }
     for (ExecBlock &B : P.blocks) {
         if (!B.tri || B.kernel != RBS_K_LEVEL) continue;
         // staged level-ELL first (short rows, narrow levels: its per-level cost
