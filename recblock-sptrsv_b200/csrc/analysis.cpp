@@ -9,6 +9,8 @@
 // (recblocking_preprocess.h get_recblock_size + L_/U_preprocessing); the
 // packed reference-format arrays are rebuilt on demand by export_reference.
 #include <algorithm>
+#include <thread>
+#include <atomic>
 #include <chrono>
 #include <climits>
 #include <cmath>
@@ -171,269 +173,307 @@ static bool wants_band(const ExecBlock &b, const rbs_options &opt) {
 // shared-memory ring in order, wrapping to 0 when the next one does not
 // fit; a record's copy is issued once every chunk whose ring bytes it reuses
 // has been solved and its mbarrier slot is free.
+// One triangle's level-chunk layout into `out`, record and table offsets
+// relative to `out` (build_lc merges the blocks in order and rebases them).
+struct LcOut {
+    std::vector<uint32_t> rec64, rec32;
+    std::vector<int> tab, segs;
+};
+static void build_lc_block(const Plan &P, ExecBlock &B, const rbs_options &opt, const std::vector<int> &level,
+                           LcOut &out) {
+    B.lc_ok = 0;
+    B.lc_nseg = 0;
+    B.lc_seg_off = -1;
+    if (!wants_level(B, opt) || B.nnz == B.m) return;
+    const int m = B.m;
+    const int *rp = P.rp_pool.data() + B.rp_off;
+    const int *cl = P.col_pool.data();
+    const double *vl = P.val_pool.data();
+    // segment of every row (ids in order of first appearance)
+    int nseg = 1;
+    std::vector<int> seg((size_t)m, 0);
+    if (!P.seg_rows.empty()) {
+        std::vector<int> id(P.seg_rows.size(), -1);
+        nseg = 0;
+        for (int r = 0; r < m; ++r) {
+            const int o = P.perm[(size_t)B.r0 + r];
+            const int sgi = (int)(std::upper_bound(P.seg_rows.begin(), P.seg_rows.end(), o) - P.seg_rows.begin()) - 1;
+            if (id[(size_t)sgi] < 0) id[(size_t)sgi] = nseg++;
+            seg[(size_t)r] = id[(size_t)sgi];
+        }
+    }
+    // rows level by level (stable), then split by segment
+    std::vector<int> lstart((size_t)B.nlv + 1, 0);
+    for (int r = 0; r < m; ++r) lstart[(size_t)level[(size_t)B.r0 + r] + 1]++;
+    for (int l = 0; l < B.nlv; ++l) lstart[(size_t)l + 1] += lstart[(size_t)l];
+    std::vector<int> bylev((size_t)m);
+    {
+        std::vector<int> fill(lstart.begin(), lstart.end() - 1);
+        for (int r = 0; r < m; ++r) bylev[(size_t)fill[(size_t)level[(size_t)B.r0 + r]]++] = r;
+    }
+    std::vector<int> scount((size_t)nseg + 1, 0);
+    for (int r = 0; r < m; ++r) scount[(size_t)seg[(size_t)r] + 1]++;
+    for (int q = 0; q < nseg; ++q) scount[(size_t)q + 1] += scount[(size_t)q];
+    std::vector<int> seq((size_t)m);
+    {
+        std::vector<int> fill(scount.begin(), scount.end() - 1);
+        for (int t = 0; t < m; ++t) {
+            const int r = bylev[(size_t)t];
+            seq[(size_t)fill[(size_t)seg[(size_t)r]]++] = r;
+        }
+    }
+    // chunks; seq is reordered inside every chunk and vpos assigned
+    struct Ch { int v0, nr, no, nrec, ncols, maxlen; };
+    std::vector<std::vector<Ch>> chunks((size_t)nseg);
+    std::vector<int> vpos((size_t)m, -1), rl((size_t)LC_RMAX);
+    auto counts = [&](const int *rows, int nr, int thr, int &no, int &nrec, int &ncols) {
+        no = nrec = ncols = 0;
+        for (int t = 0; t < nr; ++t) {
+            const int r = rows[t];
+            int rr = 0;
+            for (int k = rp[r]; k < rp[r + 1]; ++k) rr += vpos[(size_t)cl[k]] >= thr;
+            rl[(size_t)t] = rr;
+            nrec += rr;
+            no += rp[r + 1] - rp[r] - rr;
+            ncols = std::max(ncols, rr);
+        }
+    };
+    bool ok = true;
+    for (int q = 0; q < nseg && ok; ++q) {
+        int *sq = seq.data() + scount[(size_t)q];
+        const int len = scount[(size_t)q + 1] - scount[(size_t)q];
+        auto &ch = chunks[(size_t)q];
+        int i = 0;
+        while (i < len) {
+            const int L = level[(size_t)B.r0 + sq[i]];
+            const int thr_c = i + LC_RMAX - LC_XW;  // no later threshold is larger
+            int nr = 0, no = 0, nrec = 0, ncols = 0;
+            while (i + nr < len && nr < LC_RMAX && level[(size_t)B.r0 + sq[i + nr]] == L) {
+                const int r = sq[i + nr];
+                int ro = 0, rr = 0;
+                for (int k = rp[r]; k < rp[r + 1]; ++k) (vpos[(size_t)cl[k]] < thr_c ? ro : rr)++;
+                if (lc_foot_bytes(nr + 1, no + ro, nrec + rr, std::max(ncols, rr), 8) > LC_FMAX) break;
+                ++nr;
+                no += ro;
+                nrec += rr;
+                ncols = std::max(ncols, rr);
+            }
+            if (nr == 0) {  // one row alone does not fit the ring
+                ok = false;
+                break;
+            }
+            // exact split with this chunk's own threshold
+            for (;;) {
+                counts(sq + i, nr, i + nr - LC_XW, no, nrec, ncols);
+                if (lc_foot_bytes(nr, no, nrec, ncols, 8) <= LC_FMAX || nr == 1) break;
+                --nr;
+            }
+            if (lc_foot_bytes(nr, no, nrec, ncols, 8) > LC_FMAX) {
+                ok = false;
+                break;
+            }
+            // rows by recent count, largest first (stable)
+            std::vector<int> idx((size_t)nr);
+            for (int t = 0; t < nr; ++t) idx[(size_t)t] = t;
+            std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return rl[(size_t)a] > rl[(size_t)b]; });
+            std::vector<int> rows((size_t)nr);
+            for (int t = 0; t < nr; ++t) rows[(size_t)t] = sq[i + idx[(size_t)t]];
+            for (int t = 0; t < nr; ++t) {
+                sq[i + t] = rows[(size_t)t];
+                vpos[(size_t)rows[(size_t)t]] = i + t;
+            }
+            int maxlen = 0;
+            for (int t = 0; t < nr; ++t) maxlen = std::max(maxlen, rp[rows[(size_t)t] + 1] - rp[rows[(size_t)t]]);
+            ch.push_back({i, nr, no, nrec, ncols, maxlen});
+            i += nr;
+        }
+    }
+    if (!ok) return;
+    // ring placement and issue iterations
+    std::vector<std::vector<int>> roff((size_t)nseg), iss((size_t)nseg);
+    for (int q = 0; q < nseg && ok; ++q) {
+        const auto &ch = chunks[(size_t)q];
+        const int nch = (int)ch.size();
+        auto &ro = roff[(size_t)q];
+        auto &is = iss[(size_t)q];
+        ro.resize((size_t)nch);
+        is.resize((size_t)nch);
+        long long head = 0;
+        std::vector<long long> fb((size_t)nch);
+        for (int j = 0; j < nch; ++j) {
+            const Ch &c = ch[(size_t)j];
+            const long long F = lc_foot_bytes(c.nr, c.no, c.nrec, c.ncols, 8);
+            fb[(size_t)j] = F;
+            if (head + F > LC_RING) head = 0;
+            ro[(size_t)j] = (int)(head / 16);
+            head += F;
+            // mbarrier slot j % LC_NB: every thread must have seen chunk j - LC_NB
+            // land (its gather, at chunk iteration j - LC_NB - LC_D or in the
+            // prologue) and passed a CTA barrier since, i.e. the end of that
+            // iteration (iteration 0 for chunks gathered in the prologue)
+            int at = j > 0 ? is[(size_t)j - 1] : 0;
+            if (j >= LC_NB) at = std::max(at, std::max(1, j - LC_NB - LC_D + 1));
+            long long scanned = 0;
+            for (int k = j - 1; k >= 0 && scanned <= 2LL * LC_RING; --k) {
+                const long long a0 = 16LL * ro[(size_t)k], a1 = a0 + fb[(size_t)k];
+                const long long b0 = 16LL * ro[(size_t)j], b1 = b0 + F;
+                if (a0 < b1 && b0 < a1) {
+                    at = std::max(at, k + 1);
+                    break;
+                }
+                scanned += fb[(size_t)k];
+            }
+            if (at > std::max(0, j - LC_D)) ok = false;
+            is[(size_t)j] = at;
+        }
+    }
+    if (!ok) return;
+    // records
+    B.lc_ok = 1;
+    B.lc_nseg = nseg;
+    B.lc_seg_off = 0;  // set when the blocks are merged
+    std::vector<int> order((size_t)nseg);
+    for (int q = 0; q < nseg; ++q) order[(size_t)q] = q;
+    auto work = [&](int q) {
+        long long e = 0;
+        for (const Ch &c : chunks[(size_t)q]) e += c.no + c.nrec;
+        return (long long)chunks[(size_t)q].size() * 4096 + e;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+    std::vector<int> dest, rlen, rpo, cs, colr, colo;
+    std::vector<double> inv, valr, valo;
+    for (int q : order) {
+        const int *sq = seq.data() + scount[(size_t)q];
+        const auto &ch = chunks[(size_t)q];
+        const int nch = (int)ch.size();
+        out.segs.insert(out.segs.end(), {(int)(out.tab.size() / LC_TAB_INTS), nch, nch ? roff[(size_t)q][0] : 0});
+        for (int j = 0; j < nch; ++j) {
+            const Ch &c = ch[(size_t)j];
+            const int thr = c.v0 + c.nr - LC_XW;
+            dest.assign((size_t)c.nr, 0);
+            rlen.assign((size_t)c.nr, 0);
+            rpo.assign(1, 0);
+            inv.assign((size_t)c.nr, 0.0);
+            colo.clear();
+            valo.clear();
+            for (int t = 0; t < c.nr; ++t) {
+                const int r = sq[c.v0 + t];
+                dest[(size_t)t] = r;
+                inv[(size_t)t] = P.inv_diag[(size_t)B.r0 + r];
+                for (int k = rp[r]; k < rp[r + 1]; ++k) {
+                    if (vpos[(size_t)cl[k]] >= thr) rlen[(size_t)t]++;
+                    else {
+                        colo.push_back(cl[k]);
+                        valo.push_back(vl[k]);
+                    }
+                }
+                rpo.push_back((int)colo.size());
+            }
+            cs.assign((size_t)c.ncols + 1, 0);
+            for (int k = 0; k < c.ncols; ++k) {
+                int cnt = 0;
+                while (cnt < c.nr && rlen[(size_t)cnt] > k) ++cnt;  // rlen is non-increasing
+                cs[(size_t)k + 1] = cs[(size_t)k] + cnt;
+            }
+            colr.assign((size_t)c.nrec, 0);
+            valr.assign((size_t)c.nrec, 0.0);
+            for (int t = 0; t < c.nr; ++t) {
+                const int r = sq[c.v0 + t];
+                int kk = 0;
+                for (int k = rp[r]; k < rp[r + 1]; ++k) {
+                    const int vd = vpos[(size_t)cl[k]];
+                    if (vd < thr) continue;
+                    colr[(size_t)(cs[(size_t)kk] + t)] = vd & (LC_XW - 1);
+                    valr[(size_t)(cs[(size_t)kk] + t)] = vl[k];
+                    ++kk;
+                }
+            }
+            const int rnext = j + 1 < nch ? roff[(size_t)q][(size_t)j + 1] : 0;
+            // contiguous block rows: the kernel bulk-copies their right-hand side
+            int dmin = dest[0], dmax = dest[0];
+            for (int t = 1; t < c.nr; ++t) {
+                dmin = std::min(dmin, dest[(size_t)t]);
+                dmax = std::max(dmax, dest[(size_t)t]);
+            }
+            const int blo = dmax - dmin + 1 == c.nr ? dmin : -1;
+            auto emit = [&](std::vector<uint32_t> &pool, int es) -> std::pair<int, int> {
+                const size_t base = pool.size();
+                const long long bytes = lc_static_bytes(c.nr, c.no, c.nrec, c.ncols, es);
+                pool.resize(base + (size_t)(bytes / 4), 0u);
+                uint32_t *w = pool.data() + base;
+                const int hdr[LC_HDR_INTS] = {c.nr, c.no, c.nrec, c.v0, rnext, c.ncols, c.maxlen, blo};
+                std::memcpy(w, hdr, sizeof(hdr));
+                size_t o = LC_HDR_INTS;
+                auto put_i = [&](const std::vector<int> &v) {
+                    if (!v.empty()) std::memcpy(w + o, v.data(), v.size() * 4);
+                    o += (size_t)lc_pad4((int)v.size());
+                };
+                auto put_v = [&](const std::vector<double> &v) {
+                    if (es == 8) {
+                        if (!v.empty()) std::memcpy(w + o, v.data(), v.size() * 8);
+                    } else {
+                        for (size_t t = 0; t < v.size(); ++t) {
+                            const float f = (float)v[t];
+                            std::memcpy(w + o + t, &f, 4);
+                        }
+                    }
+                    o += (size_t)(lc_padv((int)v.size(), es) / 4);
+                };
+                put_i(dest);
+                put_i(rlen);
+                put_i(rpo);
+                put_i(cs);
+                put_v(inv);
+                put_i(colr);
+                put_v(valr);
+                put_i(colo);
+                put_v(valo);
+                return {(int)(base / 4), (int)(bytes / 16)};
+            };
+            const auto r64 = emit(out.rec64, 8);
+            const auto r32 = emit(out.rec32, 4);
+            const int bs64 = (int)((lc_static_bytes(c.nr, c.no, c.nrec, c.ncols, 8) + lc_padv(c.no, 8)) / 16);
+            const int bs32 = (int)((lc_static_bytes(c.nr, c.no, c.nrec, c.ncols, 4) + lc_padv(c.no, 4)) / 16);
+            out.tab.insert(out.tab.end(), {r64.first, r64.second, r32.first, r32.second, roff[(size_t)q][(size_t)j],
+                                             iss[(size_t)q][(size_t)j], blo, blo >= 0 ? c.nr : 0, bs64, bs32});
+        }
+    }
+}
+
 static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &level) {
     P.lc_rec64.clear();
     P.lc_rec32.clear();
     P.lc_tab.clear();
     P.lc_segs.clear();
-    for (ExecBlock &B : P.blocks) {
-        B.lc_ok = 0;
-        B.lc_nseg = 0;
-        B.lc_seg_off = -1;
-        if (!wants_level(B, opt) || B.nnz == B.m) continue;
-        const int m = B.m;
-        const int *rp = P.rp_pool.data() + B.rp_off;
-        const int *cl = P.col_pool.data();
-        const double *vl = P.val_pool.data();
-        // segment of every row (ids in order of first appearance)
-        int nseg = 1;
-        std::vector<int> seg((size_t)m, 0);
-        if (!P.seg_rows.empty()) {
-            std::vector<int> id(P.seg_rows.size(), -1);
-            nseg = 0;
-            for (int r = 0; r < m; ++r) {
-                const int o = P.perm[(size_t)B.r0 + r];
-                const int sgi = (int)(std::upper_bound(P.seg_rows.begin(), P.seg_rows.end(), o) - P.seg_rows.begin()) - 1;
-                if (id[(size_t)sgi] < 0) id[(size_t)sgi] = nseg++;
-                seg[(size_t)r] = id[(size_t)sgi];
-            }
-        }
-        // rows level by level (stable), then split by segment
-        std::vector<int> lstart((size_t)B.nlv + 1, 0);
-        for (int r = 0; r < m; ++r) lstart[(size_t)level[(size_t)B.r0 + r] + 1]++;
-        for (int l = 0; l < B.nlv; ++l) lstart[(size_t)l + 1] += lstart[(size_t)l];
-        std::vector<int> bylev((size_t)m);
-        {
-            std::vector<int> fill(lstart.begin(), lstart.end() - 1);
-            for (int r = 0; r < m; ++r) bylev[(size_t)fill[(size_t)level[(size_t)B.r0 + r]]++] = r;
-        }
-        std::vector<int> scount((size_t)nseg + 1, 0);
-        for (int r = 0; r < m; ++r) scount[(size_t)seg[(size_t)r] + 1]++;
-        for (int q = 0; q < nseg; ++q) scount[(size_t)q + 1] += scount[(size_t)q];
-        std::vector<int> seq((size_t)m);
-        {
-            std::vector<int> fill(scount.begin(), scount.end() - 1);
-            for (int t = 0; t < m; ++t) {
-                const int r = bylev[(size_t)t];
-                seq[(size_t)fill[(size_t)seg[(size_t)r]]++] = r;
-            }
-        }
-        // chunks; seq is reordered inside every chunk and vpos assigned
-        struct Ch { int v0, nr, no, nrec, ncols, maxlen; };
-        std::vector<std::vector<Ch>> chunks((size_t)nseg);
-        std::vector<int> vpos((size_t)m, -1), rl((size_t)LC_RMAX);
-        auto counts = [&](const int *rows, int nr, int thr, int &no, int &nrec, int &ncols) {
-            no = nrec = ncols = 0;
-            for (int t = 0; t < nr; ++t) {
-                const int r = rows[t];
-                int rr = 0;
-                for (int k = rp[r]; k < rp[r + 1]; ++k) rr += vpos[(size_t)cl[k]] >= thr;
-                rl[(size_t)t] = rr;
-                nrec += rr;
-                no += rp[r + 1] - rp[r] - rr;
-                ncols = std::max(ncols, rr);
-            }
-        };
-        bool ok = true;
-        for (int q = 0; q < nseg && ok; ++q) {
-            int *sq = seq.data() + scount[(size_t)q];
-            const int len = scount[(size_t)q + 1] - scount[(size_t)q];
-            auto &ch = chunks[(size_t)q];
-            int i = 0;
-            while (i < len) {
-                const int L = level[(size_t)B.r0 + sq[i]];
-                const int thr_c = i + LC_RMAX - LC_XW;  // no later threshold is larger
-                int nr = 0, no = 0, nrec = 0, ncols = 0;
-                while (i + nr < len && nr < LC_RMAX && level[(size_t)B.r0 + sq[i + nr]] == L) {
-                    const int r = sq[i + nr];
-                    int ro = 0, rr = 0;
-                    for (int k = rp[r]; k < rp[r + 1]; ++k) (vpos[(size_t)cl[k]] < thr_c ? ro : rr)++;
-                    if (lc_foot_bytes(nr + 1, no + ro, nrec + rr, std::max(ncols, rr), 8) > LC_FMAX) break;
-                    ++nr;
-                    no += ro;
-                    nrec += rr;
-                    ncols = std::max(ncols, rr);
-                }
-                if (nr == 0) {  // one row alone does not fit the ring
-                    ok = false;
-                    break;
-                }
-                // exact split with this chunk's own threshold
-                for (;;) {
-                    counts(sq + i, nr, i + nr - LC_XW, no, nrec, ncols);
-                    if (lc_foot_bytes(nr, no, nrec, ncols, 8) <= LC_FMAX || nr == 1) break;
-                    --nr;
-                }
-                if (lc_foot_bytes(nr, no, nrec, ncols, 8) > LC_FMAX) {
-                    ok = false;
-                    break;
-                }
-                // rows by recent count, largest first (stable)
-                std::vector<int> idx((size_t)nr);
-                for (int t = 0; t < nr; ++t) idx[(size_t)t] = t;
-                std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return rl[(size_t)a] > rl[(size_t)b]; });
-                std::vector<int> rows((size_t)nr);
-                for (int t = 0; t < nr; ++t) rows[(size_t)t] = sq[i + idx[(size_t)t]];
-                for (int t = 0; t < nr; ++t) {
-                    sq[i + t] = rows[(size_t)t];
-                    vpos[(size_t)rows[(size_t)t]] = i + t;
-                }
-                int maxlen = 0;
-                for (int t = 0; t < nr; ++t) maxlen = std::max(maxlen, rp[rows[(size_t)t] + 1] - rp[rows[(size_t)t]]);
-                ch.push_back({i, nr, no, nrec, ncols, maxlen});
-                i += nr;
-            }
-        }
-        if (!ok) continue;
-        // ring placement and issue iterations
-        std::vector<std::vector<int>> roff((size_t)nseg), iss((size_t)nseg);
-        for (int q = 0; q < nseg && ok; ++q) {
-            const auto &ch = chunks[(size_t)q];
-            const int nch = (int)ch.size();
-            auto &ro = roff[(size_t)q];
-            auto &is = iss[(size_t)q];
-            ro.resize((size_t)nch);
-            is.resize((size_t)nch);
-            long long head = 0;
-            std::vector<long long> fb((size_t)nch);
-            for (int j = 0; j < nch; ++j) {
-                const Ch &c = ch[(size_t)j];
-                const long long F = lc_foot_bytes(c.nr, c.no, c.nrec, c.ncols, 8);
-                fb[(size_t)j] = F;
-                if (head + F > LC_RING) head = 0;
-                ro[(size_t)j] = (int)(head / 16);
-                head += F;
-                // mbarrier slot j % LC_NB: every thread must have seen chunk j - LC_NB
-                // land (its gather, at chunk iteration j - LC_NB - LC_D or in the
-                // prologue) and passed a CTA barrier since, i.e. the end of that
-                // iteration (iteration 0 for chunks gathered in the prologue)
-                int at = j > 0 ? is[(size_t)j - 1] : 0;
-                if (j >= LC_NB) at = std::max(at, std::max(1, j - LC_NB - LC_D + 1));
-                long long scanned = 0;
-                for (int k = j - 1; k >= 0 && scanned <= 2LL * LC_RING; --k) {
-                    const long long a0 = 16LL * ro[(size_t)k], a1 = a0 + fb[(size_t)k];
-                    const long long b0 = 16LL * ro[(size_t)j], b1 = b0 + F;
-                    if (a0 < b1 && b0 < a1) {
-                        at = std::max(at, k + 1);
-                        break;
-                    }
-                    scanned += fb[(size_t)k];
-                }
-                if (at > std::max(0, j - LC_D)) ok = false;
-                is[(size_t)j] = at;
-            }
-        }
-        if (!ok) continue;
-        // records
-        B.lc_ok = 1;
-        B.lc_nseg = nseg;
+    // blocks are independent: built on host threads, merged in block order
+    const size_t nb = P.blocks.size();
+    std::vector<LcOut> outs(nb);
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+        for (size_t b; (b = next.fetch_add(1)) < nb;) build_lc_block(P, P.blocks[b], opt, level, outs[b]);
+    };
+    const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nth; ++t) th.emplace_back(work);
+    work();
+    for (auto &t : th) t.join();
+    for (size_t b = 0; b < nb; ++b) {
+        ExecBlock &B = P.blocks[b];
+        if (!B.lc_ok) continue;
+        LcOut &o = outs[b];
+        const int tab_base = (int)(P.lc_tab.size() / LC_TAB_INTS);
+        const int r64_base = (int)(P.lc_rec64.size() / 4), r32_base = (int)(P.lc_rec32.size() / 4);
         B.lc_seg_off = (long long)P.lc_segs.size() / 3;
-        std::vector<int> order((size_t)nseg);
-        for (int q = 0; q < nseg; ++q) order[(size_t)q] = q;
-        auto work = [&](int q) {
-            long long e = 0;
-            for (const Ch &c : chunks[(size_t)q]) e += c.no + c.nrec;
-            return (long long)chunks[(size_t)q].size() * 4096 + e;
-        };
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
-        std::vector<int> dest, rlen, rpo, cs, colr, colo;
-        std::vector<double> inv, valr, valo;
-        for (int q : order) {
-            const int *sq = seq.data() + scount[(size_t)q];
-            const auto &ch = chunks[(size_t)q];
-            const int nch = (int)ch.size();
-            P.lc_segs.insert(P.lc_segs.end(), {(int)(P.lc_tab.size() / LC_TAB_INTS), nch, nch ? roff[(size_t)q][0] : 0});
-            for (int j = 0; j < nch; ++j) {
-                const Ch &c = ch[(size_t)j];
-                const int thr = c.v0 + c.nr - LC_XW;
-                dest.assign((size_t)c.nr, 0);
-                rlen.assign((size_t)c.nr, 0);
-                rpo.assign(1, 0);
-                inv.assign((size_t)c.nr, 0.0);
-                colo.clear();
-                valo.clear();
-                for (int t = 0; t < c.nr; ++t) {
-                    const int r = sq[c.v0 + t];
-                    dest[(size_t)t] = r;
-                    inv[(size_t)t] = P.inv_diag[(size_t)B.r0 + r];
-                    for (int k = rp[r]; k < rp[r + 1]; ++k) {
-                        if (vpos[(size_t)cl[k]] >= thr) rlen[(size_t)t]++;
-                        else {
-                            colo.push_back(cl[k]);
-                            valo.push_back(vl[k]);
-                        }
-                    }
-                    rpo.push_back((int)colo.size());
-                }
-                cs.assign((size_t)c.ncols + 1, 0);
-                for (int k = 0; k < c.ncols; ++k) {
-                    int cnt = 0;
-                    while (cnt < c.nr && rlen[(size_t)cnt] > k) ++cnt;  // rlen is non-increasing
-                    cs[(size_t)k + 1] = cs[(size_t)k] + cnt;
-                }
-                colr.assign((size_t)c.nrec, 0);
-                valr.assign((size_t)c.nrec, 0.0);
-                for (int t = 0; t < c.nr; ++t) {
-                    const int r = sq[c.v0 + t];
-                    int kk = 0;
-                    for (int k = rp[r]; k < rp[r + 1]; ++k) {
-                        const int vd = vpos[(size_t)cl[k]];
-                        if (vd < thr) continue;
-                        colr[(size_t)(cs[(size_t)kk] + t)] = vd & (LC_XW - 1);
-                        valr[(size_t)(cs[(size_t)kk] + t)] = vl[k];
-                        ++kk;
-                    }
-                }
-                const int rnext = j + 1 < nch ? roff[(size_t)q][(size_t)j + 1] : 0;
-                // contiguous block rows: the kernel bulk-copies their right-hand side
-                int dmin = dest[0], dmax = dest[0];
-                for (int t = 1; t < c.nr; ++t) {
-                    dmin = std::min(dmin, dest[(size_t)t]);
-                    dmax = std::max(dmax, dest[(size_t)t]);
-                }
-                const int blo = dmax - dmin + 1 == c.nr ? dmin : -1;
-                auto emit = [&](std::vector<uint32_t> &pool, int es) -> std::pair<int, int> {
-                    const size_t base = pool.size();
-                    const long long bytes = lc_static_bytes(c.nr, c.no, c.nrec, c.ncols, es);
-                    pool.resize(base + (size_t)(bytes / 4), 0u);
-                    uint32_t *w = pool.data() + base;
-                    const int hdr[LC_HDR_INTS] = {c.nr, c.no, c.nrec, c.v0, rnext, c.ncols, c.maxlen, blo};
-                    std::memcpy(w, hdr, sizeof(hdr));
-                    size_t o = LC_HDR_INTS;
-                    auto put_i = [&](const std::vector<int> &v) {
-                        if (!v.empty()) std::memcpy(w + o, v.data(), v.size() * 4);
-                        o += (size_t)lc_pad4((int)v.size());
-                    };
-                    auto put_v = [&](const std::vector<double> &v) {
-                        if (es == 8) {
-                            if (!v.empty()) std::memcpy(w + o, v.data(), v.size() * 8);
-                        } else {
-                            for (size_t t = 0; t < v.size(); ++t) {
-                                const float f = (float)v[t];
-                                std::memcpy(w + o + t, &f, 4);
-                            }
-                        }
-                        o += (size_t)(lc_padv((int)v.size(), es) / 4);
-                    };
-                    put_i(dest);
-                    put_i(rlen);
-                    put_i(rpo);
-                    put_i(cs);
-                    put_v(inv);
-                    put_i(colr);
-                    put_v(valr);
-                    put_i(colo);
-                    put_v(valo);
-                    return {(int)(base / 4), (int)(bytes / 16)};
-                };
-                const auto r64 = emit(P.lc_rec64, 8);
-                const auto r32 = emit(P.lc_rec32, 4);
-                const int bs64 = (int)((lc_static_bytes(c.nr, c.no, c.nrec, c.ncols, 8) + lc_padv(c.no, 8)) / 16);
-                const int bs32 = (int)((lc_static_bytes(c.nr, c.no, c.nrec, c.ncols, 4) + lc_padv(c.no, 4)) / 16);
-                P.lc_tab.insert(P.lc_tab.end(), {r64.first, r64.second, r32.first, r32.second, roff[(size_t)q][(size_t)j],
-                                                 iss[(size_t)q][(size_t)j], blo, blo >= 0 ? c.nr : 0, bs64, bs32});
-            }
+        for (size_t i = 0; i < o.segs.size(); i += 3) P.lc_segs.insert(P.lc_segs.end(), {o.segs[i] + tab_base, o.segs[i + 1], o.segs[i + 2]});
+        for (size_t i = 0; i < o.tab.size(); i += LC_TAB_INTS) {
+            o.tab[i] += r64_base;  // record starts, in 16-byte units
+            o.tab[i + 2] += r32_base;
         }
+        P.lc_tab.insert(P.lc_tab.end(), o.tab.begin(), o.tab.end());
+        P.lc_rec64.insert(P.lc_rec64.end(), o.rec64.begin(), o.rec64.end());
+        P.lc_rec32.insert(P.lc_rec32.end(), o.rec32.begin(), o.rec32.end());
+        LcOut().rec64.swap(o.rec64);
+        LcOut().rec32.swap(o.rec32);
     }
 }
 
