@@ -28,23 +28,66 @@ constexpr int kMedRow = 32;     // RBS_MEDROW (kernels.cuh)
 
 int lowbit(int t) { return t & -t; }
 
+// fn(i) for every i in [0, count) on up to 16 host threads (an atomic work
+// counter); fn writes only what index i owns.
+template <typename F> void parallel_for(size_t count, F &&fn) {
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+        for (size_t i; (i = next.fetch_add(1)) < count;) fn(i);
+    };
+    const unsigned nth = (unsigned)std::min<size_t>(count, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nth; ++t) th.emplace_back(work);
+    work();
+    for (auto &t : th) t.join();
+}
+
 // Stable CSR(rows x cols) -> CSC transposition (tranpose.h:7-54 semantics:
-// entries of a column appear in ascending row order).
-void transpose(int rows, int cols, const int *ptr, const int *idx, const double *val, std::vector<int> &tptr,
-               std::vector<int> &tidx, std::vector<double> &tval) {
+// entries of a column appear in ascending row order).  Large matrices are
+// transposed on host threads, each owning a range of output columns of about
+// equal size and scanning in order the rows of every row group whose column
+// span meets its range.
+template <typename IV, typename DV>
+void transpose(int rows, int cols, const int *ptr, const int *idx, const double *val, std::vector<int> &tptr, IV &tidx,
+               DV &tval) {
     int nnz = ptr[rows];
     tptr.assign((size_t)cols + 1, 0);
     for (int k = 0; k < nnz; ++k) tptr[(size_t)idx[k] + 1]++;
     for (int c = 0; c < cols; ++c) tptr[(size_t)c + 1] += tptr[c];
     tidx.resize((size_t)nnz);
     tval.resize(val ? (size_t)nnz : 0);
-    std::vector<int> fill(tptr.begin(), tptr.end() - 1);
-    for (int r = 0; r < rows; ++r)
-        for (int k = ptr[r]; k < ptr[r + 1]; ++k) {
-            int d = fill[idx[k]]++;
-            tidx[d] = r;
-            if (val) tval[d] = val[k];
+    const int parts = nnz < (1 << 20) ? 1 : 16;
+    std::vector<int> cut((size_t)parts + 1, cols);  // output columns [cut[t], cut[t+1])
+    for (int t = 1; t < parts; ++t)
+        cut[t] = (int)(std::lower_bound(tptr.begin(), tptr.end(), (int)((long long)nnz * t / parts)) - tptr.begin());
+    cut[0] = 0;
+    constexpr int kGroup = 256;  // rows per group
+    const int ngroup = (rows + kGroup - 1) / kGroup;
+    std::vector<int> gmin((size_t)ngroup, INT_MAX), gmax((size_t)ngroup, -1);  // column span of a group
+    if (parts > 1)
+        parallel_for(((size_t)ngroup + 1023) / 1024, [&](size_t i) {
+            for (int g = (int)i * 1024; g < std::min(ngroup, (int)i * 1024 + 1024); ++g)
+                for (int k = ptr[g * kGroup]; k < ptr[std::min(rows, g * kGroup + kGroup)]; ++k) {
+                    gmin[g] = std::min(gmin[g], idx[k]);
+                    gmax[g] = std::max(gmax[g], idx[k]);
+                }
+        });
+    parallel_for((size_t)parts, [&](size_t t) {
+        const int lo = cut[t], hi = cut[t + 1];
+        if (lo >= hi) return;
+        std::vector<int> fill(tptr.begin() + lo, tptr.begin() + hi);
+        for (int g = 0; g < ngroup; ++g) {
+            if (parts > 1 && (gmax[g] < lo || gmin[g] >= hi)) continue;
+            for (int r = g * kGroup; r < std::min(rows, g * kGroup + kGroup); ++r)
+                for (int k = ptr[r]; k < ptr[r + 1]; ++k) {
+                    const int c = idx[k];
+                    if (c < lo || c >= hi) continue;
+                    const int d = fill[c - lo]++;
+                    tidx[d] = r;
+                    if (val) tval[d] = val[k];
+                }
         }
+    });
 }
 
 // Kahn breadth-first level sets in the discovery order of findlevel.h:7-83:
@@ -135,6 +178,54 @@ void select_kernel(ExecBlock &b, const rbs_options &opt, const std::vector<int> 
     if (t_level < best) { best = t_level; b.kernel = RBS_K_LEVEL; }
     if (t_seq < best) { best = t_seq; b.kernel = RBS_K_SEQ; }
     if (t_scan < best) { best = t_scan; b.kernel = RBS_K_BANDSCAN; }
+}
+
+// The processing-order CSR (full_rp/col/val) from a row view of the matrix:
+// row r holds entries rp[r]..rp[r+1] (columns rc, values rv), the entries of
+// one column in the order the CSC holds them.  Processing row p is row
+// perm[p] with its columns renumbered to processing positions and stably
+// sorted -- the arrays of the column walk in processing order (a stable sort
+// by processing column, then by row), built row by row on host threads.
+void full_csr_from_rows(Plan &P, const int *rp, const int *rc, const double *rv, const std::vector<int> &pos_of) {
+    const int n = P.n;
+    P.full_rp.assign((size_t)n + 1, 0);
+    for (int p = 0; p < n; ++p) {
+        const int r = P.perm[p];
+        P.full_rp[(size_t)p + 1] = P.full_rp[p] + (rp[r + 1] - rp[r]);
+    }
+    P.full_col.resize((size_t)P.full_rp[n]);
+    P.full_val.resize((size_t)P.full_rp[n]);
+    constexpr int kRows = 1 << 14;
+    parallel_for(((size_t)n + kRows - 1) / kRows, [&](size_t chunk) {
+        std::vector<std::pair<int, int>> key;  // (processing column, entry) of a long row
+        const int p0 = (int)chunk * kRows, p1 = std::min(n, p0 + kRows);
+        for (int p = p0; p < p1; ++p) {
+            const int r = P.perm[p], b = rp[r], len = rp[r + 1] - b;
+            int *oc = P.full_col.data() + P.full_rp[p];
+            double *ov = P.full_val.data() + P.full_rp[p];
+            if (len <= 64) {
+                for (int j = 0; j < len; ++j) {  // insertion: equal columns keep their order
+                    const int q = pos_of[rc[b + j]];
+                    const double v = rv[b + j];
+                    int i = j;
+                    for (; i > 0 && oc[i - 1] > q; --i) {
+                        oc[i] = oc[i - 1];
+                        ov[i] = ov[i - 1];
+                    }
+                    oc[i] = q;
+                    ov[i] = v;
+                }
+            } else {
+                key.resize((size_t)len);
+                for (int j = 0; j < len; ++j) key[j] = {pos_of[rc[b + j]], j};
+                std::sort(key.begin(), key.end());  // by column, then entry: stable
+                for (int j = 0; j < len; ++j) {
+                    oc[j] = key[j].first;
+                    ov[j] = rv[b + key[j].second];
+                }
+            }
+        }
+    });
 }
 
 }  // namespace
@@ -529,8 +620,14 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
         transpose(n, n, ptr, idx, val, P.in_cp, P.in_ri, P.in_va);
     } else {
         P.in_cp.assign(ptr, ptr + n + 1);
-        P.in_ri.assign(idx, idx + nnz);
-        P.in_va.assign(val, val + nnz);
+        P.in_ri.resize((size_t)nnz);
+        P.in_va.resize((size_t)nnz);
+        constexpr int kCopy = 1 << 22;  // entries per host-thread copy
+        parallel_for(((size_t)nnz + kCopy - 1) / kCopy, [&](size_t i) {
+            const size_t k0 = i * kCopy, len = std::min<size_t>(kCopy, (size_t)nnz - k0);
+            std::memcpy(P.in_ri.data() + k0, idx + k0, len * sizeof(int));
+            std::memcpy(P.in_va.data() + k0, val + k0, len * sizeof(double));
+        });
     }
     const int *cp = P.in_cp.data(), *ri = P.in_ri.data();
     const double *va = P.in_va.data();
@@ -582,25 +679,17 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
         pos_of[orig] = i;
     }
 
-    // 4. processing-order CSR with columns ascending: rows counted, then the
-    //    columns walked in processing order (column perm[q] is processing
-    //    column q), each appending its entries to their rows -- the result
-    //    of a stable sort by column and then by row, in one pass
-    {
-        P.full_rp.assign((size_t)n + 1, 0);
-        for (int k = 0; k < nnz; ++k) P.full_rp[(size_t)pos_of[ri[k]] + 1]++;
-        for (int p = 0; p < n; ++p) P.full_rp[(size_t)p + 1] += P.full_rp[p];
-        std::vector<int> fill(P.full_rp.begin(), P.full_rp.end() - 1);
-        P.full_col.resize((size_t)nnz);
-        P.full_val.resize((size_t)nnz);
-        for (int q = 0; q < n; ++q) {
-            const int c = P.perm[q];
-            for (int k = cp[c]; k < cp[c + 1]; ++k) {
-                const int d = fill[pos_of[ri[k]]]++;
-                P.full_col[d] = q;
-                P.full_val[d] = va[k];
-            }
-        }
+    // 4. processing-order CSR with columns ascending (the result of a stable
+    //    sort by processing column and then by row), row by row from the
+    //    input rows (CSR input) or from the CSC's stable transpose
+    if (fmt == RBS_FMT_CSR) {
+        full_csr_from_rows(P, ptr, idx, val, pos_of);
+    } else {
+        std::vector<int> rp;
+        bulk_vector<int> rc;
+        bulk_vector<double> rv;
+        transpose(n, n, cp, ri, va, rp, rc, rv);
+        full_csr_from_rows(P, rp.data(), rc.data(), rv.data(), pos_of);
     }
     P.analyse_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return analyse_after_levels(P, n, nnz, substitution, lv, opt, err, seg_rows);
@@ -673,33 +762,60 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
     // per-row entry counts of every block, local levels, bandwidth
     std::vector<std::vector<int>> rowcnt((size_t)P.sum_block);
     for (int b = 0; b < P.sum_block; ++b) rowcnt[b].assign((size_t)P.blocks[b].m, 0);
-    std::vector<int> level((size_t)n, 0);
+    std::vector<int> level((size_t)n, 0), reach((size_t)n);
     P.inv_diag.resize((size_t)n);
-    for (int p = 0; p < n; ++p) {
-        int i = tri_of(p);
-        int tb = 2 * i;
-        ExecBlock &TB = P.blocks[tb];
-        int lvmax = -1, minq = p;
-        for (int k = frp[p]; k < frp[p + 1]; ++k) {
-            int q = fcol[k];
-            if (q == p) {
-                P.inv_diag[p] = 1.0 / fval[k];
-                continue;
+    // counts, inverse diagonals and the reach p - (first column) of every row
+    // on host threads (row p owns row p of every block it meets) ...
+    constexpr int kRows = 1 << 14;
+    parallel_for(((size_t)n + kRows - 1) / kRows, [&](size_t chunk) {
+        for (int p = (int)chunk * kRows; p < std::min(n, (int)chunk * kRows + kRows); ++p) {
+            int i = tri_of(p);
+            int tb = 2 * i;
+            const ExecBlock &TB = P.blocks[tb];
+            int minq = p;
+            for (int k = frp[p]; k < frp[p + 1]; ++k) {
+                int q = fcol[k];
+                if (q == p) {
+                    P.inv_diag[p] = 1.0 / fval[k];
+                    continue;
+                }
+                if (q >= TB.r0) {
+                    rowcnt[tb][p - TB.r0]++;
+                    minq = std::min(minq, q);
+                } else {
+                    int j = tri_of(q);
+                    int h = 31 - __builtin_clz((unsigned)(i ^ j));
+                    int t = i & ~((1 << h) - 1);
+                    int sb = 2 * t - 1;
+                    rowcnt[sb][p - P.blocks[sb].r0]++;
+                }
             }
-            if (q >= TB.r0) {
-                rowcnt[tb][p - TB.r0]++;
-                lvmax = std::max(lvmax, level[q]);
-                minq = std::min(minq, q);
-            } else {
-                int j = tri_of(q);
-                int h = 31 - __builtin_clz((unsigned)(i ^ j));
-                int t = i & ~((1 << h) - 1);
-                int sb = 2 * t - 1;
-                rowcnt[sb][p - P.blocks[sb].r0]++;
-            }
+            reach[p] = p - minq;
         }
-        level[p] = lvmax + 1;
-        TB.bandwidth = std::max(TB.bandwidth, p - minq);
+    });
+    // ... then the local levels: a recurrence in row order within each
+    // triangle (triangles on host threads).  The local levels of a single
+    // triangle are the level sets themselves (a row's level is one more than
+    // the highest level among its dependencies in both).
+    if (T == 1) {
+        for (size_t L = 0; L + 1 < P.bfs_ptr.size(); ++L)
+            std::fill(level.begin() + P.bfs_ptr[L], level.begin() + P.bfs_ptr[L + 1], (int)L);
+    } else {
+        parallel_for((size_t)T, [&](size_t i) {
+            const ExecBlock &TB = P.blocks[2 * i];
+            for (int p = TB.r0; p < TB.r0 + TB.m; ++p) {
+                int lvmax = -1;
+                for (int k = frp[p]; k < frp[p + 1]; ++k) {
+                    const int q = fcol[k];
+                    if (q != p && q >= TB.r0) lvmax = std::max(lvmax, level[q]);
+                }
+                level[p] = lvmax + 1;
+            }
+        });
+    }
+    for (int p = 0; p < n; ++p) {
+        ExecBlock &TB = P.blocks[2 * tri_of(p)];
+        TB.bandwidth = std::max(TB.bandwidth, reach[p]);
     }
     // block statistics and the reference's method codes
     std::vector<std::vector<int>> lvl_sizes((size_t)P.sum_block);
@@ -843,29 +959,33 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
     {
         std::vector<std::vector<int>> cur((size_t)P.sum_block);
         for (int b = 0; b < P.sum_block; ++b) cur[b].assign(rowstart[b].begin(), rowstart[b].end() - 1);
-        for (int p = 0; p < n; ++p) {
-            int i = tri_of(p);
-            int tb = 2 * i;
-            const ExecBlock &TB = P.blocks[tb];
-            for (int k = frp[p]; k < frp[p + 1]; ++k) {
-                int q = fcol[k];
-                if (q == p) continue;
-                int b, lc;
-                if (q >= TB.r0) {
-                    b = tb;
-                    lc = q - TB.r0;
-                } else {
-                    int j = tri_of(q);
-                    int h = 31 - __builtin_clz((unsigned)(i ^ j));
-                    int t = i & ~((1 << h) - 1);
-                    b = 2 * t - 1;
-                    lc = q - P.blocks[b].c0;
+        // row p owns row p of every block it meets: rows filled on host threads
+        constexpr int kRows = 1 << 14;
+        parallel_for(((size_t)n + kRows - 1) / kRows, [&](size_t chunk) {
+            for (int p = (int)chunk * kRows; p < std::min(n, (int)chunk * kRows + kRows); ++p) {
+                int i = tri_of(p);
+                int tb = 2 * i;
+                const ExecBlock &TB = P.blocks[tb];
+                for (int k = frp[p]; k < frp[p + 1]; ++k) {
+                    int q = fcol[k];
+                    if (q == p) continue;
+                    int b, lc;
+                    if (q >= TB.r0) {
+                        b = tb;
+                        lc = q - TB.r0;
+                    } else {
+                        int j = tri_of(q);
+                        int h = 31 - __builtin_clz((unsigned)(i ^ j));
+                        int t = i & ~((1 << h) - 1);
+                        b = 2 * t - 1;
+                        lc = q - P.blocks[b].c0;
+                    }
+                    int d = cur[b][p - P.blocks[b].r0]++;
+                    P.col_pool[d] = lc;
+                    P.val_pool[d] = fval[k];
                 }
-                int d = cur[b][p - P.blocks[b].r0]++;
-                P.col_pool[d] = lc;
-                P.val_pool[d] = fval[k];
             }
-        }
+        });
     }
     // 7. band layout of band-scan triangles: row r of the block is row
     //    i = r % C of chunk j = r / C; its coefficient of x_{r-1-d} sits at

@@ -26,8 +26,8 @@ struct Writer {
     void pod(const T &v) {
         ok = ok && std::fwrite(&v, sizeof(T), 1, f) == 1;
     }
-    template <typename T>
-    void vec(const std::vector<T> &v) {
+    template <typename T, typename A>
+    void vec(const std::vector<T, A> &v) {
         const uint64_t n = v.size();
         pod(n);
         if (n) ok = ok && std::fwrite(v.data(), sizeof(T), n, f) == n;
@@ -41,8 +41,8 @@ struct Reader {
     void pod(T &v) {
         ok = ok && std::fread(&v, sizeof(T), 1, f) == 1;
     }
-    template <typename T>
-    void vec(std::vector<T> &v) {
+    template <typename T, typename A>
+    void vec(std::vector<T, A> &v) {
         uint64_t n = 0;
         pod(n);
         if (!ok || n > (1ull << 40) / sizeof(T)) {

@@ -20,13 +20,50 @@
 #pragma once
 
 #include <cuda_runtime_api.h>
+#include <sys/mman.h>
+
 #include <cstdint>
+#include <cstdlib>
+#include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "rbs.h"
 
 namespace rbs {
+
+// Allocator of the plan's arrays of matrix entries (input, processing-order
+// and pool layouts).  resize() leaves new elements uninitialised: each of
+// these arrays is written in full by the pass that sizes it, on host
+// threads, so its pages are first touched in parallel instead of zeroed by
+// one thread.  Blocks of 32 MB or more are 2 MB aligned and advised for
+// transparent huge pages.
+template <typename T> struct BulkAlloc {
+    using value_type = T;
+    BulkAlloc() noexcept = default;
+    template <typename U> BulkAlloc(const BulkAlloc<U> &) noexcept {}
+    T *allocate(size_t n) {
+        constexpr size_t kHuge = size_t(2) << 20;
+        const size_t bytes = n * sizeof(T);
+        void *p;
+        if (bytes >= 16 * kHuge) {
+            const size_t rounded = (bytes + kHuge - 1) & ~(kHuge - 1);
+            p = std::aligned_alloc(kHuge, rounded);
+            if (p) madvise(p, rounded, MADV_HUGEPAGE);
+        } else {
+            p = std::malloc(bytes ? bytes : 1);
+        }
+        if (!p) throw std::bad_alloc();
+        return static_cast<T *>(p);
+    }
+    void deallocate(T *p, size_t) noexcept { std::free(p); }
+    template <typename U> void construct(U *p) noexcept { ::new ((void *)p) U; }
+    template <typename U, typename... A> void construct(U *p, A &&...a) { ::new ((void *)p) U(std::forward<A>(a)...); }
+};
+template <typename T, typename U> bool operator==(const BulkAlloc<T> &, const BulkAlloc<U> &) { return true; }
+template <typename T, typename U> bool operator!=(const BulkAlloc<T> &, const BulkAlloc<U> &) { return false; }
+template <typename T> using bulk_vector = std::vector<T, BulkAlloc<T>>;
 
 // Per-block execution record (processing order).  Offsets index the pools
 // of the plan.
@@ -93,8 +130,9 @@ struct Plan {
     int device_bfs = 0;            // 1: the level search itself ran on the device
 
     // inputs kept for the reference-format export (CSC, caller's entry order)
-    std::vector<int> in_cp, in_ri;
-    std::vector<double> in_va;
+    std::vector<int> in_cp;
+    bulk_vector<int> in_ri;
+    bulk_vector<double> in_va;
     std::vector<int> bfs_item;   // BFS level order (findlevel.h:7-83)
     std::vector<int> bfs_ptr;    // level pointers (nlevel+1)
     std::vector<int> label;      // original row -> reference label
@@ -103,8 +141,9 @@ struct Plan {
     std::vector<int> perm;       // processing position -> original row
     std::vector<ExecBlock> blocks;
     // pools (uploaded to the device)
-    std::vector<int> rp_pool, col_pool, lvl_pool, map_pool, rows_pool;
-    std::vector<double> val_pool;
+    std::vector<int> rp_pool, lvl_pool, map_pool, rows_pool;
+    bulk_vector<int> col_pool;
+    bulk_vector<double> val_pool;
     std::vector<double> inv_diag;
     std::vector<double> band_coef, band_inv;  // chunk-interleaved band layout of band-scan triangles
     std::vector<int> ell_col;                  // ELL columns of single-CTA triangles (-1 = padding)
@@ -124,8 +163,9 @@ struct Plan {
     // by the device analysis (rbs_analyse_device); empty after a host analysis
     std::vector<int> dev_reorder_cp, dev_reorder_ri;
     // full processing-order CSR (with diagonal) for FP64 residuals
-    std::vector<int> full_rp, full_col;
-    std::vector<double> full_val;
+    std::vector<int> full_rp;
+    bulk_vector<int> full_col;
+    bulk_vector<double> full_val;
 
     DeviceState *dev = nullptr;
 };

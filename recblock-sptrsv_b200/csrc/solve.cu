@@ -100,8 +100,8 @@ namespace {
         }                                                                            \
     } while (0)
 
-template <typename T>
-int upload(DeviceState &D, T *&dst, const std::vector<T> &src, std::string &err) {
+template <typename T, typename A>
+int upload(DeviceState &D, T *&dst, const std::vector<T, A> &src, std::string &err) {
     // 256 bytes of padding: staged bulk copies round their end up to 16 bytes
     size_t bytes = std::max<size_t>(src.size(), 1) * sizeof(T) + 256;
     cudaError_t e = cudaMalloc(&dst, bytes);
