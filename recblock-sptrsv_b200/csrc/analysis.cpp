@@ -267,11 +267,56 @@ static bool wants_band(const ExecBlock &b, const rbs_options &opt) {
 // One triangle's level-chunk layout into `out`, record and table offsets
 // relative to `out` (build_lc merges the blocks in order and rebases them).
 struct LcOut {
-    std::vector<uint32_t> rec64, rec32;
+    bulk_vector<uint32_t> rec64, rec32;
     std::vector<int> tab, segs;
 };
+// Appends parts to dst in order: record starts in the tables (16-byte
+// units) and the first chunk of every segment triple rebased; the copies run
+// on host threads and the parts are emptied.  first_seg[i] receives the
+// index of part i's first segment triple in dst.
+static void lc_append(LcOut &dst, const std::vector<LcOut *> &parts, std::vector<long long> *first_seg = nullptr) {
+    const size_t np = parts.size();
+    if (np == 1 && dst.rec64.empty() && dst.rec32.empty() && dst.tab.empty() && dst.segs.empty()) {
+        std::swap(dst, *parts[0]);  // nothing to rebase
+        if (first_seg) first_seg->assign(1, 0);
+        return;
+    }
+    std::vector<size_t> o64(np), o32(np), otab(np), oseg(np);
+    size_t n64 = dst.rec64.size(), n32 = dst.rec32.size(), ntab = dst.tab.size(), nseg = dst.segs.size();
+    for (size_t i = 0; i < np; ++i) {
+        o64[i] = n64;
+        o32[i] = n32;
+        otab[i] = ntab;
+        oseg[i] = nseg;
+        n64 += parts[i]->rec64.size();
+        n32 += parts[i]->rec32.size();
+        ntab += parts[i]->tab.size();
+        nseg += parts[i]->segs.size();
+    }
+    dst.rec64.resize(n64);
+    dst.rec32.resize(n32);
+    dst.tab.resize(ntab);
+    dst.segs.resize(nseg);
+    if (first_seg) {
+        first_seg->resize(np);
+        for (size_t i = 0; i < np; ++i) (*first_seg)[i] = (long long)(oseg[i] / 3);
+    }
+    parallel_for(np, [&](size_t i) {
+        LcOut &p = *parts[i];
+        if (!p.rec64.empty()) std::memcpy(dst.rec64.data() + o64[i], p.rec64.data(), p.rec64.size() * 4);
+        if (!p.rec32.empty()) std::memcpy(dst.rec32.data() + o32[i], p.rec32.data(), p.rec32.size() * 4);
+        const int r64_base = (int)(o64[i] / 4), r32_base = (int)(o32[i] / 4), tab_base = (int)(otab[i] / LC_TAB_INTS);
+        for (size_t j = 0; j < p.tab.size(); ++j) {
+            const size_t f = j % LC_TAB_INTS;
+            dst.tab[otab[i] + j] = p.tab[j] + (f == 0 ? r64_base : f == 2 ? r32_base : 0);
+        }
+        for (size_t j = 0; j < p.segs.size(); ++j) dst.segs[oseg[i] + j] = p.segs[j] + (j % 3 == 0 ? tab_base : 0);
+        LcOut().rec64.swap(p.rec64);
+        LcOut().rec32.swap(p.rec32);
+    });
+}
 static void build_lc_block(const Plan &P, ExecBlock &B, const rbs_options &opt, const std::vector<int> &level,
-                           LcOut &out) {
+                           LcOut &out, bool seg_threads) {
     B.lc_ok = 0;
     B.lc_nseg = 0;
     B.lc_seg_off = -1;
@@ -313,24 +358,32 @@ static void build_lc_block(const Plan &P, ExecBlock &B, const rbs_options &opt, 
             seq[(size_t)fill[(size_t)seg[(size_t)r]]++] = r;
         }
     }
-    // chunks; seq is reordered inside every chunk and vpos assigned
+    // Segments are independent systems (no entry of one refers to a row of
+    // another): chunks, ring placement and records are built per segment,
+    // on host threads when seg_threads is set, and the records merged in
+    // the segment order below.
     struct Ch { int v0, nr, no, nrec, ncols, maxlen; };
     std::vector<std::vector<Ch>> chunks((size_t)nseg);
-    std::vector<int> vpos((size_t)m, -1), rl((size_t)LC_RMAX);
-    auto counts = [&](const int *rows, int nr, int thr, int &no, int &nrec, int &ncols) {
-        no = nrec = ncols = 0;
-        for (int t = 0; t < nr; ++t) {
-            const int r = rows[t];
-            int rr = 0;
-            for (int k = rp[r]; k < rp[r + 1]; ++k) rr += vpos[(size_t)cl[k]] >= thr;
-            rl[(size_t)t] = rr;
-            nrec += rr;
-            no += rp[r + 1] - rp[r] - rr;
-            ncols = std::max(ncols, rr);
-        }
-    };
-    bool ok = true;
-    for (int q = 0; q < nseg && ok; ++q) {
+    std::vector<std::vector<int>> roff((size_t)nseg), iss((size_t)nseg);
+    std::vector<char> seg_ok((size_t)nseg, 1);
+    std::vector<int> vpos((size_t)m, -1);
+    // chunks of segment q (its rows in seq reordered inside every chunk and
+    // their vpos assigned), then their ring offsets and issue iterations
+    auto layout = [&](size_t qz) {
+        const int q = (int)qz;
+        std::vector<int> rl((size_t)LC_RMAX);
+        auto counts = [&](const int *rows, int nr, int thr, int &no, int &nrec, int &ncols) {
+            no = nrec = ncols = 0;
+            for (int t = 0; t < nr; ++t) {
+                const int r = rows[t];
+                int rr = 0;
+                for (int k = rp[r]; k < rp[r + 1]; ++k) rr += vpos[(size_t)cl[k]] >= thr;
+                rl[(size_t)t] = rr;
+                nrec += rr;
+                no += rp[r + 1] - rp[r] - rr;
+                ncols = std::max(ncols, rr);
+            }
+        };
         int *sq = seq.data() + scount[(size_t)q];
         const int len = scount[(size_t)q + 1] - scount[(size_t)q];
         auto &ch = chunks[(size_t)q];
@@ -350,8 +403,8 @@ static void build_lc_block(const Plan &P, ExecBlock &B, const rbs_options &opt, 
                 ncols = std::max(ncols, rr);
             }
             if (nr == 0) {  // one row alone does not fit the ring
-                ok = false;
-                break;
+                seg_ok[(size_t)q] = 0;
+                return;
             }
             // exact split with this chunk's own threshold
             for (;;) {
@@ -360,8 +413,8 @@ static void build_lc_block(const Plan &P, ExecBlock &B, const rbs_options &opt, 
                 --nr;
             }
             if (lc_foot_bytes(nr, no, nrec, ncols, 8) > LC_FMAX) {
-                ok = false;
-                break;
+                seg_ok[(size_t)q] = 0;
+                return;
             }
             // rows by recent count, largest first (stable)
             std::vector<int> idx((size_t)nr);
@@ -378,12 +431,7 @@ static void build_lc_block(const Plan &P, ExecBlock &B, const rbs_options &opt, 
             ch.push_back({i, nr, no, nrec, ncols, maxlen});
             i += nr;
         }
-    }
-    if (!ok) return;
-    // ring placement and issue iterations
-    std::vector<std::vector<int>> roff((size_t)nseg), iss((size_t)nseg);
-    for (int q = 0; q < nseg && ok; ++q) {
-        const auto &ch = chunks[(size_t)q];
+        // ring placement and issue iterations
         const int nch = (int)ch.size();
         auto &ro = roff[(size_t)q];
         auto &is = iss[(size_t)q];
@@ -414,30 +462,26 @@ static void build_lc_block(const Plan &P, ExecBlock &B, const rbs_options &opt, 
                 }
                 scanned += fb[(size_t)k];
             }
-            if (at > std::max(0, j - LC_D)) ok = false;
+            if (at > std::max(0, j - LC_D)) {
+                seg_ok[(size_t)q] = 0;
+                return;
+            }
             is[(size_t)j] = at;
         }
-    }
-    if (!ok) return;
-    // records
-    B.lc_ok = 1;
-    B.lc_nseg = nseg;
-    B.lc_seg_off = 0;  // set when the blocks are merged
-    std::vector<int> order((size_t)nseg);
-    for (int q = 0; q < nseg; ++q) order[(size_t)q] = q;
-    auto work = [&](int q) {
-        long long e = 0;
-        for (const Ch &c : chunks[(size_t)q]) e += c.no + c.nrec;
-        return (long long)chunks[(size_t)q].size() * 4096 + e;
     };
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
-    std::vector<int> dest, rlen, rpo, cs, colr, colo;
-    std::vector<double> inv, valr, valo;
-    for (int q : order) {
+    if (seg_threads) parallel_for((size_t)nseg, layout);
+    else
+        for (int q = 0; q < nseg; ++q) layout((size_t)q);
+    for (int q = 0; q < nseg; ++q)
+        if (!seg_ok[(size_t)q]) return;
+    // records of segment q into so, offsets relative to so
+    auto records = [&](int q, LcOut &so) {
         const int *sq = seq.data() + scount[(size_t)q];
         const auto &ch = chunks[(size_t)q];
         const int nch = (int)ch.size();
-        out.segs.insert(out.segs.end(), {(int)(out.tab.size() / LC_TAB_INTS), nch, nch ? roff[(size_t)q][0] : 0});
+        so.segs.insert(so.segs.end(), {(int)(so.tab.size() / LC_TAB_INTS), nch, nch ? roff[(size_t)q][0] : 0});
+        std::vector<int> dest, rlen, rpo, cs, colr, colo;
+        std::vector<double> inv, valr, valo;
         for (int j = 0; j < nch; ++j) {
             const Ch &c = ch[(size_t)j];
             const int thr = c.v0 + c.nr - LC_XW;
@@ -487,7 +531,7 @@ static void build_lc_block(const Plan &P, ExecBlock &B, const rbs_options &opt, 
                 dmax = std::max(dmax, dest[(size_t)t]);
             }
             const int blo = dmax - dmin + 1 == c.nr ? dmin : -1;
-            auto emit = [&](std::vector<uint32_t> &pool, int es) -> std::pair<int, int> {
+            auto emit = [&](bulk_vector<uint32_t> &pool, int es) -> std::pair<int, int> {
                 const size_t base = pool.size();
                 const long long bytes = lc_static_bytes(c.nr, c.no, c.nrec, c.ncols, es);
                 pool.resize(base + (size_t)(bytes / 4), 0u);
@@ -521,14 +565,35 @@ static void build_lc_block(const Plan &P, ExecBlock &B, const rbs_options &opt, 
                 put_v(valo);
                 return {(int)(base / 4), (int)(bytes / 16)};
             };
-            const auto r64 = emit(out.rec64, 8);
-            const auto r32 = emit(out.rec32, 4);
+            const auto r64 = emit(so.rec64, 8);
+            const auto r32 = emit(so.rec32, 4);
             const int bs64 = (int)((lc_static_bytes(c.nr, c.no, c.nrec, c.ncols, 8) + lc_padv(c.no, 8)) / 16);
             const int bs32 = (int)((lc_static_bytes(c.nr, c.no, c.nrec, c.ncols, 4) + lc_padv(c.no, 4)) / 16);
-            out.tab.insert(out.tab.end(), {r64.first, r64.second, r32.first, r32.second, roff[(size_t)q][(size_t)j],
-                                             iss[(size_t)q][(size_t)j], blo, blo >= 0 ? c.nr : 0, bs64, bs32});
+            so.tab.insert(so.tab.end(), {r64.first, r64.second, r32.first, r32.second, roff[(size_t)q][(size_t)j],
+                                         iss[(size_t)q][(size_t)j], blo, blo >= 0 ? c.nr : 0, bs64, bs32});
         }
+    };
+    // segments in order of decreasing work (the persistent kernel's queue)
+    B.lc_ok = 1;
+    B.lc_nseg = nseg;
+    B.lc_seg_off = 0;  // set when the blocks are merged
+    std::vector<int> order((size_t)nseg);
+    for (int q = 0; q < nseg; ++q) order[(size_t)q] = q;
+    auto work = [&](int q) {
+        long long e = 0;
+        for (const Ch &c : chunks[(size_t)q]) e += c.no + c.nrec;
+        return (long long)chunks[(size_t)q].size() * 4096 + e;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+    if (!seg_threads) {
+        for (int q : order) records(q, out);
+        return;
     }
+    std::vector<LcOut> so((size_t)nseg);
+    parallel_for((size_t)nseg, [&](size_t q) { records((int)q, so[q]); });
+    std::vector<LcOut *> parts;
+    for (int q : order) parts.push_back(&so[(size_t)q]);
+    lc_append(out, parts);
 }
 
 static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &level) {
@@ -536,36 +601,30 @@ static void build_lc(Plan &P, const rbs_options &opt, const std::vector<int> &le
     P.lc_rec32.clear();
     P.lc_tab.clear();
     P.lc_segs.clear();
-    // blocks are independent: built on host threads, merged in block order
+    // blocks are independent: built on host threads (or, in a batch, one
+    // after another with their systems on host threads), merged in block
+    // order
     const size_t nb = P.blocks.size();
     std::vector<LcOut> outs(nb);
-    std::atomic<size_t> next{0};
-    auto work = [&] {
-        for (size_t b; (b = next.fetch_add(1)) < nb;) build_lc_block(P, P.blocks[b], opt, level, outs[b]);
-    };
-    const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    std::vector<std::thread> th;
-    for (unsigned t = 1; t < nth; ++t) th.emplace_back(work);
-    work();
-    for (auto &t : th) t.join();
-    for (size_t b = 0; b < nb; ++b) {
-        ExecBlock &B = P.blocks[b];
-        if (!B.lc_ok) continue;
-        LcOut &o = outs[b];
-        const int tab_base = (int)(P.lc_tab.size() / LC_TAB_INTS);
-        const int r64_base = (int)(P.lc_rec64.size() / 4), r32_base = (int)(P.lc_rec32.size() / 4);
-        B.lc_seg_off = (long long)P.lc_segs.size() / 3;
-        for (size_t i = 0; i < o.segs.size(); i += 3) P.lc_segs.insert(P.lc_segs.end(), {o.segs[i] + tab_base, o.segs[i + 1], o.segs[i + 2]});
-        for (size_t i = 0; i < o.tab.size(); i += LC_TAB_INTS) {
-            o.tab[i] += r64_base;  // record starts, in 16-byte units
-            o.tab[i + 2] += r32_base;
+    if (P.seg_rows.empty())
+        parallel_for(nb, [&](size_t b) { build_lc_block(P, P.blocks[b], opt, level, outs[b], false); });
+    else
+        for (size_t b = 0; b < nb; ++b) build_lc_block(P, P.blocks[b], opt, level, outs[b], true);
+    std::vector<LcOut *> parts;
+    std::vector<size_t> which;
+    for (size_t b = 0; b < nb; ++b)
+        if (P.blocks[b].lc_ok) {
+            parts.push_back(&outs[b]);
+            which.push_back(b);
         }
-        P.lc_tab.insert(P.lc_tab.end(), o.tab.begin(), o.tab.end());
-        P.lc_rec64.insert(P.lc_rec64.end(), o.rec64.begin(), o.rec64.end());
-        P.lc_rec32.insert(P.lc_rec32.end(), o.rec32.begin(), o.rec32.end());
-        LcOut().rec64.swap(o.rec64);
-        LcOut().rec32.swap(o.rec32);
-    }
+    LcOut all;
+    std::vector<long long> first;
+    lc_append(all, parts, &first);
+    for (size_t i = 0; i < which.size(); ++i) P.blocks[which[i]].lc_seg_off = first[i];
+    P.lc_rec64.swap(all.rec64);
+    P.lc_rec32.swap(all.rec32);
+    P.lc_tab.swap(all.tab);
+    P.lc_segs.swap(all.segs);
 }
 
 int host_bfs_levels(const int *cp, const int *ri, int m, std::vector<int> &levelPtr, std::vector<int> &item) {
@@ -1087,6 +1146,10 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
     P.ell_val.clear();
     P.ell_chunks.clear();
     constexpr int RMAX = 512, EMAX = 2048;
+    // chunk bounds and pool offsets first (chunk starts 16-byte aligned),
+    // then the pool filled chunk by chunk on host threads
+    std::vector<int> ell_blocks;
+    long long ell_size = 0;
     for (ExecBlock &B : P.blocks) {
         if (!wants_level(B, opt)) continue;
         // only the kernel choice's fallback outside tuning: a triangle with a
@@ -1117,30 +1180,45 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
         B.ell_ok = 1;
         B.ell_nchunks = nch;
         B.ell_chunk_off = (long long)P.ell_chunks.size() / 4;
-        B.ell_lo = (long long)P.ell_col.size();
+        B.ell_lo = ell_size;
         for (int q = 0; q < nch; ++q) {
-            while (P.ell_col.size() % 4) {  // 16-byte aligned chunk starts
-                P.ell_col.push_back(-1);
-                P.ell_val.push_back(0.0);
-            }
-            const int R0 = cuts[q], R1 = cuts[q + 1], W = widths[q], R = R1 - R0;
-            const long long off = (long long)P.ell_col.size();
-            P.ell_chunks.insert(P.ell_chunks.end(), {R0, R1, W, (int)off});
-            P.ell_col.resize(P.ell_col.size() + (size_t)R * W, -1);
-            P.ell_val.resize(P.ell_val.size() + (size_t)R * W, 0.0);
-            for (int i = 0; i < R; ++i) {
-                const int r = R0 + i;
-                for (int j = 0; j < rp[r + 1] - rp[r]; ++j) {
-                    P.ell_col[(size_t)(off + (long long)j * R + i)] = P.col_pool[rp[r] + j];
-                    P.ell_val[(size_t)(off + (long long)j * R + i)] = P.val_pool[rp[r] + j];
-                }
-            }
+            ell_size = (ell_size + 3) & ~3LL;
+            const int R0 = cuts[q], R1 = cuts[q + 1], W = widths[q];
+            P.ell_chunks.insert(P.ell_chunks.end(), {R0, R1, W, (int)ell_size});
+            ell_size += (long long)(R1 - R0) * W;
         }
-        B.ell_hi = (long long)P.ell_col.size();
+        B.ell_hi = ell_size;
+        ell_blocks.push_back(B.index);
     }
-    if (P.ell_col.size() > (size_t)0x7fffffff) {
+    if (ell_size > 0x7fffffffLL) {
         err = "rbs_analyse: ELL pool too large";
         return RBS_ERR_NOMEM;
+    }
+    P.ell_col.resize((size_t)ell_size);
+    P.ell_val.resize((size_t)ell_size);
+    {
+        // chunk i of the pool fills its slots and the alignment gap before it
+        std::vector<std::pair<int, int>> where;  // (block, chunk) of every pool chunk in order
+        for (int b : ell_blocks)
+            for (int q = 0; q < P.blocks[(size_t)b].ell_nchunks; ++q) where.push_back({b, q});
+        parallel_for(where.size(), [&](size_t i) {
+            const ExecBlock &B = P.blocks[(size_t)where[i].first];
+            const int *ch = P.ell_chunks.data() + 4 * (B.ell_chunk_off + where[i].second);
+            const int R0 = ch[0], R = ch[1] - ch[0], W = ch[2];
+            const long long off = ch[3];
+            const long long gap0 = i == 0 ? 0 : (where[i].second == 0 ? P.blocks[(size_t)where[i - 1].first].ell_hi
+                                                                       : (long long)ch[-1] + (long long)(ch[-3] - ch[-4]) * ch[-2]);
+            std::fill(P.ell_col.begin() + gap0, P.ell_col.begin() + off + (long long)R * W, -1);
+            std::fill(P.ell_val.begin() + gap0, P.ell_val.begin() + off + (long long)R * W, 0.0);
+            const int *rp = P.rp_pool.data() + B.rp_off;
+            for (int t = 0; t < R; ++t) {
+                const int r = R0 + t;
+                for (int j = 0; j < rp[r + 1] - rp[r]; ++j) {
+                    P.ell_col[(size_t)(off + (long long)j * R + t)] = P.col_pool[rp[r] + j];
+                    P.ell_val[(size_t)(off + (long long)j * R + t)] = P.val_pool[rp[r] + j];
+                }
+            }
+        });
     }
     for (ExecBlock &B : P.blocks) {
         if (!B.tri || B.kernel != RBS_K_LEVEL) continue;
@@ -1228,11 +1306,14 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
         for (int b = 0; b < sum; ++b) iv[b] = P.blocks[b].tri ? P.blocks[b].nlv : 0;
         return RBS_OK;
     }
-    if (name == "ell_col") return put(P.ell_col);
+    if (name == "ell_col") {
+        iv.assign(P.ell_col.begin(), P.ell_col.end());
+        return RBS_OK;
+    }
     if (name == "ell_chunks") return put(P.ell_chunks);
     if (name == "ell_val") {
         is_double = true;
-        dv = P.ell_val;
+        dv.assign(P.ell_val.begin(), P.ell_val.end());
         return RBS_OK;
     }
     if (name == "ell_block") {  // per block: first chunk, chunk count (-1 if not ELL)

@@ -146,15 +146,15 @@ struct Plan {
     bulk_vector<double> val_pool;
     std::vector<double> inv_diag;
     std::vector<double> band_coef, band_inv;  // chunk-interleaved band layout of band-scan triangles
-    std::vector<int> ell_col;                  // ELL columns of single-CTA triangles (-1 = padding)
-    std::vector<double> ell_val;
+    bulk_vector<int> ell_col;                  // ELL columns of single-CTA triangles (-1 = padding)
+    bulk_vector<double> ell_val;
     std::vector<int> ell_chunks;
     std::vector<int> ca_tab, ca_col;           // level tables and level-ELL columns (-1 = padding)
     std::vector<double> ca_val;
     // level-chunk records (level_lc.cuh): 16-byte words of the FP64 and FP32
     // layouts, one LcChunk (lc_layout.h) per chunk, 3 ints per segment (first
     // chunk, chunks, ring offset of the first chunk)
-    std::vector<uint32_t> lc_rec64, lc_rec32;
+    bulk_vector<uint32_t> lc_rec64, lc_rec32;
     std::vector<int> lc_tab, lc_segs;
     // original-row offsets of independent systems (batched plans); empty
     // for a single system
