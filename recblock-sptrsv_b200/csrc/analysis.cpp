@@ -28,20 +28,6 @@ constexpr int kMedRow = 32;     // RBS_MEDROW (kernels.cuh)
 
 int lowbit(int t) { return t & -t; }
 
-// fn(i) for every i in [0, count) on up to 16 host threads (an atomic work
-// counter); fn writes only what index i owns.
-template <typename F> void parallel_for(size_t count, F &&fn) {
-    std::atomic<size_t> next{0};
-    auto work = [&] {
-        for (size_t i; (i = next.fetch_add(1)) < count;) fn(i);
-    };
-    const unsigned nth = (unsigned)std::min<size_t>(count, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
-    std::vector<std::thread> th;
-    for (unsigned t = 1; t < nth; ++t) th.emplace_back(work);
-    work();
-    for (auto &t : th) t.join();
-}
-
 // Stable CSR(rows x cols) -> CSC transposition (tranpose.h:7-54 semantics:
 // entries of a column appear in ascending row order).  Large matrices are
 // transposed on host threads, each owning a range of output columns of about
@@ -331,11 +317,17 @@ static void build_lc_block(const Plan &P, ExecBlock &B, const rbs_options &opt, 
     if (!P.seg_rows.empty()) {
         std::vector<int> id(P.seg_rows.size(), -1);
         nseg = 0;
+        constexpr int kRows = 1 << 14;
+        parallel_for(((size_t)m + kRows - 1) / kRows, [&](size_t ch) {
+            for (int r = (int)ch * kRows; r < std::min(m, (int)ch * kRows + kRows); ++r) {
+                const int o = P.perm[(size_t)B.r0 + r];
+                seg[(size_t)r] = (int)(std::upper_bound(P.seg_rows.begin(), P.seg_rows.end(), o) - P.seg_rows.begin()) - 1;
+            }
+        });
         for (int r = 0; r < m; ++r) {
-            const int o = P.perm[(size_t)B.r0 + r];
-            const int sgi = (int)(std::upper_bound(P.seg_rows.begin(), P.seg_rows.end(), o) - P.seg_rows.begin()) - 1;
-            if (id[(size_t)sgi] < 0) id[(size_t)sgi] = nseg++;
-            seg[(size_t)r] = id[(size_t)sgi];
+            int &sg = seg[(size_t)r];
+            if (id[(size_t)sg] < 0) id[(size_t)sg] = nseg++;
+            sg = id[(size_t)sg];
         }
     }
     // rows level by level (stable), then split by segment
@@ -659,16 +651,14 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
         err = "rbs_analyse: pointer array must start at 0 and end at nnz";
         return RBS_ERR_STRUCTURE;
     }
-    for (int c = 0; c < n; ++c)
-        if (ptr[c + 1] < ptr[c]) {
-            err = "rbs_analyse: pointer array decreases at " + std::to_string(c);
-            return RBS_ERR_STRUCTURE;
-        }
-    for (int k = 0; k < nnz; ++k)
-        if (idx[k] < 0 || idx[k] >= n) {
-            err = "rbs_analyse: index out of range at entry " + std::to_string(k);
-            return RBS_ERR_STRUCTURE;
-        }
+    if (long long c = first_bad(n, [&](long long c) { return ptr[c + 1] < ptr[c]; }); c >= 0) {
+        err = "rbs_analyse: pointer array decreases at " + std::to_string(c);
+        return RBS_ERR_STRUCTURE;
+    }
+    if (long long k = first_bad(nnz, [&](long long k) { return idx[k] < 0 || idx[k] >= n; }); k >= 0) {
+        err = "rbs_analyse: index out of range at entry " + std::to_string(k);
+        return RBS_ERR_STRUCTURE;
+    }
     P.opt = opt;
     P.n = n;
     P.nnz = nnz;
@@ -690,7 +680,20 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
     }
     const int *cp = P.in_cp.data(), *ri = P.in_ri.data();
     const double *va = P.in_va.data();
-    for (int c = 0; c < n; ++c) {
+    // the first column that breaks a rule (found on host threads), then its
+    // message from the checks below
+    const long long bad_col = first_bad(n, [&](long long c) {
+        const int b = cp[c], e = cp[c + 1];
+        if (b == e) return true;
+        const int dpos = substitution == RBS_FORWARD ? b : e - 1;
+        if (ri[dpos] != c || va[dpos] == 0.0) return true;
+        for (int k = b; k < e; ++k) {
+            const int r = ri[k];
+            if (!(substitution == RBS_FORWARD ? r >= c : r <= c) || (k != dpos && r == c)) return true;
+        }
+        return false;
+    });
+    for (int c = bad_col < 0 ? n : (int)bad_col; c < n; ++c) {
         int b = cp[c], e = cp[c + 1];
         if (b == e) {
             err = "rbs_analyse: column " + std::to_string(c) + " has no diagonal";

@@ -158,24 +158,29 @@ int rbs_batch_analyse(int count, const int *const *ptr, const int *const *idx, c
         Z += nnz[i];
     }
     if (N > 0x7fffffffLL || Z > 0x7fffffffLL) return fail(RBS_ERR_ARG, "rbs_batch_analyse: batch exceeds 2^31 rows or entries");
-    std::vector<int> bp((size_t)N + 1), bi((size_t)Z);
-    std::vector<double> bv((size_t)Z);
-    long long r0 = 0, z0 = 0;
-    row_offsets[0] = 0;
-    for (int i = 0; i < count; ++i) {
+    for (int i = 0; i < count; ++i)
         if (ptr[i][0] != 0 || ptr[i][n[i]] != nnz[i])
             return fail(RBS_ERR_STRUCTURE, "rbs_batch_analyse: pointer array of system " + std::to_string(i) +
                                                " must run from 0 to nnz");
-        for (int c = 0; c < n[i]; ++c) bp[(size_t)(r0 + c)] = (int)(z0 + ptr[i][c]);
+    std::vector<long long> z0((size_t)count + 1, 0);
+    row_offsets[0] = 0;
+    for (int i = 0; i < count; ++i) {
+        row_offsets[i + 1] = row_offsets[i] + n[i];
+        z0[(size_t)i + 1] = z0[(size_t)i] + nnz[i];
+    }
+    // the block-diagonal matrix, system by system on host threads
+    std::vector<int> bp((size_t)N + 1);
+    rbs::bulk_vector<int> bi((size_t)Z);
+    rbs::bulk_vector<double> bv((size_t)Z);
+    rbs::parallel_for((size_t)count, [&](size_t i) {
+        const int r0 = row_offsets[i];
+        for (int c = 0; c < n[i]; ++c) bp[(size_t)(r0 + c)] = (int)(z0[i] + ptr[i][c]);
         for (int k = 0; k < nnz[i]; ++k) {
             const int v = idx[i][k];
-            bi[(size_t)(z0 + k)] = (v >= 0 && v < n[i]) ? (int)(v + r0) : -1;  // -1 is rejected by the analysis
-            bv[(size_t)(z0 + k)] = val[i][k];
+            bi[(size_t)(z0[i] + k)] = (v >= 0 && v < n[i]) ? v + r0 : -1;  // -1 is rejected by the analysis
+            bv[(size_t)(z0[i] + k)] = val[i][k];
         }
-        r0 += n[i];
-        z0 += nnz[i];
-        row_offsets[i + 1] = (int)r0;
-    }
+    });
     bp[(size_t)N] = (int)Z;
     const std::vector<int> segs(row_offsets, row_offsets + count);
     return analyse_impl(bp.data(), bi.data(), bv.data(), (int)N, (int)Z, fmt, substitution, lv < 0 ? 0 : lv, opt, plan,

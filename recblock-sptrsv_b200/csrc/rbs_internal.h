@@ -22,10 +22,13 @@
 #include <cuda_runtime_api.h>
 #include <sys/mman.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstdlib>
 #include <new>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -64,6 +67,38 @@ template <typename T> struct BulkAlloc {
 template <typename T, typename U> bool operator==(const BulkAlloc<T> &, const BulkAlloc<U> &) { return true; }
 template <typename T, typename U> bool operator!=(const BulkAlloc<T> &, const BulkAlloc<U> &) { return false; }
 template <typename T> using bulk_vector = std::vector<T, BulkAlloc<T>>;
+
+// fn(i) for every i in [0, count) on up to 16 host threads (an atomic work
+// counter); fn writes only what index i owns.
+template <typename F> void parallel_for(size_t count, F &&fn) {
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+        for (size_t i; (i = next.fetch_add(1)) < count;) fn(i);
+    };
+    const unsigned nth = (unsigned)std::min<size_t>(count, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nth; ++t) th.emplace_back(work);
+    work();
+    for (auto &t : th) t.join();
+}
+
+// Smallest i in [0, count) with bad(i), or -1 (chunks scanned on host
+// threads): the index a serial check would stop at.
+template <typename F> long long first_bad(long long count, F &&bad) {
+    constexpr long long kChunk = 1 << 18;
+    const size_t nchunk = (size_t)((count + kChunk - 1) / kChunk);
+    std::vector<long long> found(nchunk, -1);
+    parallel_for(nchunk, [&](size_t c) {
+        for (long long i = (long long)c * kChunk, e = std::min(count, i + kChunk); i < e; ++i)
+            if (bad(i)) {
+                found[c] = i;
+                return;
+            }
+    });
+    for (long long f : found)
+        if (f >= 0) return f;
+    return -1;
+}
 
 // Per-block execution record (processing order).  Offsets index the pools
 // of the plan.

@@ -111,3 +111,55 @@ def test_empty_square_block_is_handled():
     kern = plan.export("kernel")
     assert (meth[1::2] == -1).all() and (kern[1::2] == rbs.K_EMPTY).all()
     assert (kern[0::2] == rbs.K_DIAG).all()
+
+
+def _big_upper_csc(n=700000):
+    # a lower CSR read as the CSC of its transpose: an upper triangle whose
+    # columns hold the diagonal last (backward substitution)
+    rp, ci, va = rbs.gen_lower_csr(rbs.GEN_BAND_POISSON, n=n, lam=2, band=8, seed=4)
+    return rp, ci, va.copy()
+
+
+def _message(*args, **kw):
+    with pytest.raises(rbs.RbsError) as e:
+        rbs.analyse(*args, opts=rbs.options(host_only=1), **kw)
+    assert e.value.code == rbs.ERR_STRUCTURE, str(e.value)
+    return str(e.value)
+
+
+def test_large_input_reports_the_first_fault():
+    # the checks run over chunks of columns and entries on host threads; the
+    # error still names the first bad column or entry, as a serial scan does
+    cp, ri, va = _big_upper_csc()
+    for a, b in ((5, 650000), (300001, 600000), (699999, 699999)):
+        v2 = va.copy()
+        v2[cp[b + 1] - 1] = 0.0
+        v2[cp[a + 1] - 1] = 0.0
+        assert f"zero diagonal in column {a}" in _message(cp, ri, v2, substitution=rbs.BACKWARD, lv=2)
+    r2 = ri.copy()
+    k1, k2 = 123457, len(ri) - 3
+    r2[k2] = -1
+    r2[k1] = 10**7
+    assert f"index out of range at entry {k1}" in _message(cp, r2, va, substitution=rbs.BACKWARD, lv=2)
+    c2 = cp.copy()
+    c2[650001] = c2[650000] - 1
+    c2[400001] = c2[400000] - 1
+    assert "pointer array decreases at 400000" in _message(c2, ri, va, substitution=rbs.BACKWARD, lv=2)
+    # a column below the diagonal in an upper system: the wrong-triangle rule
+    r3 = ri.copy()
+    col = 500000 + int(np.argmax(np.diff(cp[500000:500100]) > 1))  # a column with an off-diagonal entry
+    r3[cp[col]] = col + 1
+    assert f"entry ({col + 1},{col}) outside the upper triangle" in _message(cp, r3, va, substitution=rbs.BACKWARD, lv=2)
+
+
+def test_batch_reports_the_first_bad_system():
+    systems = [rbs.gen_lower_csr(rbs.GEN_BAND_POISSON, n=3000, lam=3, band=20, seed=s) for s in range(6)]
+    bad = [list(s) for s in systems]
+    for i in (4, 2):
+        p = bad[i][0].copy()
+        p[-1] += 1
+        bad[i][0] = p
+    with pytest.raises(rbs.RbsError) as e:
+        rbs.batch_analyse([tuple(s) for s in bad], substitution=rbs.FORWARD, fmt=rbs.FMT_CSR,
+                          opts=rbs.options(host_only=1))
+    assert e.value.code == rbs.ERR_STRUCTURE and "system 2 " in str(e.value)
