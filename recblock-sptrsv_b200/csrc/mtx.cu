@@ -468,7 +468,7 @@ struct Source {
 // one chunk read by several host threads (page-cache copies scale with
 // threads; the device copy of the previous chunk runs meanwhile)
 bool read_parallel(const Source &src, long long off, long long n, unsigned char *dst) {
-    const int P = n >= (4LL << 20) ? (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency())) : 1;
+    const int P = n >= (4LL << 20) ? (int)std::min(8u, host_threads()) : 1;
     if (P == 1) return src.read(off, n, dst);
     std::vector<char> ok((size_t)P, 1);
     std::vector<std::thread> th;
@@ -714,7 +714,7 @@ int read_impl(const Source &src, const rbs_options &opt, DeviceMtx &M, std::stri
                     }
                 }
             };
-            const int nth = H < 65536 ? 1 : (int)std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()));
+            const int nth = H < 65536 ? 1 : (int)host_threads();
             std::vector<std::thread> th;
             for (int t = 1; t < nth; ++t) th.emplace_back(work, (int)((long long)H * t / nth), (int)((long long)H * (t + 1) / nth));
             work(0, (int)((long long)H / nth));
@@ -867,7 +867,7 @@ int mtx_read(const char *path, const void *bytes, long long len, const rbs_optio
 int mtx_write(const char *path, int m, int n, const int *rp, const int *ci, const double *val, int symmetric,
               std::string &err) {
     // rows in parallel into per-thread text, then written in row order
-    const int nth = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+    const int nth = (int)host_threads();
     std::vector<std::string> part((size_t)nth);
     long long total = 0;
     for (int i = 0; i < m; ++i)

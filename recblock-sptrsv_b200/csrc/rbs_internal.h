@@ -68,14 +68,26 @@ template <typename T, typename U> bool operator==(const BulkAlloc<T> &, const Bu
 template <typename T, typename U> bool operator!=(const BulkAlloc<T> &, const BulkAlloc<U> &) { return false; }
 template <typename T> using bulk_vector = std::vector<T, BulkAlloc<T>>;
 
-// fn(i) for every i in [0, count) on up to 16 host threads (an atomic work
-// counter); fn writes only what index i owns.
+// Host threads of the analysis: RBS_HOST_THREADS (1..64) when set, else the
+// hardware's, at most 16.  Results do not depend on the count.
+inline unsigned host_threads() {
+    static const unsigned n = [] {
+        const char *e = std::getenv("RBS_HOST_THREADS");
+        const int v = e ? std::atoi(e) : 0;
+        if (v >= 1) return (unsigned)std::min(v, 64);
+        return std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    }();
+    return n;
+}
+
+// fn(i) for every i in [0, count) on up to host_threads() threads (an
+// atomic work counter); fn writes only what index i owns.
 template <typename F> void parallel_for(size_t count, F &&fn) {
     std::atomic<size_t> next{0};
     auto work = [&] {
         for (size_t i; (i = next.fetch_add(1)) < count;) fn(i);
     };
-    const unsigned nth = (unsigned)std::min<size_t>(count, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+    const unsigned nth = (unsigned)std::min<size_t>(count, host_threads());
     std::vector<std::thread> th;
     for (unsigned t = 1; t < nth; ++t) th.emplace_back(work);
     work();
