@@ -734,12 +734,15 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
     P.label.resize(n);
     P.perm.resize(n);
     std::vector<int> pos_of((size_t)n);
-    for (int i = 0; i < n; ++i) {
-        int orig = P.bfs_item[i];
-        P.label[orig] = substitution == RBS_FORWARD ? i : n - 1 - i;
-        P.perm[i] = orig;  // processing position i is BFS position i in both directions
-        pos_of[orig] = i;
-    }
+    constexpr int kLab = 1 << 16;  // positions per host-thread chunk (the level order is a permutation)
+    parallel_for(((size_t)n + kLab - 1) / kLab, [&](size_t ch) {
+        for (int i = (int)ch * kLab; i < std::min(n, (int)ch * kLab + kLab); ++i) {
+            int orig = P.bfs_item[i];
+            P.label[orig] = substitution == RBS_FORWARD ? i : n - 1 - i;
+            P.perm[i] = orig;  // processing position i is BFS position i in both directions
+            pos_of[orig] = i;
+        }
+    });
 
     // 4. processing-order CSR with columns ascending (the result of a stable
     //    sort by processing column and then by row), row by row from the
