@@ -3,7 +3,11 @@
 // that restarts.  The file holds the plan's host side (scalars, options,
 // the reference-format inputs kept for export, level order, labels, the
 // execution blocks and every pool) in a versioned binary layout of this
-// build; the device state is rebuilt from it on load.
+// build, followed by a 64-bit digest of everything before it; the device
+// state is rebuilt from it on load.  A file whose digest does not match is
+// rejected, so a damaged plan never reaches the kernels (plan files are this
+// library's own output: the digest guards against damage, not forgery).
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -17,29 +21,78 @@ namespace rbs {
 
 namespace {
 
-constexpr char kMagic[8] = {'R', 'B', 'S', 'P', 'L', 'A', 'N', '1'};
+constexpr char kMagic[8] = {'R', 'B', 'S', 'P', 'L', 'A', 'N', '2'};
+
+// The SplitMix64 output function (Steele, Lea and Flood, "Fast splittable
+// pseudorandom number generators", OOPSLA 2014): a 64-bit mixing step.
+inline uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+// Digest of n bytes: 8-byte words folded through mix64 in 1 MB chunks (on
+// host threads for large ranges), the chunk digests then folded in order.
+uint64_t digest(const void *p, size_t n) {
+    const unsigned char *b = static_cast<const unsigned char *>(p);
+    constexpr size_t kChunk = size_t(1) << 20;
+    const size_t nch = (n + kChunk - 1) / kChunk;
+    std::vector<uint64_t> part(nch);
+    auto one = [&](size_t c) {
+        const size_t s = c * kChunk, e = std::min(n, s + kChunk);
+        uint64_t h = mix64(0x9e3779b97f4a7c15ULL + c);
+        size_t i = s;
+        for (; i + 8 <= e; i += 8) {
+            uint64_t w;
+            std::memcpy(&w, b + i, 8);
+            h = mix64(h ^ w);
+        }
+        if (i < e) {
+            uint64_t w = 0;
+            std::memcpy(&w, b + i, e - i);
+            h = mix64(h ^ w ^ ((uint64_t)(e - i) << 56));
+        }
+        part[c] = h;
+    };
+    if (nch > 4)
+        parallel_for(nch, one);
+    else
+        for (size_t c = 0; c < nch; ++c) one(c);
+    uint64_t h = mix64(n);
+    for (uint64_t x : part) h = mix64(h ^ x);
+    return h;
+}
 
 struct Writer {
     FILE *f;
     bool ok = true;
+    uint64_t sum = 0;  // digest of every byte written through pod/vec
+    void fold(const void *p, size_t n) { sum = mix64(sum ^ digest(p, n)); }
     template <typename T>
     void pod(const T &v) {
+        fold(&v, sizeof(T));
         ok = ok && std::fwrite(&v, sizeof(T), 1, f) == 1;
     }
     template <typename T, typename A>
     void vec(const std::vector<T, A> &v) {
         const uint64_t n = v.size();
         pod(n);
-        if (n) ok = ok && std::fwrite(v.data(), sizeof(T), n, f) == n;
+        if (n) {
+            fold(v.data(), sizeof(T) * (size_t)n);
+            ok = ok && std::fwrite(v.data(), sizeof(T), n, f) == n;
+        }
     }
 };
 
 struct Reader {
     FILE *f;
     bool ok = true;
+    uint64_t sum = 0;  // digest of every byte read through pod/vec
+    void fold(const void *p, size_t n) { sum = mix64(sum ^ digest(p, n)); }
     template <typename T>
     void pod(T &v) {
         ok = ok && std::fread(&v, sizeof(T), 1, f) == 1;
+        if (ok) fold(&v, sizeof(T));
     }
     template <typename T, typename A>
     void vec(std::vector<T, A> &v) {
@@ -50,7 +103,10 @@ struct Reader {
             return;
         }
         v.resize((size_t)n);
-        if (n) ok = ok && std::fread(v.data(), sizeof(T), n, f) == n;
+        if (n) {
+            ok = ok && std::fread(v.data(), sizeof(T), n, f) == n;
+            if (ok) fold(v.data(), sizeof(T) * (size_t)n);
+        }
     }
 };
 
@@ -120,6 +176,8 @@ int plan_save(const Plan &P, const char *path, std::string &err) {
     w.ok = std::fwrite(kMagic, 1, sizeof(kMagic), f) == sizeof(kMagic);
     w.pod(layout_signature());
     fields(w, const_cast<Plan &>(P));
+    const uint64_t sum = w.sum;
+    w.ok = w.ok && std::fwrite(&sum, sizeof(sum), 1, f) == 1;
     const bool ok = w.ok && std::fclose(f) == 0;
     if (!ok) {
         err = std::string("rbs_plan_save: write failed: ") + path;
@@ -145,9 +203,16 @@ int plan_load(Plan &P, const char *path, std::string &err) {
         return RBS_ERR_ARG;
     }
     fields(r, P);
+    uint64_t stored = 0;
+    const bool have_sum = r.ok && std::fread(&stored, sizeof(stored), 1, f) == 1;
+    const bool at_end = have_sum && std::fgetc(f) == EOF;
     std::fclose(f);
-    if (!r.ok) {
+    if (!r.ok || !have_sum) {
         err = std::string("rbs_plan_load: truncated or corrupt plan file: ") + path;
+        return RBS_ERR_ARG;
+    }
+    if (stored != r.sum || !at_end) {
+        err = std::string("rbs_plan_load: plan file damaged (digest mismatch): ") + path;
         return RBS_ERR_ARG;
     }
     // consistency of the sizes the executor relies on

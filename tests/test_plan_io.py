@@ -1,6 +1,7 @@
 """Saved plans (rbs_plan_save / rbs_plan_load) restore the analysis exactly:
 every reference-format array and the execution layouts, without a new level
-search; bad files are rejected."""
+search; bad files (wrong magic, truncated, damaged: a file digest covers
+every byte) are rejected."""
 import os
 
 import numpy as np
@@ -42,6 +43,18 @@ def test_load_rejects_bad_files(tmp_path):
         rbs.load_plan(cut, rbs.options(host_only=1))
     with pytest.raises(rbs.RbsError):
         rbs.load_plan(tmp_path / "missing.rbs", rbs.options(host_only=1))
+    # one flipped bit anywhere in the body (here inside the pools), or bytes
+    # appended, fail the file digest before anything reaches the device
+    for at in (len(raw) // 3, len(raw) - 9):
+        flip = bytearray(raw)
+        flip[at] ^= 0x10
+        (tmp_path / "flip.rbs").write_bytes(bytes(flip))
+        with pytest.raises(rbs.RbsError) as e:
+            rbs.load_plan(tmp_path / "flip.rbs", rbs.options(host_only=1))
+        assert "damaged" in str(e.value)
+    (tmp_path / "long.rbs").write_bytes(raw + b"\0")
+    with pytest.raises(rbs.RbsError):
+        rbs.load_plan(tmp_path / "long.rbs", rbs.options(host_only=1))
 
 
 @pytest.mark.gpu
