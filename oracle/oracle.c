@@ -10,6 +10,9 @@
 #include "oracle.h"
 
 #include <math.h>
+#include <pthread.h>
+#include <sched.h>
+#include <stdatomic.h>
 #include <ctype.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -535,6 +538,166 @@ int orc_sptrsv_csr_compensated(int n, const int *rowptr, const int *colidx, cons
         x[i] = (sum + comp) / val[d];
     }
     return 0;
+}
+
+/* Level-scheduled substitution (the CPU baseline of the benchmark; not used
+ * as a checker).  prepare: level of row i = 1 + the highest level among its
+ * dependencies (columns j < i forward, j > i backward), rows bucketed by
+ * level in row order, and a copy of the matrix in that order (the order the
+ * reference's level-set reordering gives, utils_reordering.h:102-210):
+ * row q of the copy is row item[q], its off-diagonal entries in stored order
+ * with columns renumbered to positions, its diagonal apart.  solve: each
+ * level's rows split over nthreads host threads (rows of one level are
+ * independent; a spin barrier between levels), each row reading its b
+ * entry and writing its x entry in the caller's order as it is solved.  Every row sums its entries in stored order and
+ * divides by the diagonal last, as orc_sptrsv_csr does, so results are
+ * identical to it bit for bit. */
+int orc_levels_prepare(int n, const int *rowptr, const int *colidx, const double *val, int substitution,
+                       orc_levels *L) {
+    memset(L, 0, sizeof(*L));
+    int *lev = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    int nl = 0;
+    for (int s = 0; s < n; ++s) {
+        int i = substitution == ORC_FORWARD ? s : n - 1 - s;
+        int d = find_diag(rowptr, colidx, i), m = -1;
+        if (d < 0 || val[d] == 0.0) {
+            free(lev);
+            return -1;
+        }
+        for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+            int j = colidx[k];
+            if (k == d) continue;
+            if ((substitution == ORC_FORWARD) ? j >= i : j <= i) {
+                free(lev);
+                return -1; /* outside the triangle */
+            }
+            if (lev[j] > m) m = lev[j];
+        }
+        lev[i] = m + 1;
+        if (m + 2 > nl) nl = m + 2;
+    }
+    L->n = n;
+    L->nlevel = nl;
+    L->lp = (int *)calloc((size_t)nl + 1, sizeof(int));
+    L->item = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    int *pos = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    for (int i = 0; i < n; ++i) L->lp[lev[i] + 1]++;
+    for (int l = 0; l < nl; ++l) L->lp[l + 1] += L->lp[l];
+    int *fill = (int *)malloc(sizeof(int) * (size_t)(nl > 0 ? nl : 1));
+    memcpy(fill, L->lp, sizeof(int) * (size_t)nl);
+    for (int i = 0; i < n; ++i) L->item[fill[lev[i]]++] = i;
+    for (int q = 0; q < n; ++q) pos[L->item[q]] = q;
+    const int off = rowptr[n] - n;
+    L->prp = (int *)malloc(sizeof(int) * ((size_t)n + 1));
+    L->pci = (int *)malloc(sizeof(int) * (size_t)(off > 0 ? off : 1));
+    L->pva = (double *)malloc(sizeof(double) * (size_t)(off > 0 ? off : 1));
+    L->pdiag = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    L->px = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    int o = 0;
+    L->prp[0] = 0;
+    for (int q = 0; q < n; ++q) {
+        int i = L->item[q], d = find_diag(rowptr, colidx, i);
+        for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+            if (k == d) continue;
+            L->pci[o] = pos[colidx[k]];
+            L->pva[o++] = val[k];
+        }
+        L->prp[q + 1] = o;
+        L->pdiag[q] = val[d];
+    }
+    free(fill);
+    free(pos);
+    free(lev);
+    return 0;
+}
+
+/* sense-reversing spin barrier of the solve's thread team */
+typedef struct {
+    atomic_int count, sense;
+    int n;
+} lv_barrier;
+
+static void lv_wait(lv_barrier *br, int *local) {
+    *local = !*local;
+    if (atomic_fetch_add(&br->count, 1) == br->n - 1) {
+        atomic_store(&br->count, 0);
+        atomic_store(&br->sense, *local);
+    } else {
+        int spins = 0;
+        while (atomic_load(&br->sense) != *local)
+            if (++spins > 4096) {
+                sched_yield();
+                spins = 0;
+            }
+    }
+}
+
+typedef struct {
+    const orc_levels *L;
+    const double *b;
+    double *x;
+    lv_barrier *br;
+    atomic_int *go; /* set once the team's size is final */
+    int t, nt;
+} lv_task;
+
+static void *lv_run(void *arg) {
+    const lv_task *w = (const lv_task *)arg;
+    while (!atomic_load(w->go)) sched_yield();
+    const orc_levels *L = w->L;
+    const int n = L->n, t = w->t, nt = w->nt;
+    const int *lp = L->lp, *item = L->item, *prp = L->prp, *pci = L->pci;
+    const double *pva = L->pva, *pdiag = L->pdiag;
+    double *px = L->px;
+    int local = 0;
+    (void)n;
+    for (int l = 0; l < L->nlevel; ++l) {
+        const int lo = lp[l], cnt = lp[l + 1] - lo;
+        for (int q = lo + (int)((long long)cnt * t / nt); q < lo + (int)((long long)cnt * (t + 1) / nt); ++q) {
+            double acc = 0.0;
+            for (int k = prp[q]; k < prp[q + 1]; ++k) acc += pva[k] * px[pci[k]];
+            const double v = (w->b[item[q]] - acc) / pdiag[q];
+            px[q] = v;
+            w->x[item[q]] = v;
+        }
+        if (nt > 1) lv_wait(w->br, &local);
+    }
+    return NULL;
+}
+
+void orc_levels_solve(const orc_levels *L, const double *b, double *x, int nthreads) {
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    lv_barrier br;
+    atomic_int go;
+    atomic_init(&br.count, 0);
+    atomic_init(&br.sense, 0);
+    atomic_init(&go, 0);
+    lv_task w[256];
+    pthread_t th[256];
+    int started = 1;
+    for (int t = 0; t < nthreads; ++t) w[t] = (lv_task){L, b, x, &br, &go, t, nthreads};
+    for (int t = 1; t < nthreads; ++t) {
+        if (pthread_create(&th[t], NULL, lv_run, &w[t]) != 0) break;
+        ++started;
+    }
+    /* the team is the threads that started (the caller included) */
+    br.n = started;
+    for (int t = 0; t < started; ++t) w[t].nt = started;
+    atomic_store(&go, 1);
+    lv_run(&w[0]);
+    for (int t = 1; t < started; ++t) pthread_join(th[t], NULL);
+}
+
+void orc_levels_free(orc_levels *L) {
+    free(L->lp);
+    free(L->item);
+    free(L->prp);
+    free(L->pci);
+    free(L->pva);
+    free(L->pdiag);
+    free(L->px);
+    memset(L, 0, sizeof(*L));
 }
 
 int orc_sptrsv_csr_multi(int n, const int *rowptr, const int *colidx, const double *val,

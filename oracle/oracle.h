@@ -97,6 +97,18 @@ int orc_sptrsv_csr(int n, const int *rowptr, const int *colidx, const double *va
 /* Same with Neumaier-compensated row sums (bounds the oracle's own rounding). */
 int orc_sptrsv_csr_compensated(int n, const int *rowptr, const int *colidx, const double *val,
                                int substitution, const double *b, double *x);
+/* Level-scheduled substitution over a level-ordered copy of the matrix, on
+ * host threads; results identical to orc_sptrsv_csr (the benchmark's
+ * threaded CPU baseline). */
+typedef struct orc_levels {
+    int n, nlevel;
+    int *lp, *item, *prp, *pci;
+    double *pva, *pdiag, *px;
+} orc_levels;
+int orc_levels_prepare(int n, const int *rowptr, const int *colidx, const double *val, int substitution,
+                       orc_levels *L);
+void orc_levels_solve(const orc_levels *L, const double *b, double *x, int nthreads);
+void orc_levels_free(orc_levels *L);
 /* k right-hand sides, column-major with leading dimension ld. */
 int orc_sptrsv_csr_multi(int n, const int *rowptr, const int *colidx, const double *val,
                          int substitution, int k, const double *b, int ldb, double *x, int ldx);

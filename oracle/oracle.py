@@ -62,6 +62,18 @@ lib.orc_tri_extract.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, _dp, 
 MTX_REF_DUMP = os.path.join(_HERE, "_ref", "mtx_dump")
 
 
+class _Levels(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("nlevel", ctypes.c_int)] + [(f, _ip) for f in ("lp", "item", "prp", "pci")] + [
+        (f, _dp) for f in ("pva", "pdiag", "px")]
+
+
+lib.orc_levels_prepare.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, ctypes.POINTER(_Levels)]
+lib.orc_levels_solve.argtypes = [ctypes.POINTER(_Levels), _dp, _dp, ctypes.c_int]
+lib.orc_levels_solve.restype = None
+lib.orc_levels_free.argtypes = [ctypes.POINTER(_Levels)]
+lib.orc_levels_free.restype = None
+
+
 def _i(a):
     return np.ascontiguousarray(a, dtype=np.int32)
 
@@ -168,6 +180,34 @@ def sptrsv_csr(rowptr, colidx, val, substitution, b, compensated=False):
             raise RuntimeError("oracle substitution: zero or missing diagonal")
         xs[c] = xc
     return xs.reshape(b.shape)
+
+
+class LevelSolver:
+    """Level-scheduled substitution on host threads over a level-ordered copy
+    of a CSR triangle (orc_levels_*): the benchmark's threaded CPU baseline.
+    Results equal sptrsv_csr's bit for bit."""
+
+    def __init__(self, rowptr, colidx, val, substitution):
+        self._keep = (_i(rowptr), _i(colidx), _d(val))
+        rp, ci, va = self._keep
+        self.n = len(rp) - 1
+        self._L = _Levels()
+        if lib.orc_levels_prepare(self.n, rp.ctypes.data_as(_ip), ci.ctypes.data_as(_ip), va.ctypes.data_as(_dp),
+                                  substitution, ctypes.byref(self._L)) != 0:
+            raise RuntimeError("oracle level solver: missing/zero diagonal or entry outside the triangle")
+        self.nlevel = self._L.nlevel
+
+    def solve(self, b, x=None, threads=1):
+        b = _d(b)
+        if x is None:
+            x = np.empty(self.n)
+        lib.orc_levels_solve(ctypes.byref(self._L), b.ctypes.data_as(_dp), x.ctypes.data_as(_dp), int(threads))
+        return x
+
+    def __del__(self):
+        if getattr(self, "_L", None) is not None:
+            lib.orc_levels_free(ctypes.byref(self._L))
+            self._L = None
 
 
 def ilu0_csr(rowptr, colidx, val):

@@ -2,7 +2,9 @@
 tolerance: plain serial substitution against the same substitution with
 Neumaier-compensated row sums (oracle.c) on the structures the GPU parity
 tests use, both directions, agree to 1e-14 relative (2-norm), and both
-recover a known solution (b = L x_true) to 1e-12."""
+recover a known solution (b = L x_true) to 1e-12.  The level-scheduled
+threaded substitution (the benchmark's CPU baseline) equals the serial one
+bit for bit."""
 import numpy as np
 import pytest
 
@@ -34,3 +36,18 @@ def test_oracle_error_is_below_the_parity_tolerance(name, csr, sub):
     xc = oracle.sptrsv_csr(rp, ci, va, sub, b, compensated=True)
     assert rel(x, xc) <= 1e-14
     assert rel(x, x_true) <= 1e-12 and rel(xc, x_true) <= 1e-12
+
+
+@pytest.mark.parametrize("name,csr", list(structures()), ids=lambda v: v if isinstance(v, str) else "")
+@pytest.mark.parametrize("sub", [rbs.FORWARD, rbs.BACKWARD])
+def test_level_scheduled_cpu_solve_equals_serial(name, csr, sub):
+    # the benchmark's threaded CPU baseline (oracle.LevelSolver) gives the
+    # serial substitution's x bit for bit at any thread count
+    rp, ci, va = csr
+    if sub == rbs.BACKWARD:
+        rp, ci, va = oracle.transpose(rp, ci, va)
+    b = rbs.gen_uniform(23, len(rp) - 1)
+    x = oracle.sptrsv_csr(rp, ci, va, sub, b)
+    lvl = oracle.LevelSolver(rp, ci, va, sub)
+    for threads in (1, 3, 8):
+        assert np.array_equal(lvl.solve(b, threads=threads).view(np.uint64), x.view(np.uint64)), threads
