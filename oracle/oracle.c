@@ -578,6 +578,7 @@ int orc_levels_prepare(int n, const int *rowptr, const int *colidx, const double
     }
     L->n = n;
     L->nlevel = nl;
+    L->substitution = substitution;
     L->lp = (int *)calloc((size_t)nl + 1, sizeof(int));
     L->item = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
     int *pos = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
@@ -604,6 +605,22 @@ int orc_levels_prepare(int n, const int *rowptr, const int *colidx, const double
         }
         L->prp[q + 1] = o;
         L->pdiag[q] = val[d];
+    }
+    L->nrp = (int *)malloc(sizeof(int) * ((size_t)n + 1));
+    L->nci = (int *)malloc(sizeof(int) * (size_t)(off > 0 ? off : 1));
+    L->nva = (double *)malloc(sizeof(double) * (size_t)(off > 0 ? off : 1));
+    L->ndiag = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    o = 0;
+    L->nrp[0] = 0;
+    for (int i = 0; i < n; ++i) {
+        int d = find_diag(rowptr, colidx, i);
+        for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+            if (k == d) continue;
+            L->nci[o] = colidx[k];
+            L->nva[o++] = val[k];
+        }
+        L->nrp[i + 1] = o;
+        L->ndiag[i] = val[d];
     }
     free(fill);
     free(pos);
@@ -666,7 +683,16 @@ static void *lv_run(void *arg) {
 }
 
 void orc_levels_solve(const orc_levels *L, const double *b, double *x, int nthreads) {
-    if (nthreads < 1) nthreads = 1;
+    if (nthreads <= 0) { /* serial, the rows' own order */
+        const int n = L->n;
+        for (int s = 0; s < n; ++s) {
+            const int i = L->substitution == ORC_FORWARD ? s : n - 1 - s;
+            double acc = 0.0;
+            for (int k = L->nrp[i]; k < L->nrp[i + 1]; ++k) acc += L->nva[k] * x[L->nci[k]];
+            x[i] = (b[i] - acc) / L->ndiag[i];
+        }
+        return;
+    }
     if (nthreads > 256) nthreads = 256;
     lv_barrier br;
     atomic_int go;
@@ -697,6 +723,10 @@ void orc_levels_free(orc_levels *L) {
     free(L->pva);
     free(L->pdiag);
     free(L->px);
+    free(L->nrp);
+    free(L->nci);
+    free(L->nva);
+    free(L->ndiag);
     memset(L, 0, sizeof(*L));
 }
 

@@ -98,12 +98,15 @@ int orc_sptrsv_csr(int n, const int *rowptr, const int *colidx, const double *va
 int orc_sptrsv_csr_compensated(int n, const int *rowptr, const int *colidx, const double *val,
                                int substitution, const double *b, double *x);
 /* Level-scheduled substitution over a level-ordered copy of the matrix, on
- * host threads; results identical to orc_sptrsv_csr (the benchmark's
- * threaded CPU baseline). */
+ * host threads (nthreads >= 1), or serial substitution over a copy in the
+ * rows' own order with the diagonal apart (nthreads == 0); results identical
+ * to orc_sptrsv_csr (the benchmark's CPU baseline). */
 typedef struct orc_levels {
-    int n, nlevel;
+    int n, nlevel, substitution;
     int *lp, *item, *prp, *pci;
     double *pva, *pdiag, *px;
+    int *nrp, *nci; /* the rows in their own order, diagonal apart (nthreads == 0) */
+    double *nva, *ndiag;
 } orc_levels;
 int orc_levels_prepare(int n, const int *rowptr, const int *colidx, const double *val, int substitution,
                        orc_levels *L);

@@ -63,8 +63,9 @@ MTX_REF_DUMP = os.path.join(_HERE, "_ref", "mtx_dump")
 
 
 class _Levels(ctypes.Structure):
-    _fields_ = [("n", ctypes.c_int), ("nlevel", ctypes.c_int)] + [(f, _ip) for f in ("lp", "item", "prp", "pci")] + [
-        (f, _dp) for f in ("pva", "pdiag", "px")]
+    _fields_ = ([("n", ctypes.c_int), ("nlevel", ctypes.c_int), ("substitution", ctypes.c_int)]
+                + [(f, _ip) for f in ("lp", "item", "prp", "pci")] + [(f, _dp) for f in ("pva", "pdiag", "px")]
+                + [(f, _ip) for f in ("nrp", "nci")] + [(f, _dp) for f in ("nva", "ndiag")])
 
 
 lib.orc_levels_prepare.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_int, ctypes.POINTER(_Levels)]
@@ -184,8 +185,9 @@ def sptrsv_csr(rowptr, colidx, val, substitution, b, compensated=False):
 
 class LevelSolver:
     """Level-scheduled substitution on host threads over a level-ordered copy
-    of a CSR triangle (orc_levels_*): the benchmark's threaded CPU baseline.
-    Results equal sptrsv_csr's bit for bit."""
+    of a CSR triangle (threads >= 1), or serial substitution over a copy in
+    the rows' own order (threads == 0) (orc_levels_*): the benchmark's CPU
+    baseline.  Results equal sptrsv_csr's bit for bit."""
 
     def __init__(self, rowptr, colidx, val, substitution):
         self._keep = (_i(rowptr), _i(colidx), _d(val))

@@ -49,5 +49,5 @@ def test_level_scheduled_cpu_solve_equals_serial(name, csr, sub):
     b = rbs.gen_uniform(23, len(rp) - 1)
     x = oracle.sptrsv_csr(rp, ci, va, sub, b)
     lvl = oracle.LevelSolver(rp, ci, va, sub)
-    for threads in (1, 3, 8):
+    for threads in (0, 1, 3, 8):  # 0: serial over the rows' own order
         assert np.array_equal(lvl.solve(b, threads=threads).view(np.uint64), x.view(np.uint64)), threads
