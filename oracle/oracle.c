@@ -628,6 +628,10 @@ int orc_levels_prepare(int n, const int *rowptr, const int *colidx, const double
     return 0;
 }
 
+/* levels of fewer rows than this are solved by one thread of the team, a
+ * run of them between two barriers (a barrier costs more than the rows) */
+#define LV_SMALL 192
+
 /* sense-reversing spin barrier of the solve's thread team */
 typedef struct {
     atomic_int count, sense;
@@ -668,9 +672,19 @@ static void *lv_run(void *arg) {
     double *px = L->px;
     int local = 0;
     (void)n;
-    for (int l = 0; l < L->nlevel; ++l) {
-        const int lo = lp[l], cnt = lp[l + 1] - lo;
-        for (int q = lo + (int)((long long)cnt * t / nt); q < lo + (int)((long long)cnt * (t + 1) / nt); ++q) {
+    for (int l = 0; l < L->nlevel;) {
+        int lo = lp[l], hi = lp[l + 1], next = l + 1;
+        if (nt > 1 && hi - lo < LV_SMALL) {
+            /* a run of small levels: thread 0 solves them in order, one barrier */
+            while (next < L->nlevel && lp[next + 1] - lp[next] < LV_SMALL) ++next;
+            hi = lp[next];
+            if (t != 0) hi = lo;
+        } else {
+            const int cnt = hi - lo;
+            hi = lo + (int)((long long)cnt * (t + 1) / nt);
+            lo = lo + (int)((long long)cnt * t / nt);
+        }
+        for (int q = lo; q < hi; ++q) {
             double acc = 0.0;
             for (int k = prp[q]; k < prp[q + 1]; ++k) acc += pva[k] * px[pci[k]];
             const double v = (w->b[item[q]] - acc) / pdiag[q];
@@ -678,6 +692,7 @@ static void *lv_run(void *arg) {
             w->x[item[q]] = v;
         }
         if (nt > 1) lv_wait(w->br, &local);
+        l = next;
     }
     return NULL;
 }
