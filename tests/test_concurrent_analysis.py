@@ -6,8 +6,6 @@ malformed one fails, with its own message."""
 import struct
 import threading
 
-import numpy as np
-
 import rbs
 from oracle import oracle
 
