@@ -546,12 +546,15 @@ int orc_sptrsv_csr_compensated(int n, const int *rowptr, const int *colidx, cons
  * level in row order, and a copy of the matrix in that order (the order the
  * reference's level-set reordering gives, utils_reordering.h:102-210):
  * row q of the copy is row item[q], its off-diagonal entries in stored order
- * with columns renumbered to positions, its diagonal apart.  solve: each
- * level's rows split over nthreads host threads (rows of one level are
- * independent; a spin barrier between levels), each row reading its b
- * entry and writing its x entry in the caller's order as it is solved.  Every row sums its entries in stored order and
- * divides by the diagonal last, as orc_sptrsv_csr does, so results are
- * identical to it bit for bit. */
+ * with columns renumbered to positions, its diagonal apart; plus a copy in
+ * the rows' own order with the diagonal apart.  solve, nthreads >= 1: each
+ * level's rows split over the threads (rows of one level are independent;
+ * a spin barrier between levels, runs of small levels solved by one
+ * thread), each row reading its b entry and writing its x entry in the
+ * caller's order as it is solved; nthreads == 0: serial substitution over
+ * the second copy.  Every row sums its entries in stored order and divides
+ * by the diagonal last, as orc_sptrsv_csr does, so results are identical to
+ * it bit for bit. */
 int orc_levels_prepare(int n, const int *rowptr, const int *colidx, const double *val, int substitution,
                        orc_levels *L) {
     memset(L, 0, sizeof(*L));
@@ -567,7 +570,7 @@ int orc_levels_prepare(int n, const int *rowptr, const int *colidx, const double
         for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
             int j = colidx[k];
             if (k == d) continue;
-            if ((substitution == ORC_FORWARD) ? j >= i : j <= i) {
+            if (j < 0 || j >= n || ((substitution == ORC_FORWARD) ? j >= i : j <= i)) {
                 free(lev);
                 return -1; /* outside the triangle */
             }
