@@ -3,7 +3,8 @@
 // a banded system large enough for every threaded step (transposition, row
 // builds, statistics, pool fill, level-chunk and ELL layouts) as CSR forward
 // and as CSC backward, in AUTO and TUNE, and a 40-system batch whose
-// level-chunk layouts are built per system on host threads.
+// level-chunk layouts are built per system on host threads, saved to a plan
+// file and loaded back.
 #include <algorithm>
 #include <cstdio>
 #include <random>
@@ -51,7 +52,7 @@ static rbs_options opts(int select) {
     return o;
 }
 
-int main() {
+int main(int argc, char **argv) {
     int bad = 0;
     std::vector<int> rp, ci;
     std::vector<double> va;
@@ -84,9 +85,17 @@ int main() {
     const int N = (int)bp.size() - 1, Z = (int)bi.size();
     for (int sel : {RBS_SELECT_AUTO, RBS_SELECT_TUNE}) {
         std::string err;
-        Plan P;
+        Plan P, Q;
         bad |= analyse_host(P, bp.data(), bi.data(), bv.data(), N, Z, RBS_FMT_CSR, RBS_FORWARD, 0, opts(sel), err, &segs);
         if (P.lc_rec64.empty()) bad = 1;
+        // the plan file round trip (its digest is computed on host threads)
+        const char *path = argc > 1 ? argv[1] : "analysis_driver.rbs";
+        bad |= plan_save(P, path, err);
+        bad |= plan_load(Q, path, err);
+        if (Q.lc_rec64 != P.lc_rec64 || Q.col_pool != P.col_pool || Q.val_pool != P.val_pool || Q.ell_col != P.ell_col)
+            bad = 1;
+        std::remove(path);
+        if (!err.empty()) std::printf("%s\n", err.c_str());
     }
     std::printf("analysis driver: %s\n", bad ? "FAILED" : "ok");
     return bad ? 1 : 0;
