@@ -94,6 +94,18 @@ template <typename F> void parallel_for(size_t count, F &&fn) {
     for (auto &t : th) t.join();
 }
 
+// FP32 copy of an FP64 array (each value rounded to nearest), converted on
+// host threads.
+template <typename V> bulk_vector<float> to_f32(const V &src) {
+    bulk_vector<float> out(src.size());
+    constexpr size_t kChunk = size_t(1) << 20;
+    parallel_for((src.size() + kChunk - 1) / kChunk, [&](size_t c) {
+        const size_t e = std::min(src.size(), (c + 1) * kChunk);
+        for (size_t i = c * kChunk; i < e; ++i) out[i] = (float)src[i];
+    });
+    return out;
+}
+
 // Smallest i in [0, count) with bad(i), or -1 (chunks scanned on host
 // threads): the index a serial check would stop at.
 template <typename F> long long first_bad(long long count, F &&bad) {

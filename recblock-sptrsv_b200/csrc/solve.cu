@@ -734,9 +734,7 @@ int device_build(Plan &P, std::string &err) {
     if ((rc = upload(D, D.inv, P.inv_diag, err))) return rc;
     D.mixed = P.opt.mixed != 0;
     if (D.mixed) {
-        std::vector<float> v32(P.val_pool.size()), i32(P.inv_diag.size());
-        for (size_t i = 0; i < v32.size(); ++i) v32[i] = (float)P.val_pool[i];
-        for (size_t i = 0; i < i32.size(); ++i) i32[i] = (float)P.inv_diag[i];
+        const auto v32 = to_f32(P.val_pool), i32 = to_f32(P.inv_diag);
         if ((rc = upload(D, D.val32, v32, err))) return rc;
         if ((rc = upload(D, D.inv32, i32, err))) return rc;
         if ((rc = upload(D, D.full_rp, P.full_rp, err))) return rc;
@@ -758,7 +756,7 @@ int device_build(Plan &P, std::string &err) {
         if ((rc = alloc(D, D.band_states, states, err))) return rc;
     }
     if (D.mixed) {
-        std::vector<float> c32(P.band_coef.begin(), P.band_coef.end()), i32(P.band_inv.begin(), P.band_inv.end());
+        const auto c32 = to_f32(P.band_coef), i32 = to_f32(P.band_inv);
         if ((rc = upload(D, D.band_coef32, c32, err))) return rc;
         if ((rc = upload(D, D.band_inv32, i32, err))) return rc;
     }
@@ -773,11 +771,11 @@ int device_build(Plan &P, std::string &err) {
     if ((rc = upload(D, D.ca_col, P.ca_col, err))) return rc;
     if ((rc = upload(D, D.ca_val, P.ca_val, err))) return rc;
     if (D.mixed) {
-        std::vector<float> c32(P.ca_val.begin(), P.ca_val.end());
+        const auto c32 = to_f32(P.ca_val);
         if ((rc = upload(D, D.ca_val32, c32, err))) return rc;
     }
     if (D.mixed) {
-        std::vector<float> e32(P.ell_val.begin(), P.ell_val.end());
+        const auto e32 = to_f32(P.ell_val);
         if ((rc = upload(D, D.ell_val32, e32, err))) return rc;
     }
     if (!P.lc_tab.empty()) {

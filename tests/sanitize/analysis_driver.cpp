@@ -4,7 +4,7 @@
 // builds, statistics, pool fill, level-chunk and ELL layouts) as CSR forward
 // and as CSC backward, in AUTO and TUNE, and a 40-system batch whose
 // level-chunk layouts are built per system on host threads, saved to a plan
-// file and loaded back.
+// file and loaded back; the FP32 copy of its value pool.
 #include <algorithm>
 #include <cstdio>
 #include <random>
@@ -88,6 +88,11 @@ int main(int argc, char **argv) {
         Plan P, Q;
         bad |= analyse_host(P, bp.data(), bi.data(), bv.data(), N, Z, RBS_FMT_CSR, RBS_FORWARD, 0, opts(sel), err, &segs);
         if (P.lc_rec64.empty()) bad = 1;
+        // the FP32 pool copy uploaded for mixed precision (converted on host threads)
+        const bulk_vector<float> v32 = to_f32(P.val_pool);
+        if (v32.size() != P.val_pool.size()) bad = 1;
+        for (size_t i = 0; i < v32.size(); ++i)
+            if (v32[i] != (float)P.val_pool[i]) bad = 1;
         // the plan file round trip (its digest is computed on host threads)
         const char *path = argc > 1 ? argv[1] : "analysis_driver.rbs";
         bad |= plan_save(P, path, err);
