@@ -1,6 +1,7 @@
 """The multi-GPU arm of bench.py runs independent replicas (a triangular
 solve has no data-path collective); the only cross-rank step is the max of
-the ranks' timed totals.  Checked here with world_size 2 over gloo on CPU."""
+the ranks' timed totals.  Checked here with world_size 2 over gloo on CPU.
+The reference arm runs on rank 0 alone and prints the contract's line."""
 import os
 import sys
 
@@ -54,3 +55,25 @@ def test_reference_arm_runs_on_rank0_only(monkeypatch, capsys):
     args = type("A", (), {"steps": 1, "warmup": 0, "gpus": 2})()
     bench.run_reference(args)  # returns without work or output on rank 1
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_line_on_rank0():
+    # the reference arm's JSON line (host CPU only): the metric of our arm,
+    # the CPU configuration it chose, an e2e with no host-device bytes, and
+    # the oracle's accuracy on the c1a workload
+    import json
+    import subprocess
+    env = dict(os.environ, RANK="0")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "2",
+                          "--warmup", "1"], capture_output=True, text=True, env=env, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    sys.path.insert(0, ROOT)
+    import bench
+    assert line["impl"] == "reference" and line["metric"] == bench.METRIC and line["unit"] == "solves/s"
+    assert line["value"] > 0 and line["steps"] == 2 and line["warmup"] == 1 and line["higher_is_better"]
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["value"] == line["value"] and 1 <= cb["cores"] <= bench.cpu_candidates()[-1]
+    assert line["e2e"] == {"value": line["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+    assert line["rel_err_vs_x_true"] <= 1e-12
