@@ -62,8 +62,11 @@ def parse():
                     help="structure of the timed solve (profiling runs; the benchmark line is c1a)")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, side measurements and the CPU baseline "
                                                                "(short runs for profilers)")
-    ap.add_argument("--side", default=None, choices=["analysis", "batched", "blocks", "ic0", "ilu0", "mtx", "serve"],
+    ap.add_argument("--side", default=None, choices=sorted(SIDE_FUNCS),
                     help="run one side measurement alone on cuda:0 and print its JSON (no benchmark line)")
+    ap.add_argument("--sides", default=None,
+                    help="comma-separated side measurements to run after the benchmark line's own "
+                         f"(default: {','.join(SIDE_DEFAULT)}; each in a child process)")
     return ap.parse_args()
 
 
@@ -77,26 +80,33 @@ def peaks():
 
 
 # ---------------------------------------------------------------- inputs ----
-def make_system(kind, sub, seed_x=1):
-    """Seeded L (or U = L^T), its CSC input, b and x_true (numpy/scipy only)."""
+FORWARD, BACKWARD = 0, 1
+SPECS = {
+    "c1a": dict(kind=1, grid=1024, seed=101),
+    "c1b": dict(kind=2, n=2000000, zipf_alpha=2.1, zipf_max=1000, seed=102),
+    "c1c": dict(kind=3, n=1000000, chain_bw=3, seed=103),
+    "c0": dict(kind=0, n=16384, lam=6, band=512, seed=100),
+    "c2r": dict(kind=0, n=4000000, lam=10, band=4096, seed=104),
+}
+
+
+def make_system(kind, sub, seed_x=1, gen=None):
+    """Seeded L (or U = L^T), its CSC input, b and x_true.  `gen` supplies
+    gen_lower_csr / gen_uniform: the library's generator for this
+    library's arm, the oracle's bit-identical restatement (oracle/gen.c,
+    tests/test_oracle_gen.py) for the CPU arm, which must not load the
+    library under test."""
     import scipy.sparse as sp
 
-    import rbs
-
-    specs = {
-        "c1a": dict(kind=rbs.GEN_LAPLACE2D, grid=1024, seed=101),
-        "c1b": dict(kind=rbs.GEN_ZIPF, n=2000000, zipf_alpha=2.1, zipf_max=1000, seed=102),
-        "c1c": dict(kind=rbs.GEN_CHAIN, n=1000000, chain_bw=3, seed=103),
-        "c0": dict(kind=rbs.GEN_BAND_POISSON, n=16384, lam=6, band=512, seed=100),
-        "c2r": dict(kind=rbs.GEN_BAND_POISSON, n=4000000, lam=10, band=4096, seed=104),
-    }
-    rp, ci, va = rbs.gen_lower_csr(**specs[kind])
+    if gen is None:
+        import rbs as gen
+    rp, ci, va = gen.gen_lower_csr(**SPECS[kind])
     n = len(rp) - 1
     L = sp.csr_matrix((va, ci, rp), shape=(n, n))
-    A = L if sub == rbs.FORWARD else L.T.tocsr()
+    A = L if sub == FORWARD else L.T.tocsr()
     csc = A.tocsc()
     csc.sort_indices()
-    x_true = rbs.gen_uniform(specs[kind]["seed"] + seed_x, n)
+    x_true = gen.gen_uniform(SPECS[kind]["seed"] + seed_x, n)
     b = A @ x_true
     return dict(n=n, nnz=A.nnz, cp=csc.indptr.astype(np.int32), ri=csc.indices.astype(np.int32),
                 cv=csc.data.astype(np.float64), b=b, x_true=x_true, A=A)
@@ -174,12 +184,11 @@ def cpu_best(system, reps=3):
     reference's preprocessing is."""
     from oracle import oracle
 
-    import rbs
     A = system["A"]
     rp, ci, va = A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data.astype(np.float64)
     b = system["b"]
-    x_serial = oracle.sptrsv_csr(rp, ci, va, rbs.FORWARD, b)
-    lvl = oracle.LevelSolver(rp, ci, va, rbs.FORWARD)
+    x_serial = oracle.sptrsv_csr(rp, ci, va, FORWARD, b)
+    lvl = oracle.LevelSolver(rp, ci, va, FORWARD)
     cands = [("serial substitution", 1, lambda bb: lvl.solve(bb, threads=0))]
     for t in cpu_candidates():
         cands.append(("level-scheduled substitution", t, lambda bb, t=t: lvl.solve(bb, threads=t)))
@@ -212,7 +221,8 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    sysm = make_system("c1a", 0)
+    from oracle import oracle
+    sysm = make_system("c1a", FORWARD, gen=oracle)
     name, threads, fn, _ = cpu_best(sysm)
     for _ in range(args.warmup):
         fn(sysm["b"])
@@ -234,7 +244,8 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "arm": arm},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} full c1a forward solves, {name}",
+                         "sample": f"{args.steps} full c1a forward solves, {name}; inputs from the oracle's "
+                                   "generator (bit-identical to the library's)",
                          "cpu": platform.processor() or "x86_64", "nproc": os.cpu_count()},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "rel_err_vs_x_true": err,
@@ -274,7 +285,7 @@ def measure(plan, dB, dX, flush, reps, k=1, prec=0):
     return float(np.mean(ms)), st
 
 
-def side_multi_rhs(plan, sysm, dev, flush, args):
+def side_multi_rhs(dev, args):
     """Multi-RHS column blocks on the 2D-Laplacian factor: k in {1, 8, 32,
     128}, FP64 and FP32 sweeps + FP64 refinement.  Columns of X_true are
     U(-1,1); B = L X_true."""
@@ -282,6 +293,9 @@ def side_multi_rhs(plan, sysm, dev, flush, args):
 
     import rbs
 
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    sysm = make_system("c1a", FORWARD)
+    plan = rbs.analyse(sysm["cp"], sysm["ri"], sysm["cv"], substitution=FORWARD, lv=-1)
     out = {}
     reps = max(3, args.steps // 10)
     A = sysm["A"]
@@ -304,12 +318,13 @@ def side_multi_rhs(plan, sysm, dev, flush, args):
     return out
 
 
-def side_structures(dev, flush, args):
+def side_structures(dev, args):
     """Config-1 structures and directions other than the headline."""
     import torch
 
     import rbs
 
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     sweep = {}
     for kind, sub in (("c1a", rbs.BACKWARD), ("c1b", rbs.FORWARD), ("c1b", rbs.BACKWARD), ("c1c", rbs.FORWARD),
                       ("c1c", rbs.BACKWARD)):
@@ -523,7 +538,7 @@ def side_ic0(dev, args):
             "apply_ms": float(np.median(apply_ms[1:]))}
 
 
-def side_mixed(dev, flush, args):
+def side_mixed(dev, args):
     """FP32 sweeps + FP64 refinement against the plain FP64 solve on the
     2D-Laplacian factor, the power-law factor and the n = 4M Poisson(10)
     band-4096 factor; errors against the serial FP64 oracle."""
@@ -532,6 +547,7 @@ def side_mixed(dev, flush, args):
     import rbs
     from oracle import oracle
 
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     out = {}
     for kind in ("c1a", "c1b", "c2r"):
         s2 = make_system(kind, rbs.FORWARD)
@@ -635,13 +651,18 @@ def serving_factors(count=64, seed=404):
     return out
 
 
-def side_serving(dev, args, n_requests=1500, loads=(200, 1000, 10000, 50000), batch_rhs=32):
-    """Poisson request arrivals over 64 device-resident factors; each request
-    carries 1-16 RHS; the server batches across and within factors and runs
-    FP32 sweeps + FP64 refinement.  Baselines: the same arrivals served one
-    request at a time with one FP64 solve of its k columns (host arrays in
-    and out), and the plain FP64 single-RHS path (one solve per column)."""
+def side_serving(dev, args, n_requests=1000, loads=(500, 1000, 2000, 10000, 50000), batch_rhs=32):
+    """Poisson request arrivals over 64 device-resident factors; each
+    request carries 1-16 right-hand sides in device arrays; the server
+    batches within factors (one multi-RHS solve per batch, columns read in
+    place) and across them (batches of all factors overlap on the device),
+    with FP32 sweeps + FP64 refinement.  Baselines, on the same arrivals and
+    device arrays: one plain FP64 rbs_solve of each request's k columns in
+    arrival order on the caller's thread, and the plain FP64 single-RHS path
+    (one rbs_solve per right-hand side, back to back)."""
     import threading
+
+    import torch
 
     import rbs
 
@@ -651,96 +672,116 @@ def side_serving(dev, args, n_requests=1500, loads=(200, 1000, 10000, 50000), ba
     plans = [rbs.analyse(*L, substitution=rbs.FORWARD, lv=-1, fmt=rbs.FMT_CSR) for L in facs]
     t_an = time.perf_counter() - t0
     rng = np.random.default_rng(505)
-    Bh = [rbs.gen_uniform(11000 + i, 16 * n).reshape(16, n) for i, n in enumerate(ns)]
-    Xh = [np.empty((16, n)) for n in ns]
+    # per factor: 16 right-hand-side columns and a 16-column output area on
+    # the device (a request of k columns uses the first k)
+    dB = [torch.tensor(rbs.gen_uniform(11000 + i, 16 * n), device=dev) for i, n in enumerate(ns)]
+    dX = [torch.empty_like(b) for b in dB]
     res = {"factors": 64, "rows": int(sum(ns)), "nnz": int(sum(len(L[1]) for L in facs)), "analyse_s": t_an,
            "requests_per_load": n_requests, "rhs_per_request": "uniform 1..16", "max_batch_rhs": batch_rhs,
-           "hbm_budget_gb": 150, "loads": {}}
+           "hbm_budget_gb": 150, "requests": "device arrays (rbs_server_submit_device)", "loads": {}}
 
     def schedule(rate):
         gaps = rng.exponential(1.0 / rate, n_requests)
         return np.cumsum(gaps), rng.integers(0, 64, n_requests), rng.integers(1, 17, n_requests)
 
     scheds = {rate: schedule(rate) for rate in loads}
+    for p in plans:  # the plain arms run at the widest request too: work vectors and graphs exist before timing
+        p.reserve(16)
+    for f in range(64):
+        for k in (1, 16):
+            for _ in range(2):
+                plans[f].solve(dB[f], dX[f], k=k)
     # plain: one FP64 solve per request, in arrival order, on the caller's thread
     plain = {}
     for rate in loads:
         arr, fid, ks = scheds[rate]
         lat = []
+        torch.cuda.synchronize()
         t_start = time.perf_counter()
         for a, f, k in zip(arr, fid, ks):
             while time.perf_counter() - t_start < a:
                 pass
-            plans[f].solve_host(Bh[f][:k], k=int(k), x=Xh[f][:k])
+            plans[f].solve(dB[f], dX[f], k=int(k))
             lat.append(time.perf_counter() - t_start - a)
         span = time.perf_counter() - t_start
         plain[rate] = {"p50_ms": 1000 * float(np.percentile(lat, 50)), "p99_ms": 1000 * float(np.percentile(lat, 99)),
                        "solves_per_s": float(ks.sum()) / span, "requests_per_s": n_requests / span}
-    # plain FP64 single-RHS path (one solve per right-hand side, host arrays),
-    # on the first requests of the 1000 req/s schedule, back to back
+    # plain FP64 single-RHS path: one solve per right-hand side, back to back,
+    # on the first 200 requests of the 1000 req/s schedule
     arr, fid, ks = scheds[loads[1] if len(loads) > 1 else loads[0]]
+    torch.cuda.synchronize()
     t_start = time.perf_counter()
     nsol = 0
     for f, k in zip(fid[:200], ks[:200]):
+        n = ns[f]
         for c in range(int(k)):
-            plans[f].solve_host(Bh[f][c], k=1, x=Xh[f][c])
+            plans[f].solve(dB[f][c * n:(c + 1) * n], dX[f][c * n:(c + 1) * n], k=1)
             nsol += 1
     single = nsol / (time.perf_counter() - t_start)
     res["plain_fp64_single_rhs"] = {"solves_per_s": single, "sample": "first 200 requests, one solve per RHS"}
     srv = rbs.Server(150 << 30, max_batch_rhs=batch_rhs)
     old_si = sys.getswitchinterval()
     sys.setswitchinterval(1e-4)  # the submit loop and the waiter share the interpreter
-    for p in plans:
-        srv.add_factor(p)
+    fids = [srv.add_factor(p) for p in plans]
     plans = None
-    for rate in loads:
-        arr, fid, ks = scheds[rate]
-        srv.reset_stats()
-        tickets = []
-        done = threading.Event()
-        lats = []
+    # warm-up: every factor once at one and at 16 columns, mixed (captures the block walks)
+    for f in range(64):
+        for k in (1, 16):
+            srv.wait(srv.submit_device(fids[f], dB[f], dX[f], k=k, prec=rbs.PREC_MIXED))
+    try:
+        for rate in loads:
+            arr, fid, ks = scheds[rate]
+            srv.reset_stats()
+            tickets = []
+            lats = []
+            failure = []
 
-        def waiter():
-            i = 0
-            while i < n_requests:
-                while i >= len(tickets):
-                    time.sleep(0)
-                lats.append(srv.wait(tickets[i])[0])
-                i += 1
-            done.set()
+            def waiter():
+                try:
+                    for i in range(n_requests):
+                        while i >= len(tickets):
+                            time.sleep(0)
+                        lats.append(srv.wait(tickets[i])[0])
+                except Exception as e:  # handed to the main thread below
+                    failure.append(e)
 
-        th = threading.Thread(target=waiter)
-        th.start()
-        lag = []
-        t_start = time.perf_counter()
-        for a, f, k in zip(arr, fid, ks):
-            while time.perf_counter() - t_start < a:
-                pass
-            lag.append(1000 * (time.perf_counter() - t_start - a))
-            tickets.append(srv.submit(int(f), Bh[f][:k], Xh[f][:k], k=int(k), prec=rbs.PREC_MIXED))
-        th.join()
-        lats = np.array(lats) + np.array(lag)  # latency from the scheduled arrival, as for the plain arm
-        span = time.perf_counter() - t_start
-        st = srv.stats()
-        res["loads"][str(rate)] = {
-            "served_mixed": {"p50_ms": float(np.percentile(lats, 50)), "p99_ms": float(np.percentile(lats, 99)),
-                             "solves_per_s": float(ks.sum()) / span, "requests_per_s": n_requests / span,
-                             "mean_batch_rhs": st.mean_batch_rhs, "batches": st.batches},
-            "plain_fp64": plain[rate]}
-        res["loads"][str(rate)]["x_plain_fp64"] = float(ks.sum()) / span / plain[rate]["solves_per_s"]
-        res["loads"][str(rate)]["x_plain_fp64_single_rhs"] = float(ks.sum()) / span / single
-    # accuracy: every factor once, b = L x_true, served mixed vs x_true
-    import scipy.sparse as sp
-    worst = 0.0
-    for i, (rp, ci, va) in enumerate(facs):
-        xt = rbs.gen_uniform(13000 + i, ns[i])
-        b = sp.csr_matrix((va, ci, rp), shape=(ns[i], ns[i])) @ xt
-        x = np.empty_like(b)
-        srv.wait(srv.submit(i, b, x, k=1, prec=rbs.PREC_MIXED))
-        worst = max(worst, rel(x, xt))
-    res["max_rel_err_vs_x_true"] = worst
-    sys.setswitchinterval(old_si)
-    srv.close()
+            th = threading.Thread(target=waiter)
+            th.start()
+            lag = []
+            t_start = time.perf_counter()
+            try:
+                for a, f, k in zip(arr, fid, ks):
+                    while time.perf_counter() - t_start < a:
+                        pass
+                    lag.append(1000 * (time.perf_counter() - t_start - a))
+                    tickets.append(srv.submit_device(fids[f], dB[f], dX[f], k=int(k), prec=rbs.PREC_MIXED))
+            finally:
+                th.join()
+            if failure:
+                raise failure[0]
+            span = time.perf_counter() - t_start
+            lats = np.array(lats) + np.array(lag)  # latency from the scheduled arrival, as for the plain arm
+            st = srv.stats()
+            res["loads"][str(rate)] = {
+                "served_mixed": {"p50_ms": float(np.percentile(lats, 50)), "p99_ms": float(np.percentile(lats, 99)),
+                                 "solves_per_s": float(ks.sum()) / span, "requests_per_s": n_requests / span,
+                                 "mean_batch_rhs": st.mean_batch_rhs, "batches": st.batches},
+                "plain_fp64": plain[rate]}
+            res["loads"][str(rate)]["x_plain_fp64"] = float(ks.sum()) / span / plain[rate]["solves_per_s"]
+            res["loads"][str(rate)]["x_plain_fp64_single_rhs"] = float(ks.sum()) / span / single
+        # accuracy: every factor once, b = L x_true, served mixed vs x_true
+        import scipy.sparse as sp
+        worst = 0.0
+        for i, (rp, ci, va) in enumerate(facs):
+            xt = rbs.gen_uniform(13000 + i, ns[i])
+            b = torch.tensor(sp.csr_matrix((va, ci, rp), shape=(ns[i], ns[i])) @ xt, device=dev)
+            x = torch.empty_like(b)
+            srv.wait(srv.submit_device(fids[i], b, x, k=1, prec=rbs.PREC_MIXED))
+            worst = max(worst, rel(x.cpu().numpy(), xt))
+        res["max_rel_err_vs_x_true"] = worst
+    finally:
+        sys.setswitchinterval(old_si)
+        srv.close()
     return res
 
 
@@ -882,6 +923,11 @@ def run_ours(args):
         "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
         "rel_err_vs_x_true": rel,
         "roofline": roofline,
+        # the single right-hand side is bounded by its dependency chain: every
+        # one of the global levels needs the previous level's results
+        "latency_floor": {"levels": info.nlevel, "us_per_level": 1000.0 * ms_per_step / max(info.nlevel, 1),
+                          "hbm_time_us": useful / (peak * 1e9) * 1e6,
+                          "note": "time per solve / global levels, against the HBM time of the useful bytes"},
         "e2e": {"value": world * args.steps / e2e_total, "unit": "solves/s", "h2d_bytes_per_step": 8 * sysm["n"],
                 "d2h_bytes_per_step": 8 * sysm["n"], "rel_err_vs_x_true": e2e_rel,
                 "path": "rbs_solve_host (C ABI, pinned host arrays)"},
@@ -890,22 +936,8 @@ def run_ours(args):
         "analyse_ms": info.analyse_ms,
     }
 
-    # side measurements (other configurations) on a single GPU only: with
-    # N replicas they would repeat the same numbers N times
-    if not args.no_sweep and world == 1:
-        line["config3_multi_rhs_c1a"] = side_multi_rhs(plan, sysm, dev, flush, args)
-        del plan
-        line["sweep_config1"] = side_structures(dev, flush, args)
-        line["config2_mixed"] = side_mixed(dev, flush, args)
-        line["analysis_host_vs_device"] = side_analysis(dev, args)
-        line["ilu0_laplace2d_1024"] = side_ilu0(dev, args)
-        line["ic0_laplace2d_1024"] = side_ic0(dev, args)
-        line["mtx_ingest_laplace2d_1024"] = side_mtx(dev, args)
-    if not args.no_batch and world == 1:
-        line["config3_batched_512"] = side_batched(dev, args)
-    if not args.no_serve and world == 1:
-        line["config4_serving"] = side_serving(dev, args)
-
+    del plan
+    torch.cuda.empty_cache()
     if rank == 0 and world == 1:
         cname, cthreads, cfn, xo = cpu_best(sysm)
         times = cpu_timed(cfn, sysm["b"], budget_s=8.0, max_reps=200)
@@ -916,10 +948,67 @@ def run_ours(args):
                                           "thread(s), the fastest CPU configuration",
                                 "cpu": platform.processor() or "x86_64", "nproc": os.cpu_count()}
         line["rel_err_vs_oracle"] = float(np.linalg.norm(x - xo) / np.linalg.norm(xo))
+    # side measurements (other configurations) on a single GPU only (with N
+    # replicas they would repeat the same numbers N times), each in a process
+    # of its own: a failing section is recorded, it cannot void this line
+    if world == 1:
+        for name in side_list(args):
+            line[SIDE_KEYS[name]] = run_side(name, args)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+SIDE_KEYS = {"multi_rhs": "config3_multi_rhs_c1a", "structures": "sweep_config1", "mixed": "config2_mixed",
+             "analysis": "analysis_host_vs_device", "ilu0": "ilu0_laplace2d_1024", "ic0": "ic0_laplace2d_1024",
+             "mtx": "mtx_ingest_laplace2d_1024", "batched": "config3_batched_512", "serve": "config4_serving",
+             "blocks": "blocks"}
+SIDE_FUNCS = {"multi_rhs": "side_multi_rhs", "structures": "side_structures", "mixed": "side_mixed",
+              "analysis": "side_analysis", "ilu0": "side_ilu0", "ic0": "side_ic0", "mtx": "side_mtx",
+              "batched": "side_batched", "serve": "side_serving", "blocks": "side_blocks"}
+SIDE_DEFAULT = ["multi_rhs", "structures", "mixed", "batched", "serve", "analysis", "ilu0", "ic0", "mtx"]
+
+
+def side_list(args):
+    if args.no_extras:
+        return []
+    if args.sides is not None:
+        return [x for x in args.sides.split(",") if x]
+    out = list(SIDE_DEFAULT)
+    if args.no_sweep:
+        out = [x for x in out if x not in ("multi_rhs", "structures", "mixed", "analysis", "ilu0", "ic0", "mtx")]
+    if args.no_batch:
+        out.remove("batched")
+    if args.no_serve:
+        out.remove("serve")
+    return out
+
+
+def run_side(name, args, timeout=900):
+    """One side measurement in a child process (bench.py --side NAME): its
+    JSON, or {"error": ...} with the end of its output."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--side", name, "--steps", str(args.steps), "--warmup",
+           str(args.warmup), "--case", args.case]
+    t0 = time.perf_counter()
+    try:
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return {"error": f"timed out after {timeout} s"}
+    wall = time.perf_counter() - t0
+    if p.returncode != 0:
+        return {"error": f"exit {p.returncode}", "tail": (p.stderr or p.stdout)[-1500:], "wall_s": wall}
+    for ln in reversed(p.stdout.strip().splitlines()):
+        try:
+            d = json.loads(ln)
+        except ValueError:
+            continue
+        if isinstance(d, dict) and name in d:
+            out = d[name]
+            if isinstance(out, dict):
+                out["wall_s"] = wall
+            return out
+    return {"error": "no JSON line", "tail": p.stdout[-1500:], "wall_s": wall}
 
 
 def side_blocks(dev, args):
@@ -951,16 +1040,11 @@ def side_blocks(dev, args):
     return out
 
 
-# side measurements that take (device, args) and can run alone (--side)
-SIDE_SECTIONS = {"mtx": "side_mtx", "ic0": "side_ic0", "ilu0": "side_ilu0", "analysis": "side_analysis",
-                 "batched": "side_batched", "serve": "side_serving", "blocks": "side_blocks"}
-
-
 def main():
     args = parse()
     if args.side:
         import torch
-        print(json.dumps({args.side: globals()[SIDE_SECTIONS[args.side]](torch.device("cuda:0"), args)}))
+        print(json.dumps({args.side: globals()[SIDE_FUNCS[args.side]](torch.device("cuda:0"), args)}))
         return
     if args.impl == "reference":
         run_reference(args)

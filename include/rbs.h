@@ -132,6 +132,10 @@ int rbs_plan_sync(rbs_plan *plan);
 
 /* cudaStream_t passed as void* (NULL = the plan's own stream). */
 int rbs_plan_set_stream(rbs_plan *plan, void *stream);
+/* Allocate the plan's work vectors for k (1..128) right-hand sides now, so
+ * later solves of up to k columns allocate and free no device memory (no
+ * counterpart in the reference, which allocates inside its solver). */
+int rbs_plan_reserve(rbs_plan *plan, int k);
 int rbs_plan_info_get(const rbs_plan *plan, rbs_plan_info *info);
 
 /* Many independent systems as one plan (no counterpart in the reference,
@@ -148,14 +152,20 @@ int rbs_batch_analyse(int count, const int *const *ptr, const int *const *idx, c
                       rbs_plan **plan, int *row_offsets);
 
 /* ---- request serving (no counterpart in the reference) ----------------
- * A server keeps analysed factors resident on the device and runs one
- * worker thread and CUDA stream per factor.  Submitted requests (host b and
- * x, column-major n x k, a precision) queue per factor; a worker takes all
- * queued requests of one precision that fit its batch width and solves
- * them as ONE multi-RHS solve, so requests arriving while a batch runs join
- * the next batch, while other factors run concurrently on their streams.
- * A factor is admitted only if its plan plus workspace fit the remaining
- * HBM budget (RBS_ERR_BUDGET otherwise). */
+ * A server keeps analysed factors resident on the device (each with its own
+ * CUDA stream and work vectors reserved at admission for the batch width,
+ * so serving allocates no device memory per solve).  Submitted requests
+ * (column-major n x k b and x, host arrays or device arrays, a precision)
+ * queue per factor.  One dispatcher thread issues all device work: a factor
+ * that is idle takes every queued request of one precision that fits the
+ * batch width and solves them as ONE multi-RHS solve, reading device
+ * requests' columns in place; requests arriving meanwhile join its next
+ * batch, and the batches of all factors overlap on the device (mixed
+ * precision refines each factor's batch on its own schedule).  A factor is
+ * admitted only if its plan plus work vectors fit the remaining HBM budget;
+ * a factor's first host-array request also charges its host staging
+ * (RBS_ERR_BUDGET otherwise).  All factors must live on the device that was
+ * current when the server was created. */
 typedef struct rbs_server rbs_server;
 typedef struct rbs_server_stats {
     long long completed;    /* requests finished since the last reset */
@@ -174,6 +184,10 @@ int rbs_server_add_factor(rbs_server *server, rbs_plan *plan, int *factor_id);
 /* b and x must stay valid until rbs_server_wait returns for the ticket. */
 int rbs_server_submit(rbs_server *server, int factor_id, const double *b, double *x, int k, int prec,
                       long long *ticket);
+/* The same with DEVICE arrays (leading dimension n), read and written in
+ * place by the batch's kernels; they must stay valid until the wait. */
+int rbs_server_submit_device(rbs_server *server, int factor_id, const double *d_b, double *d_x, int k, int prec,
+                             long long *ticket);
 int rbs_server_wait(rbs_server *server, long long ticket, double *latency_ms, int *batch_rhs);
 int rbs_server_stats_get(rbs_server *server, rbs_server_stats *stats);
 int rbs_server_reset_stats(rbs_server *server);

@@ -150,6 +150,14 @@ void orc_free(void *p);
 int orc_tri_extract(int m, const int *rowptr, const int *colidx, const double *val, int substitution,
                     const double *strict_val, int *trowptr, int *tcolidx, double *tval);
 
+/* gen.c: the seeded systems of include/rbs_gen.h (kind: 0 band Poisson,
+ * 1 2D Laplacian, 2 Zipf, 3 chain, 4 diagonal), restated so that CPU-side
+ * inputs need no GPU library; arrays from malloc (free with orc_free). */
+int orc_gen_lower_csr(int kind, int n, int grid, double lambda, int band, double zipf_alpha, int zipf_max,
+                      int chain_bw, unsigned long long seed, int *n_out, long long *nnz_out, int **rowptr,
+                      int **colidx, double **val);
+int orc_gen_uniform(unsigned long long seed, long long n, double lo, double hi, double *out);
+
 #ifdef __cplusplus
 }
 #endif

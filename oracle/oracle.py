@@ -330,3 +330,38 @@ def reference_mtx_ms(path):
         return None
     out = subprocess.run([MTX_REF_DUMP, "--time", path], check=True, capture_output=True, text=True).stdout
     return float(out.strip())
+
+
+lib.orc_gen_lower_csr.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                  ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
+                                  _ip, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_ip), ctypes.POINTER(_ip),
+                                  ctypes.POINTER(_dp)]
+lib.orc_gen_uniform.argtypes = [ctypes.c_ulonglong, ctypes.c_longlong, ctypes.c_double, ctypes.c_double, _dp]
+
+GEN_BAND_POISSON, GEN_LAPLACE2D, GEN_ZIPF, GEN_CHAIN, GEN_DIAG = range(5)
+
+
+def gen_lower_csr(kind, n=0, grid=0, lam=0.0, band=0, zipf_alpha=0.0, zipf_max=0, chain_bw=0, seed=0):
+    """The seeded lower-triangular CSR of include/rbs_gen.h (columns ascending, diagonal last)."""
+    nn = ctypes.c_int()
+    nnz = ctypes.c_longlong()
+    rp, ci, va = _ip(), _ip(), _dp()
+    rc = lib.orc_gen_lower_csr(kind, n, grid, lam, band, zipf_alpha, zipf_max, chain_bw, seed, ctypes.byref(nn),
+                               ctypes.byref(nnz), ctypes.byref(rp), ctypes.byref(ci), ctypes.byref(va))
+    if rc:
+        raise RuntimeError(f"orc_gen_lower_csr failed ({rc})")
+    try:
+        n_, z = nn.value, nnz.value
+        return (np.ctypeslib.as_array(rp, shape=(n_ + 1,)).copy(),
+                np.ctypeslib.as_array(ci, shape=(max(z, 1),))[:z].copy(),
+                np.ctypeslib.as_array(va, shape=(max(z, 1),))[:z].copy())
+    finally:
+        for p in (rp, ci, va):
+            lib.orc_free(p)
+
+
+def gen_uniform(seed, n, lo=-1.0, hi=1.0):
+    out = np.empty(n, dtype=np.float64)
+    if lib.orc_gen_uniform(seed, n, lo, hi, out.ctypes.data_as(_dp)):
+        raise RuntimeError("orc_gen_uniform failed")
+    return out

@@ -11,10 +11,6 @@
 #include "rbs.h"
 #include "rbs_internal.h"
 
-struct rbs_plan {
-    rbs::Plan p;
-};
-
 namespace rbs {
 namespace {
 thread_local std::string g_error;
@@ -264,6 +260,14 @@ int rbs_plan_set_stream(rbs_plan *plan, void *stream) {
     std::string err;
     int rc = rbs::device_set_stream(plan->p, stream, err);
     if (rc) return fail(rc, err);
+    return RBS_OK;
+}
+
+int rbs_plan_reserve(rbs_plan *plan, int k) {
+    if (!plan) return fail(RBS_ERR_ARG, "rbs_plan_reserve: plan is NULL");
+    std::string err;
+    int rc = rbs::device_reserve(plan->p, k, err);
+    if (rc) return fail(rc, "rbs_plan_reserve: " + err);
     return RBS_OK;
 }
 

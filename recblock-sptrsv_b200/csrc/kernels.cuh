@@ -108,6 +108,34 @@ __global__ void k_scatter_reset(VT *__restrict__ xw, const int *__restrict__ per
     }
 }
 
+// The same from a table of column pointers (one device pointer per
+// right-hand side, e.g. the columns of several requests batched together):
+// out[p*K + c] = cols[c][perm[p]], 0 for c >= k.
+template <typename VT, int K>
+__global__ void k_gather_cols(const double *const *__restrict__ cols, int k, const int *__restrict__ perm, int n,
+                              VT *__restrict__ out) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)n * K;
+    for (; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int p = (int)(t / K), c = (int)(t % K);
+        out[t] = c < k ? (VT)cols[c][perm[p]] : VT(0);
+    }
+}
+
+// cols[c][perm[p]] = xw[p*K + c] for c < k; xw reset to the sentinel.
+template <typename VT, int K>
+__global__ void k_scatter_cols(VT *__restrict__ xw, const int *__restrict__ perm, int n, int k,
+                               double *const *__restrict__ cols) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)n * K;
+    for (; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int p = (int)(t / K), c = (int)(t % K);
+        const VT v = xw[t];
+        if (c < k) cols[c][perm[p]] = (double)v;
+        xw[t] = Sent<VT>::value();
+    }
+}
+
 template <typename VT>
 __global__ void k_fill(VT *__restrict__ v, long long count, VT value) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -472,6 +500,18 @@ __global__ void k_scatter64(const double *__restrict__ x64, const int *__restric
     for (; t < total; t += (long long)gridDim.x * blockDim.x) {
         int p = (int)(t / K), c = (int)(t % K);
         if (c < k) x[(long long)c * ld + perm[p]] = x64[t];
+    }
+}
+
+// cols[c][perm[p]] = x64[p*K + c] for c < k (column-pointer table form)
+template <int K>
+__global__ void k_scatter64_cols(const double *__restrict__ x64, const int *__restrict__ perm, int n, int k,
+                                 double *const *__restrict__ cols) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)n * K;
+    for (; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int p = (int)(t / K), c = (int)(t % K);
+        if (c < k) cols[c][perm[p]] = x64[t];
     }
 }
 

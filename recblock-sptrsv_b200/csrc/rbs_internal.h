@@ -298,9 +298,26 @@ int device_profile(Plan &P, int enable, std::string &err);
 int device_tune(Plan &P, std::string &err);
 int device_block_times(const Plan &P, std::vector<double> &ms, long long &solves);
 int device_staging(Plan &P, size_t bytes, double *&db, double *&dx, std::string &err);
+// work vectors for k right-hand sides allocated now, so solves up to that
+// width allocate nothing
+int device_reserve(Plan &P, int k, std::string &err);
+// Asynchronous solve of k columns on the plan's stream: bcols / xcols are
+// device tables of k column pointers (right-hand sides read, solutions
+// written).  After start, and after every next that sets *more, the caller
+// waits for the stream and calls next again while *more is set (mixed
+// refinement: one correction per call); then finish reports the status.
+int device_batch_start(Plan &P, const double *const *bcols, double *const *xcols, int k, int prec, int *more,
+                       std::string &err);
+int device_batch_next(Plan &P, int *more, std::string &err);
+int device_batch_finish(Plan &P, int *iters, double *corr, std::string &err);
 double block_bytes(const Plan &P, const ExecBlock &B);
 long long device_bytes(const Plan &P);
 
 void set_error(const std::string &msg);
 
 }  // namespace rbs
+
+// the opaque handle of include/rbs.h
+struct rbs_plan {
+    rbs::Plan p;
+};

@@ -83,6 +83,10 @@ struct DeviceState {
     size_t stage_bytes = 0;
     int last_iters = 0;
     double last_corr = 0;
+    // the asynchronous batch in flight (device_batch_*)
+    int bat_K = 0, bat_k = 0, bat_prec = 0, bat_iters = 0;
+    double bat_corr = 0;
+    double *const *bat_xcols = nullptr;
     // captured block walks per (precision, K, profiling)
     bool use_graphs = true;
     std::map<long long, cudaGraphExec_t> graphs;
@@ -164,32 +168,54 @@ void free_work(DeviceState &D) {
 
 void drop_graphs_fwd(DeviceState &D);
 
+float sent32_host() {
+    unsigned bits = RBS_SENT32;
+    float v;
+    std::memcpy(&v, &bits, 4);
+    return v;
+}
+
 // Work vectors sized for K right-hand sides; solution vectors start filled
-// with the sentinel and every solve leaves them that way.
+// with the sentinel and every solve leaves them that way.  Growing frees the
+// old vectors and every captured block walk that points into them; if an
+// allocation fails, the plan is left with no work vectors at all (kcap 0),
+// so the next solve allocates again instead of running on freed memory.
 int ensure_work(Plan &P, int K, std::string &err) {
     DeviceState &D = *P.dev;
     if (K <= D.kcap) return RBS_OK;
+    // the old vectors may still be read by work queued on the stream
+    CK(cudaStreamSynchronize(D.stream));
     drop_graphs_fwd(D);
     free_work(D);
     D.bytes -= D.work_bytes;
+    D.work_bytes = 0;
+    D.kcap = 0;
     const long long before = D.bytes;
-    size_t cnt = (size_t)P.n * K;
+    const size_t cnt = (size_t)P.n * K;
+    auto undo = [&](int rc) {
+        free_work(D);
+        D.bytes = before;
+        return rc;
+    };
     int rc;
-    if ((rc = alloc(D, D.bw64, cnt, err))) return rc;
-    if ((rc = alloc(D, D.xw64, cnt, err))) return rc;
-    k_fill<double><<<grid_for((long long)cnt, 256, D.num_sms), 256, 0, D.stream>>>(
-        D.xw64, (long long)cnt, sent64_host());
+    if ((rc = alloc(D, D.bw64, cnt, err))) return undo(rc);
+    if ((rc = alloc(D, D.xw64, cnt, err))) return undo(rc);
     if (D.mixed) {
-        if ((rc = alloc(D, D.b64keep, cnt, err))) return rc;
-        if ((rc = alloc(D, D.x64acc, cnt, err))) return rc;
-        if ((rc = alloc(D, D.bw32, cnt, err))) return rc;
-        if ((rc = alloc(D, D.xw32, cnt, err))) return rc;
-        unsigned s32 = RBS_SENT32;
-        float f32;
-        std::memcpy(&f32, &s32, 4);
-        k_fill<float><<<grid_for((long long)cnt, 256, D.num_sms), 256, 0, D.stream>>>(D.xw32, (long long)cnt, f32);
+        if ((rc = alloc(D, D.b64keep, cnt, err))) return undo(rc);
+        if ((rc = alloc(D, D.x64acc, cnt, err))) return undo(rc);
+        if ((rc = alloc(D, D.bw32, cnt, err))) return undo(rc);
+        if ((rc = alloc(D, D.xw32, cnt, err))) return undo(rc);
     }
-    CK(cudaGetLastError());
+    k_fill<double><<<grid_for((long long)cnt, 256, D.num_sms), 256, 0, D.stream>>>(D.xw64, (long long)cnt,
+                                                                                    sent64_host());
+    if (D.mixed)
+        k_fill<float><<<grid_for((long long)cnt, 256, D.num_sms), 256, 0, D.stream>>>(D.xw32, (long long)cnt,
+                                                                                       sent32_host());
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        err = std::string("ensure_work: ") + cudaGetErrorString(e);
+        return undo(RBS_ERR_CUDA);
+    }
     D.kcap = K;
     D.work_bytes = D.bytes - before;
     return RBS_OK;
@@ -656,6 +682,48 @@ int solve_fp32(Plan &P, const double *b, double *x, int k, int ld, std::string &
 // FP32 sweeps with FP64 residuals and FP64 accumulation:
 //   x0 = L32^-1 b;  repeat  r = b - L x (FP64),  d = L32^-1 r,  x += d
 // until ||d||/||x|| <= ir_tol for every right-hand side.
+//
+// mixed_first: x0 = L32^-1 b (b already gathered into b64keep and bw32).
+template <int K>
+int mixed_first(Plan &P, std::string &err) {
+    DeviceState &D = *P.dev;
+    int rc = run_blocks<float, K>(P, err);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(D.norms, 0, sizeof(double) * 2 * K, D.stream));
+    k_update<K><<<grid_for((long long)P.n * K, 256, D.num_sms), 256, 0, D.stream>>>(D.x64acc, D.xw32, P.n, 1,
+                                                                                      D.norms);
+    return RBS_OK;
+}
+
+// mixed_step: one correction r = b - L x, d = L32^-1 r, x += d, with the
+// per-column sums of squares of d and x copied to the host (h_norms).
+template <int K>
+int mixed_step(Plan &P, std::string &err) {
+    DeviceState &D = *P.dev;
+    const int n = P.n;
+    const int G = P.nnz / std::max(1, n) < 6 ? 4 : 8;
+    k_residual<K><<<grid_for((long long)n * (K == 1 ? G : std::min(K, 32)), 256, D.num_sms), 256, 0, D.stream>>>(
+        D.full_rp, D.full_col, D.full_val, D.x64acc, D.b64keep, D.bw32, n, G);
+    int rc = run_blocks<float, K>(P, err);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(D.norms, 0, sizeof(double) * 2 * K, D.stream));
+    k_update<K><<<grid_for((long long)n * K, 256, D.num_sms), 256, 0, D.stream>>>(D.x64acc, D.xw32, n, 0, D.norms);
+    CK(cudaMemcpyAsync(D.h_norms, D.norms, sizeof(double) * 2 * K, cudaMemcpyDeviceToHost, D.stream));
+    return RBS_OK;
+}
+
+// Largest ||d||/||x|| over the first k columns of the last step's norms
+// (NaN propagates).
+double mixed_correction(const DeviceState &D, int K, int k) {
+    double corr = 0;
+    for (int c = 0; c < k; ++c) {
+        const double dn = std::sqrt(D.h_norms[c]), xn = std::sqrt(D.h_norms[K + c]);
+        const double r = xn > 0 ? dn / xn : dn;
+        if (!(r <= corr)) corr = r;
+    }
+    return corr;
+}
+
 template <int K>
 int solve_mixed(Plan &P, const double *b, double *x, int k, int ld, int &iters, double &corr, std::string &err) {
     DeviceState &D = *P.dev;
@@ -663,30 +731,15 @@ int solve_mixed(Plan &P, const double *b, double *x, int k, int ld, int &iters, 
     const int grid = grid_for((long long)n * K, 256, D.num_sms);
     k_gather<double, K><<<grid, 256, 0, D.stream>>>(b, ld, k, D.perm, n, D.b64keep);
     k_gather<float, K><<<grid, 256, 0, D.stream>>>(b, ld, k, D.perm, n, D.bw32);
-    int rc = run_blocks<float, K>(P, err);
+    int rc = mixed_first<K>(P, err);
     if (rc) return rc;
-    CK(cudaMemsetAsync(D.norms, 0, sizeof(double) * 2 * K, D.stream));
-    k_update<K><<<grid_for((long long)n * K, 256, D.num_sms), 256, 0, D.stream>>>(D.x64acc, D.xw32, n, 1, D.norms);
-    const int G = P.nnz / std::max(1, n) < 6 ? 4 : 8;
     iters = 0;
     corr = 1.0;
     for (int it = 0; it < P.opt.ir_max_iter; ++it) {
-        k_residual<K><<<grid_for((long long)n * (K == 1 ? G : std::min(K, 32)), 256, D.num_sms), 256, 0, D.stream>>>(
-            D.full_rp, D.full_col, D.full_val, D.x64acc, D.b64keep, D.bw32, n, G);
-        rc = run_blocks<float, K>(P, err);
-        if (rc) return rc;
-        CK(cudaMemsetAsync(D.norms, 0, sizeof(double) * 2 * K, D.stream));
-        k_update<K><<<grid_for((long long)n * K, 256, D.num_sms), 256, 0, D.stream>>>(D.x64acc, D.xw32, n, 0,
-                                                                                        D.norms);
-        CK(cudaMemcpyAsync(D.h_norms, D.norms, sizeof(double) * 2 * K, cudaMemcpyDeviceToHost, D.stream));
+        if ((rc = mixed_step<K>(P, err))) return rc;
         CK(cudaStreamSynchronize(D.stream));
         ++iters;
-        corr = 0;
-        for (int c = 0; c < k; ++c) {
-            double dn = std::sqrt(D.h_norms[c]), xn = std::sqrt(D.h_norms[K + c]);
-            double r = xn > 0 ? dn / xn : dn;
-            if (!(r <= corr)) corr = r;  // NaN-propagating max
-        }
+        corr = mixed_correction(D, K, k);
         if (corr <= P.opt.ir_tol) break;
     }
     k_scatter64<K><<<grid, 256, 0, D.stream>>>(D.x64acc, D.perm, n, k, x, ld);
@@ -697,6 +750,131 @@ int solve_mixed(Plan &P, const double *b, double *x, int k, int ld, int &iters, 
     }
     return RBS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Asynchronous batches for the request server: the right-hand sides and the
+// solutions are given as device tables of column pointers (the columns of
+// several requests side by side).  Nothing here waits for the device; the
+// caller drains the plan's stream between the phases (an event), so one
+// host thread can keep many plans' solves in flight.
+// ---------------------------------------------------------------------------
+#define RBS_FOR_K(K, EXPR)                                   \
+    switch (K) {                                             \
+    case 1: { constexpr int KC = 1; EXPR; } break;           \
+    case 2: { constexpr int KC = 2; EXPR; } break;           \
+    case 4: { constexpr int KC = 4; EXPR; } break;           \
+    case 8: { constexpr int KC = 8; EXPR; } break;           \
+    case 16: { constexpr int KC = 16; EXPR; } break;         \
+    case 32: { constexpr int KC = 32; EXPR; } break;         \
+    case 64: { constexpr int KC = 64; EXPR; } break;         \
+    default: { constexpr int KC = 128; EXPR; } break;        \
+    }
+
+template <int K>
+int batch_start_k(Plan &P, const double *const *bcols, double *const *xcols, int k, int prec, std::string &err) {
+    DeviceState &D = *P.dev;
+    const int n = P.n;
+    const int grid = grid_for((long long)n * K, 256, D.num_sms);
+    int rc;
+    if (prec == RBS_PREC_FP64) {
+        k_gather_cols<double, K><<<grid, 256, 0, D.stream>>>(bcols, k, D.perm, n, D.bw64);
+        if ((rc = run_blocks<double, K>(P, err))) return rc;
+        k_scatter_cols<double, K><<<grid, 256, 0, D.stream>>>(D.xw64, D.perm, n, k, xcols);
+    } else if (prec == RBS_PREC_FP32) {
+        k_gather_cols<float, K><<<grid, 256, 0, D.stream>>>(bcols, k, D.perm, n, D.bw32);
+        if ((rc = run_blocks<float, K>(P, err))) return rc;
+        k_scatter_cols<float, K><<<grid, 256, 0, D.stream>>>(D.xw32, D.perm, n, k, xcols);
+    } else {
+        k_gather_cols<double, K><<<grid, 256, 0, D.stream>>>(bcols, k, D.perm, n, D.b64keep);
+        k_gather_cols<float, K><<<grid, 256, 0, D.stream>>>(bcols, k, D.perm, n, D.bw32);
+        if ((rc = mixed_first<K>(P, err))) return rc;
+        if ((rc = mixed_step<K>(P, err))) return rc;
+    }
+    CK(cudaGetLastError());
+    return RBS_OK;
+}
+
+template <int K>
+int batch_end_k(Plan &P, double *const *xcols, int k, std::string &err) {
+    DeviceState &D = *P.dev;
+    k_scatter64_cols<K><<<grid_for((long long)P.n * K, 256, D.num_sms), 256, 0, D.stream>>>(D.x64acc, D.perm, P.n,
+                                                                                          k, xcols);
+    CK(cudaGetLastError());
+    return RBS_OK;
+}
+
+}  // namespace
+
+int device_reserve(Plan &P, int k, std::string &err) {
+    if (!P.dev) {
+        err = "plan has no device state";
+        return RBS_ERR_ARG;
+    }
+    if (k < 1 || k > 128) {
+        err = "reserve: k must be in [1, 128]";
+        return RBS_ERR_ARG;
+    }
+    int rc = ensure_work(P, pow2_at_least(k), err);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(P.dev->stream));
+    return RBS_OK;
+}
+
+int device_batch_start(Plan &P, const double *const *bcols, double *const *xcols, int k, int prec, int *more,
+                       std::string &err) {
+    DeviceState &D = *P.dev;
+    if (k < 1 || k > 128 || (prec != RBS_PREC_FP64 && !D.mixed)) {
+        err = "batch: k must be in [1, 128]; FP32 and mixed batches need a plan with FP32 copies";
+        return RBS_ERR_ARG;
+    }
+    const int K = pow2_at_least(k);
+    int rc = ensure_work(P, K, err);
+    if (rc) return rc;
+    D.bat_K = K;
+    D.bat_k = k;
+    D.bat_prec = prec;
+    D.bat_iters = 0;
+    D.bat_corr = 0;
+    D.bat_xcols = xcols;
+    RBS_FOR_K(K, rc = batch_start_k<KC>(P, bcols, xcols, k, prec, err));
+    if (rc) return rc;
+    *more = prec == RBS_PREC_MIXED ? 1 : 0;
+    if (!*more) CK(cudaMemcpyAsync(D.h_status, D.status, sizeof(int), cudaMemcpyDeviceToHost, D.stream));
+    return RBS_OK;
+}
+
+int device_batch_next(Plan &P, int *more, std::string &err) {
+    DeviceState &D = *P.dev;
+    const int K = D.bat_K;
+    ++D.bat_iters;
+    D.bat_corr = mixed_correction(D, K, D.bat_k);
+    int rc = RBS_OK;
+    if (D.bat_corr <= P.opt.ir_tol || D.bat_iters >= P.opt.ir_max_iter) {
+        RBS_FOR_K(K, rc = batch_end_k<KC>(P, D.bat_xcols, D.bat_k, err));
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(D.h_status, D.status, sizeof(int), cudaMemcpyDeviceToHost, D.stream));
+        *more = 0;
+        return RBS_OK;
+    }
+    RBS_FOR_K(K, rc = mixed_step<KC>(P, err));
+    if (rc) return rc;
+    *more = 1;
+    return RBS_OK;
+}
+
+int device_batch_finish(Plan &P, int *iters, double *corr, std::string &err) {
+    DeviceState &D = *P.dev;
+    if (iters) *iters = D.bat_iters;
+    if (corr) *corr = D.bat_corr;
+    if (*D.h_status & RBS_STATUS_TIMEOUT) return device_sync(P, err);  // resets the status and the work vectors
+    if (D.bat_prec == RBS_PREC_MIXED && !(D.bat_corr <= P.opt.ir_tol)) {
+        err = "mixed-precision refinement stopped at ||dx||/||x|| = " + std::to_string(D.bat_corr);
+        return RBS_ERR_NOCONV;
+    }
+    return RBS_OK;
+}
+
+namespace {
 
 template <int K>
 int solve_k(Plan &P, const double *b, double *x, int k, int ld, int prec, int &iters, double &corr,
@@ -1005,10 +1183,14 @@ int device_sync(Plan &P, std::string &err) {
     CK(cudaStreamSynchronize(D.stream));
     if (*D.h_status & RBS_STATUS_TIMEOUT) {
         CK(cudaMemsetAsync(D.status, 0, sizeof(int), D.stream));
-        // the solution work vector may hold leftovers of the aborted solve
+        // the solution work vectors may hold leftovers of the aborted solve
         size_t cnt = (size_t)P.n * D.kcap;
-        k_fill<double><<<grid_for((long long)cnt, 256, D.num_sms), 256, 0, D.stream>>>(
-            D.xw64, (long long)cnt, sent64_host());
+        if (D.xw64)
+            k_fill<double><<<grid_for((long long)cnt, 256, D.num_sms), 256, 0, D.stream>>>(
+                D.xw64, (long long)cnt, sent64_host());
+        if (D.xw32)
+            k_fill<float><<<grid_for((long long)cnt, 256, D.num_sms), 256, 0, D.stream>>>(
+                D.xw32, (long long)cnt, sent32_host());
         CK(cudaStreamSynchronize(D.stream));
         err = "a device wait exceeded its poll budget (dependency never produced)";
         return RBS_ERR_TIMEOUT;

@@ -108,9 +108,9 @@ EXPORTS = [
     "rbs_plan_free", "rbs_last_error", "rbs_auto_lv", "recblocking_solver_cuda", "recblocking_solver",
     "rbs_gen_lower_csr", "rbs_gen_uniform", "rbs_gen_free", "rbs_plan_profile", "rbs_plan_block_times",
     "rbs_sptrsv_csr_noalloc", "rbs_batch_analyse", "rbs_server_create", "rbs_server_add_factor",
-    "rbs_server_submit", "rbs_server_wait", "rbs_server_stats_get", "rbs_server_reset_stats", "rbs_server_destroy",
+    "rbs_server_submit", "rbs_server_submit_device", "rbs_server_wait", "rbs_server_stats_get", "rbs_server_reset_stats", "rbs_server_destroy",
     "rbs_plan_save", "rbs_plan_load", "rbs_ilu0_device", "rbs_mtx_read", "rbs_mtx_read_buffer", "rbs_mtx_info_get",
-    "rbs_mtx_csr", "rbs_mtx_triangle", "rbs_mtx_free", "rbs_mtx_write", "rbs_ic0_device",
+    "rbs_mtx_csr", "rbs_mtx_triangle", "rbs_mtx_free", "rbs_mtx_write", "rbs_ic0_device", "rbs_plan_reserve",
 ]
 
 MTX_REAL, MTX_INTEGER, MTX_PATTERN, MTX_COMPLEX = range(4)
@@ -179,6 +179,9 @@ def _load():
     lib.rbs_server_add_factor.argtypes = [P, P, ip]
     lib.rbs_server_submit.argtypes = [P, ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_longlong)]
+    lib.rbs_server_submit_device.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_longlong)]
+    lib.rbs_plan_reserve.argtypes = [P, ctypes.c_int]
     lib.rbs_server_wait.argtypes = [P, ctypes.c_longlong, dp, ip]
     lib.rbs_server_stats_get.argtypes = [P, ctypes.POINTER(ServerStats)]
     lib.rbs_server_reset_stats.argtypes = [P]
@@ -298,6 +301,10 @@ class Plan:
         """rbs_plan_save: the analysis to a file."""
         _check(lib.rbs_plan_save(self._h, str(path).encode()))
 
+    def reserve(self, k: int):
+        """Work vectors for k right-hand sides now (no allocation in later solves up to k)."""
+        _check(lib.rbs_plan_reserve(self._h, k))
+
     def set_stream(self, stream_ptr: int | None):
         _check(lib.rbs_plan_set_stream(self._h, ctypes.c_void_p(stream_ptr) if stream_ptr else None))
 
@@ -345,6 +352,15 @@ class Server:
         _check(lib.rbs_server_add_factor(self._h, plan.handle, ctypes.byref(fid)))
         plan._h = None  # owned by the server now
         return fid.value
+
+    def submit_device(self, factor: int, b, x, k: int = 1, prec: int = PREC_FP64) -> int:
+        """Device arrays (torch CUDA tensors, float64, n*k elements, column-major), read and
+        written in place; kept alive here until the wait."""
+        t = ctypes.c_longlong()
+        _check(lib.rbs_server_submit_device(self._h, factor, ctypes.c_void_p(b.data_ptr()),
+                                            ctypes.c_void_p(x.data_ptr()), k, prec, ctypes.byref(t)))
+        self._keep[t.value] = (b, x)
+        return t.value
 
     def submit(self, factor: int, b: np.ndarray, x: np.ndarray, k: int = 1, prec: int = PREC_FP64) -> int:
         assert b.dtype == np.float64 and x.dtype == np.float64 and b.flags.c_contiguous and x.flags.c_contiguous

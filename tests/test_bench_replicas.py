@@ -77,3 +77,20 @@ def test_reference_arm_line_on_rank0():
     assert line["e2e"] == {"value": line["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
     assert line["rel_err_vs_x_true"] <= 1e-12
+
+
+def test_reference_arm_loads_no_library_under_test():
+    # the CPU arm builds its inputs with the oracle's generator and solves
+    # with the oracle: the only shared object of this repository it maps is
+    # oracle/liboracle.so, never recblock-sptrsv_b200/librbs.so
+    import subprocess
+    code = ("import runpy, sys\n"
+            "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0']\n"
+            "runpy.run_path('bench.py', run_name='__main__')\n"
+            "maps = open('/proc/self/maps').read().split()\n"
+            "print('MAPPED', sorted({w for w in maps if w.endswith('.so') and w.startswith(%r)}))\n" % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT,
+                         env=dict(os.environ, RANK="0"))
+    assert out.returncode == 0, out.stderr[-2000:]
+    mapped = eval(out.stdout.strip().splitlines()[-1].split(" ", 1)[1])
+    assert mapped == [os.path.join(ROOT, "oracle", "liboracle.so")], mapped
