@@ -1237,6 +1237,157 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
     return RBS_OK;
 }
 
+// The reference-format packing of recblocking_preprocess.h:298-967 (see
+// export_reference): the level-permuted CSC, every block cut out with the
+// reference's bounds filter and packed into recblock_Ptr/Index/Val and the
+// DCSR row lists, local level sets of the triangles.
+static int build_ref_pack(const Plan &P, bool fwd, const std::vector<int> &blk_m, const std::vector<int> &blk_n,
+                          const std::vector<int> &blk_nnz, const std::vector<int> &stu, const std::vector<int> &std_,
+                          const std::vector<int> &sru, const std::vector<int> &srd, const std::vector<int> &srl,
+                          const std::vector<int> &srr, const std::vector<int> &method, RefPack &R,
+                          std::string &err) {
+    const int n = P.n, nnz = P.nnz, sum = P.sum_block;
+    std::vector<int> cp_new((size_t)n + 1), ri_new((size_t)nnz);
+    std::vector<double> va_new((size_t)nnz);
+    cp_new[0] = 0;
+    for (int i = 0; i < n; ++i) {
+        int src = fwd ? P.bfs_item[i] : P.bfs_item[n - 1 - i];
+        int len = P.in_cp[src + 1] - P.in_cp[src];
+        cp_new[i + 1] = cp_new[i] + len;
+        for (int j = 0; j < len; ++j) {
+            ri_new[cp_new[i] + j] = P.label[P.in_ri[P.in_cp[src] + j]];
+            va_new[cp_new[i] + j] = P.in_va[P.in_cp[src] + j];
+        }
+    }
+    auto &ptr_offset = R.ptr_offset, &index_offset = R.index_offset, &dcsr_offset = R.dcsr_offset;
+    ptr_offset.assign(sum + 1, 0);
+    index_offset.assign(sum + 1, 0);
+    dcsr_offset.assign(sum + 1, 0);
+    int ps = 1, is = 0, ds = 0;
+    for (int b = 0; b < sum; ++b) {
+        if ((b & 1) == 0) { ps += blk_n[b] + 1; is += blk_nnz[b]; }
+        else { ps += blk_m[b]; is += blk_nnz[b]; ds += blk_m[b]; }
+    }
+    auto &Ptr = R.Ptr, &Index = R.Index, &Dcsr = R.Dcsr;
+    auto &Val = R.Val;
+    auto &nlv = R.nlv, &longrow = R.longrow, &m_new_dcsr = R.m_new_dcsr;
+    auto &lvl_ptr = R.lvl_ptr, &lvl_item = R.lvl_item, &m_lv = R.m_lv, &off_lv = R.off_lv, &nnz_lv = R.nnz_lv;
+    Ptr.assign((size_t)ps, 0);
+    Index.assign((size_t)std::max(is, 1), 0);
+    Dcsr.assign((size_t)std::max(ds, 1), 0);
+    Val.assign((size_t)std::max(is, 1), 0.0);
+    nlv.assign(sum, 0);
+    longrow.assign(sum, 0);
+    m_new_dcsr.assign(sum, -1);
+    ptr_offset[0] = 1;
+    index_offset[0] = 0;
+    dcsr_offset[0] = 0;
+    int nz = 0;
+    for (int b = 0; b < sum; ++b) {
+        const int bm = blk_m[b], bn = blk_n[b];
+        int po = ptr_offset[b];
+        std::vector<int> scp((size_t)bn + 1, 0), sri;
+        std::vector<double> sva;
+        if ((b & 1) == 0) {
+            int up = stu[b], down = std_[b];
+            for (int c = up; c < down; ++c) {
+                for (int k = cp_new[c]; k < cp_new[c + 1]; ++k) {
+                    int r = ri_new[k];
+                    if (fwd ? r < down : r >= up) {
+                        sri.push_back(r - up);
+                        sva.push_back(va_new[k]);
+                    }
+                }
+                scp[(size_t)(c - up) + 1] = (int)sri.size();
+            }
+            std::vector<int> rrp, rci;
+            std::vector<double> rva;
+            transpose(bn, bm, scp.data(), sri.data(), sva.data(), rrp, rci, rva);
+            std::vector<int> lp, li;
+            int nl = 1;
+            if (bm == (int)sri.size()) {
+                lp = {0, bm};
+                li.resize((size_t)bm);
+                for (int i = 0; i < bm; ++i) li[i] = i;
+            } else {
+                nl = bfs_levels(scp.data(), sri.data(), bm, lp, li);
+                if (nl < 0) { err = "export: local level search stuck"; return RBS_ERR_STRUCTURE; }
+            }
+            nlv[b] = nl;
+            lvl_ptr.insert(lvl_ptr.end(), lp.begin(), lp.end());
+            lvl_item.insert(lvl_item.end(), li.begin(), li.end());
+            int meth = method[b];
+            if (meth == 0 || meth == 3) {
+                for (int i = 0; i < bn; ++i) {
+                    for (int k = scp[i]; k < scp[i + 1]; ++k) { Index[nz] = sri[k]; Val[nz] = sva[k]; ++nz; }
+                    Ptr[po + i] = Ptr[po + i - 1] + scp[i + 1] - scp[i];
+                }
+            } else if (meth == 2) {
+                for (int l = 0; l < nl; ++l) {
+                    m_lv.push_back(lp[l + 1] - lp[l]);
+                    off_lv.push_back(lp[l]);
+                    int sacc = 0;
+                    for (int q = lp[l]; q < lp[l + 1]; ++q) sacc += rrp[q + 1] - rrp[q];
+                    nnz_lv.push_back(sacc);
+                }
+                for (int i = 0; i < bm; ++i) {
+                    for (int k = rrp[i]; k < rrp[i + 1]; ++k) { Index[nz] = rci[k]; Val[nz] = rva[k]; ++nz; }
+                    Ptr[po + i] = Ptr[po + i - 1] + rrp[i + 1] - rrp[i];
+                }
+            } else {
+                Ptr[po] = 0;
+                int c = 0;
+                for (int i = 0; i < bm; ++i) {
+                    for (int k = rrp[i]; k < rrp[i + 1]; ++k) { Index[nz] = rci[k]; Val[nz] = rva[k]; ++nz; ++c; }
+                    Ptr[po + i + 1] = c;
+                }
+            }
+            ptr_offset[b + 1] = po + bm + (meth == 1 ? 1 : 0);
+            index_offset[b + 1] = nz;
+            dcsr_offset[b + 1] = dcsr_offset[b];
+        } else {
+            int up = sru[b], down = srd[b], left = srl[b], right = srr[b];
+            for (int c = left; c < right; ++c) {
+                for (int k = cp_new[c]; k < cp_new[c + 1]; ++k) {
+                    int r = ri_new[k];
+                    if (r >= up && r < down) {
+                        sri.push_back(r - up);
+                        sva.push_back(va_new[k]);
+                    }
+                }
+                scp[(size_t)(c - left) + 1] = (int)sri.size();
+            }
+            std::vector<int> rrp, rci;
+            std::vector<double> rva;
+            transpose(bn, bm, scp.data(), sri.data(), sva.data(), rrp, rci, rva);
+            for (int i = 0; i < bm; ++i)
+                for (int k = rrp[i]; k < rrp[i + 1]; ++k) { Index[nz] = rci[k]; Val[nz] = rva[k]; ++nz; }
+            int real_i = 0, dcsr_i = 0, meth = method[b];
+            int lr = 0;
+            for (int i = 0; i < bm; ++i)
+                if (rrp[i + 1] - rrp[i] > kLongRow) ++lr;
+            longrow[b] = meth >= 0 ? lr : 0;
+            if (meth == 0 || meth == 2) {
+                for (int i = 0; i < bm; ++i) Ptr[po + i] = Ptr[po + i - 1] + rrp[i + 1] - rrp[i];
+                real_i = bm;
+            } else if (meth == 1 || meth == 3) {
+                for (int i = 0; i < bm; ++i)
+                    if (rrp[i + 1] != rrp[i]) {
+                        Ptr[po + dcsr_i] = Ptr[po + dcsr_i - 1] + rrp[i + 1] - rrp[i];
+                        Dcsr[dcsr_offset[b] + dcsr_i] = i;
+                        ++dcsr_i;
+                    }
+                real_i = dcsr_i;
+                m_new_dcsr[b] = dcsr_i;
+            }
+            ptr_offset[b + 1] = po + real_i;
+            index_offset[b + 1] = nz;
+            dcsr_offset[b + 1] = dcsr_offset[b] + dcsr_i;
+        }
+    }
+    return RBS_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Reference-format outputs, rebuilt from the plan on request.  This follows
 // recblocking_preprocess.h:298-967 (get_recblock_size, L_preprocessing) and
@@ -1418,135 +1569,19 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
         return RBS_OK;
     }
     // Everything below needs the reference-order permuted CSC and the
-    // per-block extraction.
-    std::vector<int> cp_new((size_t)n + 1), ri_new((size_t)nnz);
-    std::vector<double> va_new((size_t)nnz);
-    cp_new[0] = 0;
-    for (int i = 0; i < n; ++i) {
-        int src = fwd ? P.bfs_item[i] : P.bfs_item[n - 1 - i];
-        int len = P.in_cp[src + 1] - P.in_cp[src];
-        cp_new[i + 1] = cp_new[i] + len;
-        for (int j = 0; j < len; ++j) {
-            ri_new[cp_new[i] + j] = P.label[P.in_ri[P.in_cp[src] + j]];
-            va_new[cp_new[i] + j] = P.in_va[P.in_cp[src] + j];
-        }
+    // per-block extraction: built once per plan, on the first request.
+    if (!P.ref_pack) {
+        auto pk = std::make_shared<RefPack>();
+        int rc = build_ref_pack(P, fwd, blk_m, blk_n, blk_nnz, stu, std_, sru, srd, srl, srr, method, *pk, err);
+        if (rc) return rc;
+        P.ref_pack = pk;
     }
-    std::vector<int> ptr_offset(sum + 1), index_offset(sum + 1), dcsr_offset(sum + 1);
-    int ps = 1, is = 0, ds = 0;
-    for (int b = 0; b < sum; ++b) {
-        if ((b & 1) == 0) { ps += blk_n[b] + 1; is += blk_nnz[b]; }
-        else { ps += blk_m[b]; is += blk_nnz[b]; ds += blk_m[b]; }
-    }
-    std::vector<int> Ptr((size_t)ps, 0), Index((size_t)std::max(is, 1)), Dcsr((size_t)std::max(ds, 1), 0);
-    std::vector<double> Val((size_t)std::max(is, 1));
-    std::vector<int> nlv(sum, 0), longrow(sum, 0), m_new_dcsr(sum, -1);
-    std::vector<int> lvl_ptr, lvl_item, m_lv, off_lv, nnz_lv;
-    ptr_offset[0] = 1;
-    index_offset[0] = 0;
-    dcsr_offset[0] = 0;
-    int nz = 0;
-    for (int b = 0; b < sum; ++b) {
-        const int bm = blk_m[b], bn = blk_n[b];
-        int po = ptr_offset[b];
-        std::vector<int> scp((size_t)bn + 1, 0), sri;
-        std::vector<double> sva;
-        if ((b & 1) == 0) {
-            int up = stu[b], down = std_[b];
-            for (int c = up; c < down; ++c) {
-                for (int k = cp_new[c]; k < cp_new[c + 1]; ++k) {
-                    int r = ri_new[k];
-                    if (fwd ? r < down : r >= up) {
-                        sri.push_back(r - up);
-                        sva.push_back(va_new[k]);
-                    }
-                }
-                scp[(size_t)(c - up) + 1] = (int)sri.size();
-            }
-            std::vector<int> rrp, rci;
-            std::vector<double> rva;
-            transpose(bn, bm, scp.data(), sri.data(), sva.data(), rrp, rci, rva);
-            std::vector<int> lp, li;
-            int nl = 1;
-            if (bm == (int)sri.size()) {
-                lp = {0, bm};
-                li.resize((size_t)bm);
-                for (int i = 0; i < bm; ++i) li[i] = i;
-            } else {
-                nl = bfs_levels(scp.data(), sri.data(), bm, lp, li);
-                if (nl < 0) { err = "export: local level search stuck"; return RBS_ERR_STRUCTURE; }
-            }
-            nlv[b] = nl;
-            lvl_ptr.insert(lvl_ptr.end(), lp.begin(), lp.end());
-            lvl_item.insert(lvl_item.end(), li.begin(), li.end());
-            int meth = method[b];
-            if (meth == 0 || meth == 3) {
-                for (int i = 0; i < bn; ++i) {
-                    for (int k = scp[i]; k < scp[i + 1]; ++k) { Index[nz] = sri[k]; Val[nz] = sva[k]; ++nz; }
-                    Ptr[po + i] = Ptr[po + i - 1] + scp[i + 1] - scp[i];
-                }
-            } else if (meth == 2) {
-                for (int l = 0; l < nl; ++l) {
-                    m_lv.push_back(lp[l + 1] - lp[l]);
-                    off_lv.push_back(lp[l]);
-                    int sacc = 0;
-                    for (int q = lp[l]; q < lp[l + 1]; ++q) sacc += rrp[q + 1] - rrp[q];
-                    nnz_lv.push_back(sacc);
-                }
-                for (int i = 0; i < bm; ++i) {
-                    for (int k = rrp[i]; k < rrp[i + 1]; ++k) { Index[nz] = rci[k]; Val[nz] = rva[k]; ++nz; }
-                    Ptr[po + i] = Ptr[po + i - 1] + rrp[i + 1] - rrp[i];
-                }
-            } else {
-                Ptr[po] = 0;
-                int c = 0;
-                for (int i = 0; i < bm; ++i) {
-                    for (int k = rrp[i]; k < rrp[i + 1]; ++k) { Index[nz] = rci[k]; Val[nz] = rva[k]; ++nz; ++c; }
-                    Ptr[po + i + 1] = c;
-                }
-            }
-            ptr_offset[b + 1] = po + bm + (meth == 1 ? 1 : 0);
-            index_offset[b + 1] = nz;
-            dcsr_offset[b + 1] = dcsr_offset[b];
-        } else {
-            int up = sru[b], down = srd[b], left = srl[b], right = srr[b];
-            for (int c = left; c < right; ++c) {
-                for (int k = cp_new[c]; k < cp_new[c + 1]; ++k) {
-                    int r = ri_new[k];
-                    if (r >= up && r < down) {
-                        sri.push_back(r - up);
-                        sva.push_back(va_new[k]);
-                    }
-                }
-                scp[(size_t)(c - left) + 1] = (int)sri.size();
-            }
-            std::vector<int> rrp, rci;
-            std::vector<double> rva;
-            transpose(bn, bm, scp.data(), sri.data(), sva.data(), rrp, rci, rva);
-            for (int i = 0; i < bm; ++i)
-                for (int k = rrp[i]; k < rrp[i + 1]; ++k) { Index[nz] = rci[k]; Val[nz] = rva[k]; ++nz; }
-            int real_i = 0, dcsr_i = 0, meth = method[b];
-            int lr = 0;
-            for (int i = 0; i < bm; ++i)
-                if (rrp[i + 1] - rrp[i] > kLongRow) ++lr;
-            longrow[b] = meth >= 0 ? lr : 0;
-            if (meth == 0 || meth == 2) {
-                for (int i = 0; i < bm; ++i) Ptr[po + i] = Ptr[po + i - 1] + rrp[i + 1] - rrp[i];
-                real_i = bm;
-            } else if (meth == 1 || meth == 3) {
-                for (int i = 0; i < bm; ++i)
-                    if (rrp[i + 1] != rrp[i]) {
-                        Ptr[po + dcsr_i] = Ptr[po + dcsr_i - 1] + rrp[i + 1] - rrp[i];
-                        Dcsr[dcsr_offset[b] + dcsr_i] = i;
-                        ++dcsr_i;
-                    }
-                real_i = dcsr_i;
-                m_new_dcsr[b] = dcsr_i;
-            }
-            ptr_offset[b + 1] = po + real_i;
-            index_offset[b + 1] = nz;
-            dcsr_offset[b + 1] = dcsr_offset[b] + dcsr_i;
-        }
-    }
+    const RefPack &R = *P.ref_pack;
+    const auto &ptr_offset = R.ptr_offset, &index_offset = R.index_offset, &dcsr_offset = R.dcsr_offset;
+    const auto &Ptr = R.Ptr, &Index = R.Index, &Dcsr = R.Dcsr;
+    const auto &Val = R.Val;
+    const auto &nlv = R.nlv, &longrow = R.longrow, &m_new_dcsr = R.m_new_dcsr;
+    const auto &lvl_ptr = R.lvl_ptr, &lvl_item = R.lvl_item, &m_lv = R.m_lv, &off_lv = R.off_lv, &nnz_lv = R.nnz_lv;
     if (name == "ptr_offset") return put(ptr_offset);
     if (name == "index_offset") return put(index_offset);
     if (name == "dcsrindex_offset") return put(dcsr_offset);

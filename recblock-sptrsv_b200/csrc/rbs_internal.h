@@ -26,6 +26,7 @@
 #include <atomic>
 #include <cstdint>
 #include <cstdlib>
+#include <memory>
 #include <new>
 #include <string>
 #include <thread>
@@ -181,6 +182,17 @@ enum { LVL_PLAIN = 0, LVL_CA = 1, LVL_CSF = 2, LVL_LC = 3 };
 
 struct DeviceState;  // executor side (solve.cu)
 
+// The reference-format packed arrays (recblock_Ptr/Index/Val, DCSR row
+// lists, block offsets, local level sets), rebuilt from a plan by
+// export_reference on the first request and kept with the plan.
+struct RefPack {
+    std::vector<int> ptr_offset, index_offset, dcsr_offset;
+    std::vector<int> Ptr, Index, Dcsr;
+    std::vector<double> Val;
+    std::vector<int> nlv, longrow, m_new_dcsr;
+    std::vector<int> lvl_ptr, lvl_item, m_lv, off_lv, nnz_lv;
+};
+
 struct Plan {
     int n = 0, nnz = 0, lv = 0, sub = 0, nlevel = 0, sum_block = 0, step = 0;
     rbs_options opt{};
@@ -227,6 +239,9 @@ struct Plan {
     bulk_vector<double> full_val;
 
     DeviceState *dev = nullptr;
+    // reference-format export cache (export_reference); exports of one plan
+    // from several threads at once are not supported
+    mutable std::shared_ptr<const RefPack> ref_pack;
 };
 
 // analysis.cpp
