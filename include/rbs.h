@@ -128,6 +128,16 @@ int rbs_solve_host(rbs_plan *plan, const double *b, double *x, int k, int ld, in
 /* Asynchronous variant: enqueue on the plan's stream and return.  Status of
  * the device-side checks is collected by rbs_plan_sync. */
 int rbs_solve_async(rbs_plan *plan, const double *d_b, double *d_x, int k, int ld, int prec);
+/* Asynchronous HOST-array solve (no counterpart in the reference): b is
+ * uploaded on a copy stream into one of two plan-owned staging slots, solved
+ * on the plan's stream, and x downloaded on a second copy stream, so
+ * consecutive calls overlap one solve with the neighbouring calls' copies.
+ * Returns after enqueueing; b must stay unchanged and x unread until
+ * rbs_plan_sync, which waits for every enqueued solve and reports the
+ * device-side checks.  Use page-locked (pinned) b and x for the copies to
+ * overlap.  RBS_PREC_MIXED runs synchronously (its refinement checks each
+ * correction on the host). */
+int rbs_solve_host_async(rbs_plan *plan, const double *b, double *x, int k, int ld, int prec);
 int rbs_plan_sync(rbs_plan *plan);
 
 /* cudaStream_t passed as void* (NULL = the plan's own stream). */
@@ -332,16 +342,20 @@ int rbs_auto_lv(int m, int device_id);
  * row), b and x, all device pointers; lower for RBS_FORWARD, upper for
  * RBS_BACKWARD.  No analysis: rows are solved in index order by the
  * sync-free kernel.  stream may be NULL (legacy default stream).  The call
- * returns when the solve is complete.
+ * is synchronous: it reads the row pointer's last entry back to the host
+ * and returns when the solve is complete.  A row without its diagonal (or
+ * with a zero one) or an entry on the wrong side of the diagonal or outside
+ * [0, n) gives RBS_ERR_STRUCTURE; such an entry is never waited on.
  *
  * Scratch: a static device array of RBS_NOALLOC_MAX_ROWS doubles plus 256
  * bytes (about 8 MB), held by every GPU that loads this library until the
  * process exits.  n > RBS_NOALLOC_MAX_ROWS is rejected with RBS_ERR_ARG.
  * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * Every call on a device shares the one array: calls whose work overlaps on
- * the GPU (different streams or host threads) race and corrupt each other's
- * results; serialise them. */
+ * (cudaGetSymbolAddress) and keeps it for the life of the process; make
+ * that first call before any stream capture begins, and do not use this
+ * entry point across a cudaDeviceReset.  Every call on a device shares the
+ * one array: calls whose work overlaps on the GPU (different streams or
+ * host threads) race and corrupt each other's results; serialise them. */
 #define RBS_NOALLOC_MAX_ROWS (1 << 20)
 int rbs_sptrsv_csr_noalloc(const int *d_rowptr, const int *d_colidx, const double *d_val, int n,
                            int substitution, const double *d_b, double *d_x, void *stream);

@@ -255,6 +255,17 @@ int rbs_solve_host(rbs_plan *plan, const double *b, double *x, int k, int ld, in
     return RBS_OK;
 }
 
+int rbs_solve_host_async(rbs_plan *plan, const double *b, double *x, int k, int ld, int prec) {
+    int rc = check_solve_args(plan, b, x, k, ld, prec);
+    if (rc) return rc;
+    if (!plan->p.dev) return fail(RBS_ERR_ARG, "rbs_solve_host_async: plan has no device state");
+    if (prec == RBS_PREC_MIXED) return rbs_solve_host(plan, b, x, k, ld, prec, nullptr);  // refinement waits per step
+    std::string err;
+    rc = rbs::device_host_async(plan->p, b, x, k, ld, prec, err);
+    if (rc) return fail(rc, "rbs_solve_host_async: " + err);
+    return RBS_OK;
+}
+
 int rbs_plan_set_stream(rbs_plan *plan, void *stream) {
     if (!plan) return fail(RBS_ERR_ARG, "rbs_plan_set_stream: plan is NULL");
     std::string err;

@@ -48,12 +48,18 @@ __device__ __forceinline__ void band_step_M(VT (&M)[W][W], VT (&c)[W], const VT 
     c[0] = c0;
 }
 
+// Several right-hand sides run side by side in one launch of each pass:
+// column c = blockIdx.y of the maps and replay passes (blockIdx.x of the
+// scan), with its own maps and states at c * nch * (W*W + W) and c * nch * W.
+//
 // Pass 1: maps[j] = composition of the row maps of chunk j.
 template <typename VT, int W>
 __global__ void __launch_bounds__(256) k_band_maps(const VT *__restrict__ coef, const VT *__restrict__ inv,
-                                                   const VT *__restrict__ b, int K, int colk, int m, int C, int nch,
+                                                   const VT *__restrict__ b, int K, int m, int C, int nch,
                                                    VT *__restrict__ maps) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int colk = blockIdx.y;
+    maps += (long long)colk * nch * (W * W + W);
     if (j >= nch) return;
     VT M[W][W], c[W];
 #pragma unroll
@@ -113,6 +119,8 @@ __device__ __forceinline__ void band_compose_after(VT (&M)[W][W], VT (&c)[W], co
 template <typename VT, int W>
 __global__ void __launch_bounds__(256) k_band_scan(const VT *__restrict__ maps, int nch, VT *__restrict__ states) {
     extern __shared__ unsigned char smem_raw[];
+    maps += (long long)blockIdx.x * nch * (W * W + W);
+    states += (long long)blockIdx.x * nch * W;
     VT *sm = reinterpret_cast<VT *>(smem_raw);
     constexpr int E = W * W + W;
     const int tid = threadIdx.x, T = blockDim.x;
@@ -191,9 +199,11 @@ __global__ void __launch_bounds__(256) k_band_scan(const VT *__restrict__ maps, 
 // Pass 3: replay chunk j from its entering state and write x.
 template <typename VT, int W>
 __global__ void __launch_bounds__(256) k_band_replay(const VT *__restrict__ coef, const VT *__restrict__ inv,
-                                                     const VT *__restrict__ b, int K, int colk, int m, int C, int nch,
+                                                     const VT *__restrict__ b, int K, int m, int C, int nch,
                                                      const VT *__restrict__ states, VT *x) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int colk = blockIdx.y;
+    states += (long long)colk * nch * W;
     if (j >= nch) return;
     VT s[W];
 #pragma unroll

@@ -136,6 +136,69 @@ __global__ void k_scatter_cols(VT *__restrict__ xw, const int *__restrict__ perm
     }
 }
 
+// Transposing forms of the gather and scatter for many right-hand sides
+// (K >= 8): a CTA takes a tile of 32 original rows, reads it column by
+// column (32 consecutive values of a column: coalesced), and writes every
+// row at its processing position (K consecutive values: coalesced), through
+// a shared-memory tile; the scatter runs the other way.  Columns come from
+// b + c*ld, or from the table cols[c] when cols is not NULL.  ipos[i] is the
+// processing position of original row i.
+constexpr int TP_ROWS = 32;
+
+template <typename VT, typename VT2, int K>
+__global__ void __launch_bounds__(256) k_gather_t(const double *__restrict__ b, int ld,
+                                                  const double *const *__restrict__ cols, int k,
+                                                  const int *__restrict__ ipos, int n, VT *__restrict__ out,
+                                                  VT2 *__restrict__ out2) {
+    __shared__ double tile[K][TP_ROWS + 1];
+    for (long long i0 = (long long)blockIdx.x * TP_ROWS; i0 < n; i0 += (long long)gridDim.x * TP_ROWS) {
+        const int rows = (int)min((long long)TP_ROWS, n - i0);
+        for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
+            const int c = e / TP_ROWS, t = e % TP_ROWS;
+            double v = 0.0;
+            if (c < k && t < rows) v = cols ? cols[c][i0 + t] : b[(long long)c * ld + i0 + t];
+            tile[c][t] = v;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
+            const int t = e / K, c = e % K;
+            if (t < rows) {
+                const long long o = (long long)ipos[i0 + t] * K + c;
+                out[o] = (VT)tile[c][t];
+                if (out2) out2[o] = (VT2)tile[c][t];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// RESET: the work vector is set back to the sentinel as it is read.
+template <typename VT, int K, bool RESET>
+__global__ void __launch_bounds__(256) k_scatter_t(VT *__restrict__ xw, const int *__restrict__ ipos, int n, int k,
+                                                   double *__restrict__ x, int ld, double *const *__restrict__ cols) {
+    __shared__ double tile[K][TP_ROWS + 1];
+    for (long long i0 = (long long)blockIdx.x * TP_ROWS; i0 < n; i0 += (long long)gridDim.x * TP_ROWS) {
+        const int rows = (int)min((long long)TP_ROWS, n - i0);
+        for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
+            const int t = e / K, c = e % K;
+            if (t < rows) {
+                const long long o = (long long)ipos[i0 + t] * K + c;
+                tile[c][t] = (double)xw[o];
+                if (RESET) xw[o] = Sent<VT>::value();
+            }
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
+            const int c = e / TP_ROWS, t = e % TP_ROWS;
+            if (c < k && t < rows) {
+                if (cols) cols[c][i0 + t] = tile[c][t];
+                else x[(long long)c * ld + i0 + t] = tile[c][t];
+            }
+        }
+        __syncthreads();
+    }
+}
+
 template <typename VT>
 __global__ void k_fill(VT *__restrict__ v, long long count, VT value) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;

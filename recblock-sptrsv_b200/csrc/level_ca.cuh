@@ -18,6 +18,15 @@
 // 4-16 byte copies and the level's loads are coalesced.
 // Dependencies within the last XW rows come from the window; older ones
 // from x in global memory (written by this CTA before an earlier barrier).
+//
+// Several right-hand sides: the work vectors are row-interleaved with a row
+// stride ld (entry (row, column c) at v[row*ld + c]); CTA y of the launch's
+// second grid dimension solves the G consecutive columns [y*G, y*G+G) on its
+// own, with no synchronisation between CTAs: every column group walks the
+// same levels with its own window (G values per slot), and the rows' columns,
+// values and inverse diagonal, which all groups share, come through L2.  One
+// dependency walk per group serves G columns; the groups run side by side
+// on separate SMs.
 #pragma once
 
 #include <type_traits>
@@ -35,19 +44,21 @@ struct CaDesc {
     const int *col;   // row-major level-ELL columns (block-local), padding -1
     const void *val;  // level-ELL values
     const void *inv;  // inverse diagonal of the block's rows
-    const void *b;    // right-hand side of the block's rows
-    void *x;          // solution of the block's rows
+    const void *b;    // right-hand side of the block's rows (row stride ld)
+    void *x;          // solution of the block's rows (row stride ld)
     const int *lvl;   // per level: lo, off, w, 0 (4 ints), then {m, 0, 0, 0}
-    int m, nlv, pad0, pad1;
+    int m, nlv, ld, pad1;
 };
 
-template <typename VT, int W, int S>
+template <typename VT, int W, int S, int G = 1>
 struct CaLayout {
     static constexpr size_t col_bytes = (size_t)W * CA_ROWS * 4;
     static constexpr size_t val_bytes = (size_t)W * CA_ROWS * sizeof(VT);
-    static constexpr size_t stage_bytes = col_bytes + val_bytes + 2 * CA_ROWS * sizeof(VT);
+    static constexpr size_t inv_bytes = (size_t)CA_ROWS * sizeof(VT);
+    static constexpr size_t b_bytes = (size_t)G * CA_ROWS * sizeof(VT);
+    static constexpr size_t stage_bytes = col_bytes + val_bytes + inv_bytes + b_bytes;
     static constexpr size_t xw_off = S * stage_bytes;
-    static constexpr size_t tab_off = xw_off + (CA_XW + 16) * sizeof(VT);
+    static constexpr size_t tab_off = xw_off + (CA_XW + 16) * G * sizeof(VT);
     static constexpr size_t total = tab_off + CA_TAB * 4;
 };
 
@@ -101,14 +112,19 @@ struct alignas(sizeof(T) * N) Vec {
 // WIN: the block's columns are window slots (every dependency within the
 // window; padding reads the zero slot), so a dependency is one shared-memory
 // load and an unconditional multiply-add.
-template <typename VT, int W, int S, bool WIN>
+// G: right-hand sides per CTA (blockIdx.y selects the column group); for
+// G == 1 and d.ld == 1 this is the single right-hand-side solve.
+template <typename VT, int W, int S, bool WIN, int G = 1>
 __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict__ descs) {
-    using Lay = CaLayout<VT, W, S>;
+    using Lay = CaLayout<VT, W, S, G>;
+    using VG = Vec<VT, G>;
     static_assert(S == 2 || S == 4, "stage count 2 or 4");
+    static_assert(G == 1 || G == 2 || G == 4, "1, 2 or 4 right-hand sides per CTA");
     extern __shared__ __align__(128) unsigned char sm[];
     const CaDesc d = descs[blockIdx.x];
-    VT *x = (VT *)d.x;
-    VT *xs = reinterpret_cast<VT *>(sm + Lay::xw_off);
+    const int ld = d.ld, j0 = blockIdx.y * G;
+    VT *x = (VT *)d.x + j0;
+    VG *xs = reinterpret_cast<VG *>(sm + Lay::xw_off);
     int *tab = reinterpret_cast<int *>(sm + Lay::tab_off);
     const int tid = threadIdx.x;
     const int nlv = d.nlv;
@@ -116,7 +132,12 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
     const bool in_smem = ntab <= CA_TAB;
     if (in_smem)
         for (int i = tid; i < ntab; i += blockDim.x) tab[i] = d.lvl[i];
-    if (tid == 0) xs[CA_XW] = VT(0);
+    if (tid == 0) {
+        VG z;
+#pragma unroll
+        for (int g = 0; g < G; ++g) z.v[g] = VT(0);
+        xs[CA_XW] = z;
+    }
     __syncthreads();
     const int4 *lt = reinterpret_cast<const int4 *>(in_smem ? tab : d.lvl);
 
@@ -124,12 +145,13 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
     const int *colp = d.col + tid * W;
     const VT *valp = (const VT *)d.val + tid * W;
     const VT *inv_t = (const VT *)d.inv + tid;
-    const VT *b_t = (const VT *)d.b + tid;
+    const VT *b_t = (const VT *)d.b + (size_t)tid * ld + j0;
     const unsigned s0 = (unsigned)__cvta_generic_to_shared(sm);
     const unsigned s_col = s0 + tid * W * 4;
     const unsigned s_val = s0 + (unsigned)Lay::col_bytes + tid * W * (unsigned)sizeof(VT);
     const unsigned s_inv = s0 + (unsigned)(Lay::col_bytes + Lay::val_bytes) + tid * (unsigned)sizeof(VT);
-    const unsigned s_b = s_inv + CA_ROWS * (unsigned)sizeof(VT);
+    const unsigned s_b = s0 + (unsigned)(Lay::col_bytes + Lay::val_bytes + Lay::inv_bytes) +
+                         tid * G * (unsigned)sizeof(VT);
 
     // stage the row data of level l into slot U (= l % S) for this thread,
     // one commit group per level
@@ -140,7 +162,7 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
             cp_async_sn<4 * W>(s_col + off, colp + e.y);
             cp_async_sn<(int)sizeof(VT) * W>(s_val + off, valp + e.y);
             cp_async_sn<(int)sizeof(VT)>(s_inv + off, inv_t + e.x);
-            cp_async_sn<(int)sizeof(VT)>(s_b + off, b_t + e.x);
+            cp_async_sn<(int)sizeof(VT) * G>(s_b + off, b_t + (size_t)e.x * ld);
         }
         cp_async_commit();
     };
@@ -164,22 +186,33 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
             const Vec<int, W> cs = reinterpret_cast<const Vec<int, W> *>(st)[tid];
             const Vec<VT, W> vs = reinterpret_cast<const Vec<VT, W> *>(st + Lay::col_bytes)[tid];
             const VT iv = reinterpret_cast<const VT *>(st + Lay::col_bytes + Lay::val_bytes)[tid];
-            const VT bv = reinterpret_cast<const VT *>(st + Lay::col_bytes + Lay::val_bytes)[CA_ROWS + tid];
-            VT sum = 0;
+            const VG bv = reinterpret_cast<const VG *>(st + Lay::col_bytes + Lay::val_bytes + Lay::inv_bytes)[tid];
+            VT sum[G];
+#pragma unroll
+            for (int g = 0; g < G; ++g) sum[g] = 0;
 #pragma unroll
             for (int j = 0; j < W; ++j) {
                 const int c = cs.v[j];
                 if constexpr (WIN) {
-                    sum += vs.v[j] * xs[c];
+                    const VG xv = xs[c];
+#pragma unroll
+                    for (int g = 0; g < G; ++g) sum[g] += vs.v[j] * xv.v[g];
                 } else if (c >= 0) {
-                    const VT xv = c >= hi - CA_XW ? xs[c & (CA_XW - 1)] : x[c];
-                    sum += vs.v[j] * xv;
+                    VG xv;
+                    if (c >= hi - CA_XW) xv = xs[c & (CA_XW - 1)];
+                    else if constexpr (G == 1) xv.v[0] = x[(size_t)c * ld];
+                    else xv = *reinterpret_cast<const VG *>(x + (size_t)c * ld);
+#pragma unroll
+                    for (int g = 0; g < G; ++g) sum[g] += vs.v[j] * xv.v[g];
                 }
             }
             const int r = lo + tid;
-            const VT xv = finalize((bv - sum) * iv);
+            VG xv;
+#pragma unroll
+            for (int g = 0; g < G; ++g) xv.v[g] = finalize((bv.v[g] - sum[g]) * iv);
             xs[r & (CA_XW - 1)] = xv;
-            x[r] = xv;
+            if constexpr (G == 1) x[(size_t)r * ld] = xv.v[0];
+            else *reinterpret_cast<VG *>(x + (size_t)r * ld) = xv;
         }
         lo = hi;
         __syncthreads();

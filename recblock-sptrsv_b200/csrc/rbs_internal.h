@@ -313,6 +313,10 @@ int device_profile(Plan &P, int enable, std::string &err);
 int device_tune(Plan &P, std::string &err);
 int device_block_times(const Plan &P, std::vector<double> &ms, long long &solves);
 int device_staging(Plan &P, size_t bytes, double *&db, double *&dx, std::string &err);
+// host-array solve enqueued without waiting: upload on a copy stream,
+// solve on the plan's stream, download on another copy stream; two staging
+// slots in turn (device_sync waits for everything)
+int device_host_async(Plan &P, const double *b, double *x, int k, int ld, int prec, std::string &err);
 // work vectors for k right-hand sides allocated now, so solves up to that
 // width allocate nothing
 int device_reserve(Plan &P, int k, std::string &err);

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <map>
 #include <set>
+#include <type_traits>
 #include <vector>
 
 #include "band.cuh"
@@ -41,13 +42,15 @@ struct DeviceState {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // plan pools
     int *rp = nullptr, *col = nullptr, *lvl = nullptr, *map = nullptr, *rows = nullptr, *perm = nullptr;
+    int *ipos = nullptr;  // original row -> processing position (inverse of perm)
     double *val = nullptr, *inv = nullptr;
     float *val32 = nullptr, *inv32 = nullptr;
     int *full_rp = nullptr, *full_col = nullptr;
     double *full_val = nullptr;
     double *band_coef = nullptr, *band_inv = nullptr;   // band-scan layout (f64)
     float *band_coef32 = nullptr, *band_inv32 = nullptr;
-    double *band_maps = nullptr, *band_states = nullptr; // scratch of the band scan (f64 or f32)
+    double *band_maps = nullptr, *band_states = nullptr; // scratch of the band scan (f64 or f32), kcap columns
+    size_t band_maps1 = 1, band_states1 = 1;             // ... elements per column
     int *ell_col = nullptr;
     double *ell_val = nullptr;
     float *ell_val32 = nullptr;
@@ -81,6 +84,17 @@ struct DeviceState {
     // staging for the host-array API
     double *stage_b = nullptr, *stage_x = nullptr;
     size_t stage_bytes = 0;
+    // asynchronous host-array solves (device_host_async): two staging slots
+    // used in turn, uploads on `cin`, downloads on `cout`, so one call's
+    // copies overlap the neighbouring calls' solves
+    struct HostPipe {
+        cudaStream_t cin = nullptr, cout = nullptr;
+        cudaEvent_t in_done[2] = {nullptr, nullptr}, solved[2] = {nullptr, nullptr}, out_done[2] = {nullptr, nullptr};
+        double *db[2] = {nullptr, nullptr}, *dx[2] = {nullptr, nullptr};
+        size_t bytes = 0;
+        int next = 0;
+        bool used[2] = {false, false};
+    } pipe;
     int last_iters = 0;
     double last_corr = 0;
     // the asynchronous batch in flight (device_batch_*)
@@ -150,6 +164,9 @@ int pow2_at_least(int k) {
 }
 
 void free_work(DeviceState &D) {
+    cudaFree(D.band_maps);
+    cudaFree(D.band_states);
+    D.band_maps = D.band_states = nullptr;
     cudaFree(D.bw64);
     cudaFree(D.xw64);
     cudaFree(D.b64keep);
@@ -206,6 +223,8 @@ int ensure_work(Plan &P, int K, std::string &err) {
         if ((rc = alloc(D, D.bw32, cnt, err))) return undo(rc);
         if ((rc = alloc(D, D.xw32, cnt, err))) return undo(rc);
     }
+    if ((rc = alloc(D, D.band_maps, D.band_maps1 * K, err))) return undo(rc);
+    if ((rc = alloc(D, D.band_states, D.band_states1 * K, err))) return undo(rc);
     k_fill<double><<<grid_for((long long)cnt, 256, D.num_sms), 256, 0, D.stream>>>(D.xw64, (long long)cnt,
                                                                                     sent64_host());
     if (D.mixed)
@@ -319,23 +338,48 @@ int ell_descs(Plan &P, CsfDesc *&out, std::string &err) {
     return RBS_OK;
 }
 
-template <typename VT, int W, int S>
+template <typename VT, int W, int S, int G = 1>
 int ca_attr(std::string &err) {
     static std::atomic<unsigned long long> done{0};
     if (!attr_done(done)) {
-        CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)CaLayout<VT, W, S>::total));
-        CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)CaLayout<VT, W, S>::total));
+        CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, false, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)CaLayout<VT, W, S, G>::total));
+        CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, true, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)CaLayout<VT, W, S, G>::total));
         attr_mark(done);
     }
     return RBS_OK;
 }
 
+// Stage counts of the staged level kernel per (value type, ELL width W,
+// right-hand sides per CTA G): the deepest staging that fits the 227 KB of
+// shared memory next to the x window of G values per slot.
+template <typename VT> constexpr int ca_stages(int W, int G) {
+    if (G == 1) return W == 4 ? 2 : 4;
+    if (sizeof(VT) == 8) return W == 4 ? 0 : 2;  // 0: no such kernel
+    return W == 4 ? 2 : 4;
+}
+
+// Right-hand sides per CTA of a staged level triangle solved for K columns:
+// one CTA per column keeps every group's dependency walk as short as the
+// single right-hand side's; two per CTA halve the shared row data the groups
+// pull through L2 when there are many groups.  RBS_CA_GROUP (1 or 2)
+// overrides the choice.
+template <typename VT> int ca_group(const ExecBlock &B, int K) {
+    if (K == 1) return 1;
+    static const int forced = [] {
+        const char *e = std::getenv("RBS_CA_GROUP");
+        return e ? std::atoi(e) : 0;
+    }();
+    int G = forced == 1 || forced == 2 ? forced : (K >= 64 ? 2 : 1);
+    if (G == 2 && ca_stages<VT>(B.ca_w, 2) == 0) G = 1;
+    return G;
+}
+
 template <typename VT>
-int ca_descs(Plan &P, CaDesc *&out, std::string &err) {
+int ca_descs(Plan &P, CaDesc *&out, int K, std::string &err) {
     DeviceState &D = *P.dev;
-    long long key = sizeof(VT) == 8 ? 0 : 1;
+    const long long key = (long long)K * 2 + (sizeof(VT) == 8 ? 0 : 1);
     auto it = D.ca_cache.find(key);
     if (it != D.ca_cache.end()) {
         out = it->second;
@@ -348,11 +392,12 @@ int ca_descs(Plan &P, CaDesc *&out, std::string &err) {
         d.col = D.ca_col + B.ca_lo;
         d.val = Pools<VT>::cav(D) + B.ca_lo;
         d.inv = Pools<VT>::inv(D) + B.r0;
-        d.b = Pools<VT>::bw(D) + B.r0;
-        d.x = Pools<VT>::xw(D) + B.r0;
+        d.b = Pools<VT>::bw(D) + (long long)B.r0 * K;
+        d.x = Pools<VT>::xw(D) + (long long)B.r0 * K;
         d.lvl = D.ca_tab + B.ca_tab_off;
         d.m = B.m;
         d.nlv = B.nlv;
+        d.ld = K;
         h.push_back(d);
     }
     CaDesc *dd = nullptr;
@@ -362,8 +407,45 @@ int ca_descs(Plan &P, CaDesc *&out, std::string &err) {
     out = dd;
     int rc;
     if ((rc = ca_attr<VT, 1, 4>(err)) || (rc = ca_attr<VT, 2, 4>(err)) || (rc = ca_attr<VT, 4, 2>(err))) return rc;
-
+    if (K > 1) {
+        if constexpr (sizeof(VT) == 8) {
+            if ((rc = ca_attr<VT, 1, 2, 2>(err)) || (rc = ca_attr<VT, 2, 2, 2>(err))) return rc;
+        } else {
+            if ((rc = ca_attr<VT, 1, 4, 2>(err)) || (rc = ca_attr<VT, 2, 4, 2>(err)) ||
+                (rc = ca_attr<VT, 4, 2, 2>(err)))
+                return rc;
+        }
+    }
     return RBS_OK;
+}
+
+// One staged level triangle: one thread per row of the widest level, one
+// CTA per group of G right-hand sides.
+template <typename VT, int W, int S, int G>
+void launch_ca(const ExecBlock &B, const CaDesc *desc, int K, cudaStream_t st) {
+    const int nt = std::min(1024, std::max(32, (B.maxwidth + 31) / 32 * 32));
+    const dim3 grid(1, K / G);
+    if (B.ca_win)
+        k_tri_level_ca<VT, W, S, true, G><<<grid, nt, CaLayout<VT, W, S, G>::total, st>>>(desc);
+    else
+        k_tri_level_ca<VT, W, S, false, G><<<grid, nt, CaLayout<VT, W, S, G>::total, st>>>(desc);
+}
+
+template <typename VT>
+void launch_ca_any(const ExecBlock &B, const CaDesc *desc, int K, cudaStream_t st) {
+    const int G = ca_group<VT>(B, K);
+    if (G == 1) {
+        if (B.ca_w == 1) launch_ca<VT, 1, 4, 1>(B, desc, K, st);
+        else if (B.ca_w == 2) launch_ca<VT, 2, 4, 1>(B, desc, K, st);
+        else launch_ca<VT, 4, 2, 1>(B, desc, K, st);
+    } else if constexpr (sizeof(VT) == 8) {
+        if (B.ca_w == 1) launch_ca<VT, 1, 2, 2>(B, desc, K, st);
+        else launch_ca<VT, 2, 2, 2>(B, desc, K, st);
+    } else {
+        if (B.ca_w == 1) launch_ca<VT, 1, 4, 2>(B, desc, K, st);
+        else if (B.ca_w == 2) launch_ca<VT, 2, 4, 2>(B, desc, K, st);
+        else launch_ca<VT, 4, 2, 2>(B, desc, K, st);
+    }
 }
 
 template <typename VT>
@@ -412,7 +494,7 @@ int syncfree_grid(const DeviceState &D) {
     return per_sm * D.num_sms;
 }
 
-// Band-scan triangle: three launches per right-hand side (see band.cuh).
+// Band-scan triangle: three launches, each over all K right-hand sides (see band.cuh).
 template <typename VT, int W>
 int run_band(Plan &P, const ExecBlock &B, const VT *bb, VT *xx, int K, std::string &err) {
     DeviceState &D = *P.dev;
@@ -428,12 +510,10 @@ int run_band(Plan &P, const ExecBlock &B, const VT *bb, VT *xx, int K, std::stri
         CK(cudaFuncSetAttribute(k_band_scan<VT, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_mark(attr_set);
     }
-    const int grid = (B.band_nch + 255) / 256;
-    for (int c = 0; c < K; ++c) {
-        k_band_maps<VT, W><<<grid, 256, 0, st>>>(coef, binv, bb, K, c, B.m, B.band_c, B.band_nch, maps);
-        k_band_scan<VT, W><<<1, tpb, smem, st>>>(maps, B.band_nch, states);
-        k_band_replay<VT, W><<<grid, 256, 0, st>>>(coef, binv, bb, K, c, B.m, B.band_c, B.band_nch, states, xx);
-    }
+    const dim3 grid((B.band_nch + 255) / 256, K);
+    k_band_maps<VT, W><<<grid, 256, 0, st>>>(coef, binv, bb, K, B.m, B.band_c, B.band_nch, maps);
+    k_band_scan<VT, W><<<K, tpb, smem, st>>>(maps, B.band_nch, states);
+    k_band_replay<VT, W><<<grid, 256, 0, st>>>(coef, binv, bb, K, B.m, B.band_c, B.band_nch, states, xx);
     return RBS_OK;
 }
 
@@ -451,7 +531,7 @@ int launch_blocks(Plan &P, std::string &err) {
     if (rc) return rc;
     CsfDesc *edescs = nullptr;
     CaDesc *cdescs = nullptr;
-    if (K == 1 && (rc = ca_descs<VT>(P, cdescs, err))) return rc;
+    if ((rc = ca_descs<VT>(P, cdescs, K, err))) return rc;
     if (K == 1 && (rc = ell_descs<VT>(P, edescs, err))) return rc;
     if (D.ntri) CK(cudaMemsetAsync(D.tickets, 0, sizeof(int) * D.ntri, st));
     if (K == 1 && D.lc_queue) {
@@ -509,10 +589,13 @@ int launch_blocks(Plan &P, std::string &err) {
         if (B.tri) {
             const VT *bb = bw + (long long)B.r0 * K;
             VT *xx = xw + (long long)B.r0 * K;
-            // Several right-hand sides: the single-CTA level kernels have no
-            // staged multi-RHS form, and one dependency walk of the multi-CTA
-            // sync-free kernel serves all K columns, so level triangles take it.
-            const int kernel = (K > 1 && B.kernel == RBS_K_LEVEL) ? RBS_K_SYNCFREE : B.kernel;
+            // Several right-hand sides: a level triangle with a staged
+            // level-ELL layout runs one CTA per group of columns; the other
+            // single-CTA level kernels have no multi-column form, and one
+            // dependency walk of the multi-CTA sync-free kernel serves all K
+            // columns, so their triangles take it.
+            const bool mc_ca = K > 1 && B.kernel == RBS_K_LEVEL && B.ca_ok;
+            const int kernel = (K > 1 && B.kernel == RBS_K_LEVEL && !mc_ca) ? RBS_K_SYNCFREE : B.kernel;
             switch (kernel) {
             case RBS_K_DIAG:
                 k_tri_diag<VT, K><<<grid_for((long long)B.m * K, 256, D.num_sms), 256, 0, st>>>(inv + B.r0, bb, xx,
@@ -524,21 +607,8 @@ int launch_blocks(Plan &P, std::string &err) {
                     k_tri_lc<VT><<<grid, LC_T, lc_smem<VT>(), st>>>(D.lc_segs + B.lc_seg_off, B.lc_nseg,
                                                                    Pools<VT>::lcrec(D), sizeof(VT) == 4 ? 1 : 0, bb,
                                                                    xx, D.lc_queue + ti, D.status, limit);
-                } else if (K == 1 && B.lvl_var == LVL_CA && B.ca_ok) {
-                    // one thread per row of the widest level: no idle warps at the barriers
-                    const int nt = std::min(1024, std::max(32, (B.maxwidth + 31) / 32 * 32));
-                    if (B.ca_w == 1 && B.ca_win)
-                        k_tri_level_ca<VT, 1, 4, true><<<1, nt, CaLayout<VT, 1, 4>::total, st>>>(cdescs + cti);
-                    else if (B.ca_w == 1)
-                        k_tri_level_ca<VT, 1, 4, false><<<1, nt, CaLayout<VT, 1, 4>::total, st>>>(cdescs + cti);
-                    else if (B.ca_w == 2 && B.ca_win)
-                        k_tri_level_ca<VT, 2, 4, true><<<1, nt, CaLayout<VT, 2, 4>::total, st>>>(cdescs + cti);
-                    else if (B.ca_w == 2)
-                        k_tri_level_ca<VT, 2, 4, false><<<1, nt, CaLayout<VT, 2, 4>::total, st>>>(cdescs + cti);
-                    else if (B.ca_win)
-                        k_tri_level_ca<VT, 4, 2, true><<<1, nt, CaLayout<VT, 4, 2>::total, st>>>(cdescs + cti);
-                    else
-                        k_tri_level_ca<VT, 4, 2, false><<<1, nt, CaLayout<VT, 4, 2>::total, st>>>(cdescs + cti);
+                } else if ((K == 1 && B.lvl_var == LVL_CA && B.ca_ok) || mc_ca) {
+                    launch_ca_any<VT>(B, cdescs + cti, K, st);
                 } else if (K == 1 && B.lvl_var == LVL_CSF && B.ell_ok) {
                     k_tri_cta_syncfree<VT><<<1, 1024, CsfLayout<VT>::total, st>>>(edescs + eti, D.status, limit);
                 } else {
@@ -653,15 +723,54 @@ void drop_graphs(DeviceState &D) {
 }
 void drop_graphs_fwd(DeviceState &D) { drop_graphs(D); }
 
+// Right-hand sides into processing order: the caller's columns (b + c*ld,
+// or the device table cols) into the row-interleaved work vector out (and
+// out2 in a second precision, when given).  Many columns take the
+// transposing tile kernel, whose reads and writes are both coalesced.
+template <typename VT, typename VT2, int K>
+void gather_in(DeviceState &D, int n, const double *b, int ld, const double *const *cols, int k, VT *out,
+               VT2 *out2) {
+    if constexpr (K >= 8) {
+        const int grid = (int)std::min<long long>(((long long)n + TP_ROWS - 1) / TP_ROWS, (long long)D.num_sms * 8);
+        k_gather_t<VT, VT2, K><<<std::max(grid, 1), 256, 0, D.stream>>>(b, ld, cols, k, D.ipos, n, out, out2);
+    } else {
+        const int grid = grid_for((long long)n * K, 256, D.num_sms);
+        if (cols) k_gather_cols<VT, K><<<grid, 256, 0, D.stream>>>(cols, k, D.perm, n, out);
+        else k_gather<VT, K><<<grid, 256, 0, D.stream>>>(b, ld, k, D.perm, n, out);
+        if (out2) {
+            if (cols) k_gather_cols<VT2, K><<<grid, 256, 0, D.stream>>>(cols, k, D.perm, n, out2);
+            else k_gather<VT2, K><<<grid, 256, 0, D.stream>>>(b, ld, k, D.perm, n, out2);
+        }
+    }
+}
+
+// Solutions out of processing order into the caller's columns (x + c*ld or
+// the table cols); RESET puts the sentinel back into the work vector.
+template <typename VT, int K, bool RESET>
+void scatter_out(DeviceState &D, int n, VT *xw, int k, double *x, int ld, double *const *cols) {
+    if constexpr (K >= 8) {
+        const int grid = (int)std::min<long long>(((long long)n + TP_ROWS - 1) / TP_ROWS, (long long)D.num_sms * 8);
+        k_scatter_t<VT, K, RESET><<<std::max(grid, 1), 256, 0, D.stream>>>(xw, D.ipos, n, k, x, ld, cols);
+    } else {
+        const int grid = grid_for((long long)n * K, 256, D.num_sms);
+        if constexpr (RESET) {
+            if (cols) k_scatter_cols<VT, K><<<grid, 256, 0, D.stream>>>(xw, D.perm, n, k, cols);
+            else k_scatter_reset<VT, K><<<grid, 256, 0, D.stream>>>(xw, D.perm, n, k, x, ld);
+        } else {
+            static_assert(RESET || std::is_same<VT, double>::value, "FP64 accumulator only");
+            if (cols) k_scatter64_cols<K><<<grid, 256, 0, D.stream>>>(xw, D.perm, n, k, cols);
+            else k_scatter64<K><<<grid, 256, 0, D.stream>>>(xw, D.perm, n, k, x, ld);
+        }
+    }
+}
+
 template <int K>
 int solve_fp64(Plan &P, const double *b, double *x, int k, int ld, std::string &err) {
     DeviceState &D = *P.dev;
-    const int n = P.n;
-    const int grid = grid_for((long long)n * K, 256, D.num_sms);
-    k_gather<double, K><<<grid, 256, 0, D.stream>>>(b, ld, k, D.perm, n, D.bw64);
+    gather_in<double, double, K>(D, P.n, b, ld, nullptr, k, D.bw64, nullptr);
     int rc = run_blocks<double, K>(P, err);
     if (rc) return rc;
-    k_scatter_reset<double, K><<<grid, 256, 0, D.stream>>>(D.xw64, D.perm, n, k, x, ld);
+    scatter_out<double, K, true>(D, P.n, D.xw64, k, x, ld, nullptr);
     CK(cudaGetLastError());
     return RBS_OK;
 }
@@ -669,12 +778,10 @@ int solve_fp64(Plan &P, const double *b, double *x, int k, int ld, std::string &
 template <int K>
 int solve_fp32(Plan &P, const double *b, double *x, int k, int ld, std::string &err) {
     DeviceState &D = *P.dev;
-    const int n = P.n;
-    const int grid = grid_for((long long)n * K, 256, D.num_sms);
-    k_gather<float, K><<<grid, 256, 0, D.stream>>>(b, ld, k, D.perm, n, D.bw32);
+    gather_in<float, float, K>(D, P.n, b, ld, nullptr, k, D.bw32, nullptr);
     int rc = run_blocks<float, K>(P, err);
     if (rc) return rc;
-    k_scatter_reset<float, K><<<grid, 256, 0, D.stream>>>(D.xw32, D.perm, n, k, x, ld);
+    scatter_out<float, K, true>(D, P.n, D.xw32, k, x, ld, nullptr);
     CK(cudaGetLastError());
     return RBS_OK;
 }
@@ -727,10 +834,7 @@ double mixed_correction(const DeviceState &D, int K, int k) {
 template <int K>
 int solve_mixed(Plan &P, const double *b, double *x, int k, int ld, int &iters, double &corr, std::string &err) {
     DeviceState &D = *P.dev;
-    const int n = P.n;
-    const int grid = grid_for((long long)n * K, 256, D.num_sms);
-    k_gather<double, K><<<grid, 256, 0, D.stream>>>(b, ld, k, D.perm, n, D.b64keep);
-    k_gather<float, K><<<grid, 256, 0, D.stream>>>(b, ld, k, D.perm, n, D.bw32);
+    gather_in<double, float, K>(D, P.n, b, ld, nullptr, k, D.b64keep, D.bw32);
     int rc = mixed_first<K>(P, err);
     if (rc) return rc;
     iters = 0;
@@ -742,7 +846,7 @@ int solve_mixed(Plan &P, const double *b, double *x, int k, int ld, int &iters, 
         corr = mixed_correction(D, K, k);
         if (corr <= P.opt.ir_tol) break;
     }
-    k_scatter64<K><<<grid, 256, 0, D.stream>>>(D.x64acc, D.perm, n, k, x, ld);
+    scatter_out<double, K, false>(D, P.n, D.x64acc, k, x, ld, nullptr);
     CK(cudaGetLastError());
     if (!(corr <= P.opt.ir_tol)) {
         err = "mixed-precision refinement stopped at ||dx||/||x|| = " + std::to_string(corr);
@@ -774,19 +878,17 @@ template <int K>
 int batch_start_k(Plan &P, const double *const *bcols, double *const *xcols, int k, int prec, std::string &err) {
     DeviceState &D = *P.dev;
     const int n = P.n;
-    const int grid = grid_for((long long)n * K, 256, D.num_sms);
     int rc;
     if (prec == RBS_PREC_FP64) {
-        k_gather_cols<double, K><<<grid, 256, 0, D.stream>>>(bcols, k, D.perm, n, D.bw64);
+        gather_in<double, double, K>(D, n, nullptr, n, bcols, k, D.bw64, nullptr);
         if ((rc = run_blocks<double, K>(P, err))) return rc;
-        k_scatter_cols<double, K><<<grid, 256, 0, D.stream>>>(D.xw64, D.perm, n, k, xcols);
+        scatter_out<double, K, true>(D, n, D.xw64, k, nullptr, n, xcols);
     } else if (prec == RBS_PREC_FP32) {
-        k_gather_cols<float, K><<<grid, 256, 0, D.stream>>>(bcols, k, D.perm, n, D.bw32);
+        gather_in<float, float, K>(D, n, nullptr, n, bcols, k, D.bw32, nullptr);
         if ((rc = run_blocks<float, K>(P, err))) return rc;
-        k_scatter_cols<float, K><<<grid, 256, 0, D.stream>>>(D.xw32, D.perm, n, k, xcols);
+        scatter_out<float, K, true>(D, n, D.xw32, k, nullptr, n, xcols);
     } else {
-        k_gather_cols<double, K><<<grid, 256, 0, D.stream>>>(bcols, k, D.perm, n, D.b64keep);
-        k_gather_cols<float, K><<<grid, 256, 0, D.stream>>>(bcols, k, D.perm, n, D.bw32);
+        gather_in<double, float, K>(D, n, nullptr, n, bcols, k, D.b64keep, D.bw32);
         if ((rc = mixed_first<K>(P, err))) return rc;
         if ((rc = mixed_step<K>(P, err))) return rc;
     }
@@ -797,8 +899,7 @@ int batch_start_k(Plan &P, const double *const *bcols, double *const *xcols, int
 template <int K>
 int batch_end_k(Plan &P, double *const *xcols, int k, std::string &err) {
     DeviceState &D = *P.dev;
-    k_scatter64_cols<K><<<grid_for((long long)P.n * K, 256, D.num_sms), 256, 0, D.stream>>>(D.x64acc, D.perm, P.n,
-                                                                                          k, xcols);
+    scatter_out<double, K, false>(D, P.n, D.x64acc, k, nullptr, P.n, xcols);
     CK(cudaGetLastError());
     return RBS_OK;
 }
@@ -909,6 +1010,11 @@ int device_build(Plan &P, std::string &err) {
     if ((rc = upload(D, D.map, P.map_pool, err))) return rc;
     if ((rc = upload(D, D.rows, P.rows_pool, err))) return rc;
     if ((rc = upload(D, D.perm, P.perm, err))) return rc;
+    {
+        std::vector<int> ipos(P.perm.size());
+        for (size_t p = 0; p < P.perm.size(); ++p) ipos[(size_t)P.perm[p]] = (int)p;
+        if ((rc = upload(D, D.ipos, ipos, err))) return rc;
+    }
     if ((rc = upload(D, D.inv, P.inv_diag, err))) return rc;
     D.mixed = P.opt.mixed != 0;
     if (D.mixed) {
@@ -930,8 +1036,8 @@ int device_build(Plan &P, std::string &err) {
                 maps = std::max(maps, (size_t)B.band_nch * (B.band_w * B.band_w + B.band_w));
                 states = std::max(states, (size_t)B.band_nch * B.band_w);
             }
-        if ((rc = alloc(D, D.band_maps, maps, err))) return rc;
-        if ((rc = alloc(D, D.band_states, states, err))) return rc;
+        D.band_maps1 = maps;  // per right-hand side; allocated with the work vectors
+        D.band_states1 = states;
     }
     if (D.mixed) {
         const auto c32 = to_f32(P.band_coef), i32 = to_f32(P.band_inv);
@@ -1023,6 +1129,83 @@ int device_staging(Plan &P, size_t bytes, double *&db, double *&dx, std::string 
     }
     db = D.stage_b;
     dx = D.stage_x;
+    return RBS_OK;
+}
+
+void pipe_release(DeviceState &D) {
+    DeviceState::HostPipe &H = D.pipe;
+    if (H.cin) cudaStreamSynchronize(H.cin);
+    if (H.cout) cudaStreamSynchronize(H.cout);
+    for (int s = 0; s < 2; ++s) {
+        cudaFree(H.db[s]);
+        cudaFree(H.dx[s]);
+        H.db[s] = H.dx[s] = nullptr;
+        for (cudaEvent_t *e : {&H.in_done[s], &H.solved[s], &H.out_done[s]})
+            if (*e) {
+                cudaEventDestroy(*e);
+                *e = nullptr;
+            }
+        H.used[s] = false;
+    }
+    D.bytes -= 4 * (long long)H.bytes;
+    H.bytes = 0;
+    if (H.cin) cudaStreamDestroy(H.cin);
+    if (H.cout) cudaStreamDestroy(H.cout);
+    H.cin = H.cout = nullptr;
+}
+
+int device_host_async(Plan &P, const double *b, double *x, int k, int ld, int prec, std::string &err) {
+    DeviceState &D = *P.dev;
+    DeviceState::HostPipe &H = D.pipe;
+    const size_t bytes = sizeof(double) * (size_t)ld * (size_t)k;
+    if (!H.cin) {
+        CK(cudaStreamCreateWithFlags(&H.cin, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&H.cout, cudaStreamNonBlocking));
+        for (int s = 0; s < 2; ++s) {
+            CK(cudaEventCreateWithFlags(&H.in_done[s], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&H.solved[s], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&H.out_done[s], cudaEventDisableTiming));
+        }
+    }
+    if (bytes > H.bytes) {  // wider than before: drain, then larger slots
+        CK(cudaStreamSynchronize(D.stream));
+        CK(cudaStreamSynchronize(H.cin));
+        CK(cudaStreamSynchronize(H.cout));
+        for (int s = 0; s < 2; ++s) {
+            cudaFree(H.db[s]);
+            cudaFree(H.dx[s]);
+            H.db[s] = H.dx[s] = nullptr;
+            H.used[s] = false;
+        }
+        D.bytes -= 4 * (long long)H.bytes;
+        H.bytes = 0;
+        int rc;
+        for (int s = 0; s < 2; ++s) {
+            if ((rc = alloc(D, H.db[s], bytes / sizeof(double), err))) return rc;
+            if ((rc = alloc(D, H.dx[s], bytes / sizeof(double), err))) return rc;
+        }
+        H.bytes = bytes + 256;
+    }
+    const int s = H.next;
+    H.next ^= 1;
+    const size_t nbytes = sizeof(double) * (size_t)P.n;
+    // the slot's previous solve has read db[s]; its previous download has read dx[s]
+    if (H.used[s]) {
+        CK(cudaStreamWaitEvent(H.cin, H.solved[s], 0));
+        CK(cudaStreamWaitEvent(D.stream, H.out_done[s], 0));
+    }
+    for (int c = 0; c < k; ++c)
+        CK(cudaMemcpyAsync(H.db[s] + (size_t)c * ld, b + (size_t)c * ld, nbytes, cudaMemcpyHostToDevice, H.cin));
+    CK(cudaEventRecord(H.in_done[s], H.cin));
+    CK(cudaStreamWaitEvent(D.stream, H.in_done[s], 0));
+    int rc = device_solve(P, H.db[s], H.dx[s], k, ld, prec, false, nullptr, err);
+    if (rc) return rc;
+    CK(cudaEventRecord(H.solved[s], D.stream));
+    CK(cudaStreamWaitEvent(H.cout, H.solved[s], 0));
+    for (int c = 0; c < k; ++c)
+        CK(cudaMemcpyAsync(x + (size_t)c * ld, H.dx[s] + (size_t)c * ld, nbytes, cudaMemcpyDeviceToHost, H.cout));
+    CK(cudaEventRecord(H.out_done[s], H.cout));
+    H.used[s] = true;
     return RBS_OK;
 }
 
@@ -1122,6 +1305,7 @@ void device_free(Plan &P) {
     if (!P.dev) return;
     DeviceState &D = *P.dev;
     if (D.stream) cudaStreamSynchronize(D.stream);
+    pipe_release(D);
     free_work(D);
     drop_graphs(D);
     for (auto &e : D.bev) cudaEventDestroy(e);
@@ -1144,9 +1328,9 @@ void device_free(Plan &P) {
     cudaFree(D.lc_queue);
     cudaFree(D.stage_b);
     cudaFree(D.stage_x);
-    void *ptrs[] = {D.rp, D.col, D.lvl, D.map, D.rows, D.perm, D.val, D.inv, D.val32, D.inv32,
+    void *ptrs[] = {D.rp, D.col, D.lvl, D.map, D.rows, D.perm, D.ipos, D.val, D.inv, D.val32, D.inv32,
                     D.full_rp, D.full_col, D.full_val, D.tickets, D.status, D.norms, D.band_coef,
-                    D.band_inv, D.band_coef32, D.band_inv32, D.band_maps, D.band_states};
+                    D.band_inv, D.band_coef32, D.band_inv32};
     for (void *p : ptrs) cudaFree(p);
     if (D.h_status) cudaFreeHost(D.h_status);
     if (D.h_norms) cudaFreeHost(D.h_norms);
@@ -1181,6 +1365,7 @@ int device_sync(Plan &P, std::string &err) {
     DeviceState &D = *P.dev;
     CK(cudaMemcpyAsync(D.h_status, D.status, sizeof(int), cudaMemcpyDeviceToHost, D.stream));
     CK(cudaStreamSynchronize(D.stream));
+    if (D.pipe.cout) CK(cudaStreamSynchronize(D.pipe.cout));  // asynchronous host-array solves' downloads
     if (*D.h_status & RBS_STATUS_TIMEOUT) {
         CK(cudaMemsetAsync(D.status, 0, sizeof(int), D.stream));
         // the solution work vectors may hold leftovers of the aborted solve

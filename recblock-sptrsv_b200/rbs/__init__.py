@@ -110,7 +110,7 @@ EXPORTS = [
     "rbs_sptrsv_csr_noalloc", "rbs_batch_analyse", "rbs_server_create", "rbs_server_add_factor",
     "rbs_server_submit", "rbs_server_submit_device", "rbs_server_wait", "rbs_server_stats_get", "rbs_server_reset_stats", "rbs_server_destroy",
     "rbs_plan_save", "rbs_plan_load", "rbs_ilu0_device", "rbs_mtx_read", "rbs_mtx_read_buffer", "rbs_mtx_info_get",
-    "rbs_mtx_csr", "rbs_mtx_triangle", "rbs_mtx_free", "rbs_mtx_write", "rbs_ic0_device", "rbs_plan_reserve",
+    "rbs_mtx_csr", "rbs_mtx_triangle", "rbs_mtx_free", "rbs_mtx_write", "rbs_ic0_device", "rbs_plan_reserve", "rbs_solve_host_async",
 ]
 
 MTX_REAL, MTX_INTEGER, MTX_PATTERN, MTX_COMPLEX = range(4)
@@ -182,6 +182,7 @@ def _load():
     lib.rbs_server_submit_device.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_longlong)]
     lib.rbs_plan_reserve.argtypes = [P, ctypes.c_int]
+    lib.rbs_solve_host_async.argtypes = [P, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.rbs_server_wait.argtypes = [P, ctypes.c_longlong, dp, ip]
     lib.rbs_server_stats_get.argtypes = [P, ctypes.POINTER(ServerStats)]
     lib.rbs_server_reset_stats.argtypes = [P]
@@ -283,6 +284,13 @@ class Plan:
         st = Stats()
         _check(lib.rbs_solve_host(self._h, _dp(b), _dp(x), k, self.n, prec, ctypes.byref(st)))
         return x, st
+
+    def solve_host_async(self, b: np.ndarray, x: np.ndarray, k: int = 1, prec: int = PREC_FP64):
+        """Enqueue a host-array solve (b, x: float64, (n,) or (k, n), ideally pinned, e.g. a
+        torch pin_memory tensor's .numpy()); b unchanged and x unread until sync()."""
+        assert b.flags.c_contiguous and x.flags.c_contiguous and b.dtype == np.float64 and x.dtype == np.float64
+        assert b.size >= k * self.n and x.size >= k * self.n
+        _check(lib.rbs_solve_host_async(self._h, _dp(b), _dp(x), k, self.n, prec))
 
     def profile(self, enable: bool = True):
         """Per-block CUDA-event timing of FP64/FP32 solves (resets the totals)."""

@@ -5,7 +5,7 @@ L_/U_preprocessing compiled from the reference sources by oracle/Makefile)
 on every case in cases.py, both directions, and writes
 tests/golden/<case>_<fwd|bwd>.npz with the inputs (unless regenerated from
 the seed) and every output.  Needs the reference sources; run here, not on
-a GPU box:  make -C oracle ref && python tests/golden/make_golden.py
+a GPU box:  make -C oracle ref REF=<reference recblock-sptrsv dir> && python tests/golden/make_golden.py
 """
 import hashlib
 import os
@@ -22,7 +22,7 @@ from oracle import oracle  # noqa: E402
 
 def main():
     if not os.path.exists(oracle.REF_DUMP):
-        sys.exit("oracle/_ref/ref_dump missing: run make -C oracle ref (needs the reference sources)")
+        sys.exit("oracle/_ref/ref_dump missing: run make -C oracle ref REF=<reference recblock-sptrsv dir>")
     with tempfile.TemporaryDirectory() as tmp:
         for name, spec in cases.CASES.items():
             for sub, tag in ((0, "fwd"), (1, "bwd")):

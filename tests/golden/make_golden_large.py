@@ -13,7 +13,7 @@ digests are committed.  Inputs come from the oracle's generator
 backward input = CSC of U = L^T = the CSR arrays of L.
 
 Needs the reference sources; run here, not on a GPU box:
-    make -C oracle ref && python tests/golden/make_golden_large.py
+    make -C oracle ref REF=<reference recblock-sptrsv dir> && python tests/golden/make_golden_large.py
 """
 import hashlib
 import json
@@ -53,7 +53,7 @@ def digest(a):
 
 def main():
     if not os.path.exists(oracle.REF_DUMP):
-        sys.exit("oracle/_ref/ref_dump missing: run make -C oracle ref (needs the reference sources)")
+        sys.exit("oracle/_ref/ref_dump missing: run make -C oracle ref REF=<reference recblock-sptrsv dir>")
     out = {}
     with tempfile.TemporaryDirectory() as tmp:
         for name, spec in LARGE.items():

@@ -6,7 +6,7 @@ the reader must take) and runs oracle/_ref/mtx_dump -- recblock-sptrsv's
 mmio_info + mmio_data compiled from the reference sources by oracle/Makefile
 -- on each, saving its CSR as tests/golden/mtx/<name>.npz.  Needs the
 reference sources; run here, not on a GPU box:
-    make -C oracle ref && python tests/golden/make_mtx_golden.py
+    make -C oracle ref REF=<reference recblock-sptrsv dir> && python tests/golden/make_mtx_golden.py
 """
 import os
 import sys
@@ -122,7 +122,7 @@ RANDOM = {
 
 def main():
     if not os.path.exists(oracle.MTX_REF_DUMP):
-        sys.exit("oracle/_ref/mtx_dump missing: run make -C oracle ref (needs the reference sources)")
+        sys.exit("oracle/_ref/mtx_dump missing: run make -C oracle ref REF=<reference recblock-sptrsv dir>")
     os.makedirs(OUT, exist_ok=True)
     for name, text in HAND.items():
         with open(os.path.join(OUT, name + ".mtx"), "w", newline="") as f:

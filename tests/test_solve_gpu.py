@@ -124,3 +124,49 @@ def test_device_analysis_entry(cuda):
     B, Xref = system(cp, ri, va, sub)
     X, _ = solve(plan, B, cuda)
     assert rel_err(X, Xref) <= TOL
+
+
+@pytest.mark.parametrize("sub", [rbs.FORWARD, rbs.BACKWARD])
+@pytest.mark.parametrize("grid", [64, 300])
+def test_multi_rhs_staged_level_triangles(cuda, grid, sub):
+    # 2D-Laplacian factors: their triangles run the staged level kernel with
+    # one CTA per group of right-hand-side columns (one column per CTA below
+    # 64 columns, two from 64 on); widths 8 and up also take the transposing
+    # gather and scatter.  Every column against the oracle, FP64 and mixed
+    # at 1e-12, FP32 at single precision.
+    rp, ci, va = rbs.gen_lower_csr(rbs.GEN_LAPLACE2D, grid=grid, seed=grid + sub)
+    cp, ri, cv = oracle.transpose(rp, ci, va) if sub == rbs.FORWARD else (rp, ci, va)
+    plan = rbs.analyse(cp, ri, cv, substitution=sub, lv=-1, opts=rbs.options(max_rhs=128))
+    kern = plan.export("kernel")
+    assert (kern[0::2] == rbs.K_LEVEL).sum() >= 1
+    for k in (2, 5, 8, 32, 64, 100, 128):
+        B, Xref = system(cp, ri, cv, sub, k=k, seed=7 * k)
+        for prec, tol in ((rbs.PREC_FP64, TOL), (rbs.PREC_MIXED, TOL), (rbs.PREC_FP32, 1e-5)):
+            X, _ = solve(plan, B, cuda, k=k, prec=prec)
+            for c in range(k):
+                assert rel_err(X[c], Xref[c]) <= tol, (k, prec, c)
+
+
+def test_host_async_pipelined(cuda):
+    # several asynchronous host-array solves in flight on two staging slots,
+    # pinned buffers, widths 1 and 3 (a wider call drains and regrows the
+    # slots), FP64 and FP32; mixed runs synchronously; all against the oracle
+    import torch
+    g, cp, ri, va, sub, lv = load_fixture("laplace40_lv2_fwd")
+    n = len(cp) - 1
+    plan = rbs.analyse(cp, ri, va, substitution=sub, lv=lv)
+    jobs = []
+    for q, (k, prec) in enumerate([(1, rbs.PREC_FP64)] * 4 + [(3, rbs.PREC_FP64), (1, rbs.PREC_FP32),
+                                                              (3, rbs.PREC_MIXED), (1, rbs.PREC_FP64)]):
+        B, Xref = system(cp, ri, va, sub, k=k, seed=100 + 10 * q)
+        hb = torch.empty(k * n, dtype=torch.float64, pin_memory=True)
+        hx = torch.full((k * n,), float("nan"), dtype=torch.float64, pin_memory=True)
+        hb.copy_(torch.from_numpy(np.ascontiguousarray(B).reshape(-1)))
+        plan.solve_host_async(hb.numpy(), hx.numpy(), k=k, prec=prec)
+        jobs.append((k, prec, Xref, hb, hx))
+    plan.sync()
+    for k, prec, Xref, hb, hx in jobs:
+        X = hx.numpy().reshape(k, n)
+        tol = 1e-5 if prec == rbs.PREC_FP32 else TOL
+        for c in range(k):
+            assert rel_err(X[c], Xref[c]) <= tol, (k, prec, c)
