@@ -191,6 +191,14 @@ typedef struct rbs_server_stats {
 int rbs_server_create(long long hbm_budget_bytes, int max_batch_rhs, rbs_server **server);
 /* On success the server owns the plan (freed by rbs_server_destroy). */
 int rbs_server_add_factor(rbs_server *server, rbs_plan *plan, int *factor_id);
+/* Several small factors served as one unit: batch_plan is the block-diagonal
+ * plan of rbs_batch_analyse over them, row_offsets its count + 1 offsets.
+ * Factor i of the group gets factor_ids[i] (its own n = row_offsets[i+1] -
+ * row_offsets[i]; requests use that n as their leading dimension); one
+ * launch serves queued requests of all members at once, column c carrying
+ * the c-th queued column of every member.  The server owns the plan. */
+int rbs_server_add_group(rbs_server *server, rbs_plan *batch_plan, int count, const int *row_offsets,
+                         int *factor_ids);
 /* b and x must stay valid until rbs_server_wait returns for the ticket. */
 int rbs_server_submit(rbs_server *server, int factor_id, const double *b, double *x, int k, int prec,
                       long long *ticket);

@@ -765,7 +765,7 @@ int analyse_host(Plan &P, const int *ptr, const int *idx, const double *val, int
 // BFS order and the labels -- computed by analyse_host above or on the
 // device (dev_analysis.cu).
 int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, const rbs_options &opt, std::string &err,
-                         const std::vector<int> *seg_rows) {
+                         const std::vector<int> *seg_rows, DevRows *dev_rows) {
     auto t0 = std::chrono::steady_clock::now();
     (void)nnz;
     P.opt = opt;
@@ -829,9 +829,24 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
     for (int b = 0; b < P.sum_block; ++b) rowcnt[b].assign((size_t)P.blocks[b].m, 0);
     std::vector<int> level((size_t)n, 0), reach((size_t)n);
     P.inv_diag.resize((size_t)n);
+    // (block, row) slots in block order, for the device path
+    std::vector<long long> slot_base((size_t)P.sum_block + 1, 0);
+    for (int b = 0; b < P.sum_block; ++b) slot_base[(size_t)b + 1] = slot_base[(size_t)b] + P.blocks[b].m;
+    constexpr int kRows = 1 << 14;
+    if (dev_rows) {
+        // counts, inverse diagonals, reach and local levels on the device (dev_pools.cu)
+        std::vector<int> flat;
+        int rc = dev_block_counts(*dev_rows, T, s, slot_base, flat, P.inv_diag, reach, err);
+        if (rc) return rc;
+        for (int b = 0; b < P.sum_block; ++b)
+            std::copy(flat.begin() + slot_base[(size_t)b], flat.begin() + slot_base[(size_t)b + 1], rowcnt[b].begin());
+        // chain-like graphs (the level search itself ran on the host): the
+        // recurrence below on the host, a dependency at a time on the device
+        // would cost an L2 round trip per row
+        if (T > 1 && P.device_bfs && (rc = dev_local_levels(*dev_rows, T, s, opt.spin_limit, level, err))) return rc;
+    } else
     // counts, inverse diagonals and the reach p - (first column) of every row
     // on host threads (row p owns row p of every block it meets) ...
-    constexpr int kRows = 1 << 14;
     parallel_for(((size_t)n + kRows - 1) / kRows, [&](size_t chunk) {
         for (int p = (int)chunk * kRows; p < std::min(n, (int)chunk * kRows + kRows); ++p) {
             int i = tri_of(p);
@@ -865,7 +880,7 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
     if (T == 1) {
         for (size_t L = 0; L + 1 < P.bfs_ptr.size(); ++L)
             std::fill(level.begin() + P.bfs_ptr[L], level.begin() + P.bfs_ptr[L + 1], (int)L);
-    } else {
+    } else if (!dev_rows || !P.device_bfs) {
         parallel_for((size_t)T, [&](size_t i) {
             const ExecBlock &TB = P.blocks[2 * i];
             for (int p = TB.r0; p < TB.r0 + TB.m; ++p) {
@@ -1019,9 +1034,12 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
             }
         }
     }
+    if (dev_rows) {  // the entry pools filled on the device
+        int rc = dev_pool_fill(*dev_rows, T, s, slot_base[(size_t)P.sum_block], ent, P.col_pool, P.val_pool, err);
+        if (rc) return rc;
+    } else {
     P.col_pool.resize((size_t)ent);
     P.val_pool.resize((size_t)ent);
-    {
         std::vector<std::vector<int>> cur((size_t)P.sum_block);
         for (int b = 0; b < P.sum_block; ++b) cur[b].assign(rowstart[b].begin(), rowstart[b].end() - 1);
         // row p owns row p of every block it meets: rows filled on host threads

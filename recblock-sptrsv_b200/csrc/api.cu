@@ -119,12 +119,15 @@ int rbs_analyse_device(const int *d_ptr, const int *d_idx, const double *d_val, 
     int rc;
     try {
         // validation, level sets, reordering and the processing-order CSR on
-        // the device; the execution layout on the host
+        // the device; then the block extraction and packing on the device
+        // (counts, local levels, entry pools) and the O(rows) layout steps
+        // on the host
         auto t0 = std::chrono::steady_clock::now();
-        rc = rbs::device_analyse(P->p, d_ptr, d_idx, d_val, n, nnz, fmt, substitution, err);
+        rbs::DevRows rows;
+        rc = rbs::device_analyse(P->p, d_ptr, d_idx, d_val, n, nnz, fmt, substitution, err, &rows);
         P->p.analyse_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         P->p.device_analyse_ms = P->p.analyse_ms;
-        if (rc == RBS_OK) rc = rbs::analyse_after_levels(P->p, n, nnz, substitution, lv, o, err);
+        if (rc == RBS_OK) rc = rbs::analyse_after_levels(P->p, n, nnz, substitution, lv, o, err, nullptr, &rows);
         if (rc == RBS_OK && !o.host_only) rc = rbs::device_build(P->p, err);
         if (rc == RBS_OK && !o.host_only && o.select == RBS_SELECT_TUNE) rc = rbs::device_tune(P->p, err);
     } catch (const std::bad_alloc &) {

@@ -395,7 +395,7 @@ int exclusive_sum(Buf &buf, const int *in, int *out, long long count, cudaStream
 // device; results land in the plan's host arrays (in_*, bfs_*, nlevel,
 // label, perm, full_*, dev_reorder_*) for the host layout step.
 int device_analyse(Plan &P, const int *d_ptr, const int *d_idx, const double *d_val, int n, int nnz, int fmt,
-                   int substitution, std::string &err) {
+                   int substitution, std::string &err, DevRows *keep) {
     cudaStream_t st = nullptr;
     DCK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     struct StreamGuard {
@@ -608,9 +608,23 @@ int device_analyse(Plan &P, const int *d_ptr, const int *d_idx, const double *d_
     DCK(buf.get(idx, (size_t)nnz));
     DCK(buf.get(keys_sorted, (size_t)nnz));
     DCK(buf.get(idx_sorted, (size_t)nnz));
-    DCK(buf.get(fcol, (size_t)nnz));
-    DCK(buf.get(fval, (size_t)nnz));
-    DCK(buf.get(frp, (size_t)n + 1));
+    if (keep) {  // the processing-order CSR outlives this function, owned by *keep
+        DCK(cudaStreamCreateWithFlags(&keep->st, cudaStreamNonBlocking));
+        keep->pool = buf.pool;
+        keep->n = n;
+        keep->nnz = nnz;
+        void *q;
+        DCK(cudaMallocFromPoolAsync(&q, sizeof(int) * std::max<size_t>((size_t)nnz, 1), buf.pool, st));
+        keep->fcol = fcol = (int *)q;
+        DCK(cudaMallocFromPoolAsync(&q, sizeof(double) * std::max<size_t>((size_t)nnz, 1), buf.pool, st));
+        keep->fval = fval = (double *)q;
+        DCK(cudaMallocFromPoolAsync(&q, sizeof(int) * ((size_t)n + 1), buf.pool, st));
+        keep->frp = frp = (int *)q;
+    } else {
+        DCK(buf.get(fcol, (size_t)nnz));
+        DCK(buf.get(fval, (size_t)nnz));
+        DCK(buf.get(frp, (size_t)n + 1));
+    }
     DCK(buf.get(rowcnt, (size_t)n + 1));
     k_labels<<<grid_of(n, TPB), TPB, 0, st>>>(item, n, fwd, label, pos);
     int rc;

@@ -78,6 +78,12 @@ __device__ __forceinline__ VT finalize(VT v) {
     return Sent<VT>::is(v) ? Sent<VT>::nan() : v;
 }
 
+// N values of type T moved as one aligned access
+template <typename T, int N>
+struct alignas(sizeof(T) * N) Vec {
+    T v[N];
+};
+
 // ---------------------------------------------------------------------------
 // Vector permutations (utils_cuda.h:858-876 levelset_reordering_vecb/vecx,
 // fused with the RHS interleave, the precision cast and the sentinel reset).
@@ -137,33 +143,110 @@ __global__ void k_scatter_cols(VT *__restrict__ xw, const int *__restrict__ perm
 }
 
 // Transposing forms of the gather and scatter for many right-hand sides
-// (K >= 8): a CTA takes a tile of 32 original rows, reads it column by
-// column (32 consecutive values of a column: coalesced), and writes every
-// row at its processing position (K consecutive values: coalesced), through
-// a shared-memory tile; the scatter runs the other way.  Columns come from
-// b + c*ld, or from the table cols[c] when cols is not NULL.  ipos[i] is the
-// processing position of original row i.
+// (K >= 8, or any K for the grouped layout): a CTA takes a tile of 32
+// original rows, reads it column by column (32 consecutive values of a
+// column: coalesced), and writes every row at its processing position (K
+// consecutive values: coalesced), through a shared-memory tile; the scatter
+// runs the other way.  Columns come from b + c*ld, or from the table cols[c]
+// when cols is not NULL.  ipos[i] is the processing position of original row
+// i.  GL = 0: row-interleaved work vector (entry (p, c) at p*K + c); GL > 0:
+// grouped (column group c / GL holds its rows contiguously, GL values each:
+// entry at (c / GL)*n*GL + p*GL + c % GL).
 constexpr int TP_ROWS = 32;
 
-template <typename VT, typename VT2, int K>
+template <int K, int GL>
+__device__ __forceinline__ long long work_index(long long p, int c, int n) {
+    if constexpr (GL == 0) return p * K + c;
+    else return (long long)(c / GL) * n * GL + p * GL + (c % GL);
+}
+
+// Columns of several independent systems solved as one block-diagonal plan
+// (a server group): column c of system f comes from tab[c*F + f] (NULL: no
+// request there, zeros in, nothing out); seg[i] is the system of original
+// row i, off[f] its first row.
+struct GroupCols {
+    const double *const *tab;
+    const int *seg, *off;
+    int F;
+};
+
+__device__ __forceinline__ const double *group_src(const GroupCols &g, int c, long long i, long long &r) {
+    const int f = g.seg[i];
+    r = i - g.off[f];
+    return g.tab[(long long)c * g.F + f];
+}
+
+template <typename VT, typename VT2, int K, int GL = 0>
 __global__ void __launch_bounds__(256) k_gather_t(const double *__restrict__ b, int ld,
                                                   const double *const *__restrict__ cols, int k,
                                                   const int *__restrict__ ipos, int n, VT *__restrict__ out,
-                                                  VT2 *__restrict__ out2) {
+                                                  VT2 *__restrict__ out2, GroupCols grp) {
     __shared__ double tile[K][TP_ROWS + 1];
     for (long long i0 = (long long)blockIdx.x * TP_ROWS; i0 < n; i0 += (long long)gridDim.x * TP_ROWS) {
         const int rows = (int)min((long long)TP_ROWS, n - i0);
         for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
             const int c = e / TP_ROWS, t = e % TP_ROWS;
             double v = 0.0;
-            if (c < k && t < rows) v = cols ? cols[c][i0 + t] : b[(long long)c * ld + i0 + t];
+            if (c < k && t < rows) {
+                if (grp.tab) {
+                    long long r;
+                    const double *src = group_src(grp, c, i0 + t, r);
+                    if (src) v = src[r];
+                } else {
+                    v = cols ? cols[c][i0 + t] : b[(long long)c * ld + i0 + t];
+                }
+            }
             tile[c][t] = v;
         }
         __syncthreads();
         for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
             const int t = e / K, c = e % K;
             if (t < rows) {
-                const long long o = (long long)ipos[i0 + t] * K + c;
+                const long long o = work_index<K, GL>(ipos[i0 + t], c, n);
+                out[o] = (VT)tile[c][t];
+                if (out2) out2[o] = (VT2)tile[c][t];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Grouped layout (GL > 0): tiles of 32 consecutive PROCESSING positions, so
+// each column group's 32 rows are written as one contiguous run of 32*GL
+// values; the right-hand-side values are read at the rows' original
+// positions perm[p] (single values, read-only).
+template <typename VT, typename VT2, int K, int GL>
+__global__ void __launch_bounds__(256) k_gather_p(const double *__restrict__ b, int ld,
+                                                  const double *const *__restrict__ cols, int k,
+                                                  const int *__restrict__ perm, int n, VT *__restrict__ out,
+                                                  VT2 *__restrict__ out2, GroupCols grp) {
+    static_assert(GL > 0 && K % GL == 0, "grouped layout");
+    __shared__ double tile[K][TP_ROWS + 1];
+    for (long long p0 = (long long)blockIdx.x * TP_ROWS; p0 < n; p0 += (long long)gridDim.x * TP_ROWS) {
+        const int rows = (int)min((long long)TP_ROWS, n - p0);
+        for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
+            const int c = e / TP_ROWS, t = e % TP_ROWS;
+            double v = 0.0;
+            if (c < k && t < rows) {
+                const long long i = perm[p0 + t];
+                if (grp.tab) {
+                    long long r;
+                    const double *src = group_src(grp, c, i, r);
+                    if (src) v = src[r];
+                } else {
+                    v = cols ? cols[c][i] : b[(long long)c * ld + i];
+                }
+            }
+            tile[c][t] = v;
+        }
+        __syncthreads();
+        // group g's rows p0.. p0+rows-1: GL values each, contiguous
+        for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
+            const int g = e / (TP_ROWS * GL), rest = e % (TP_ROWS * GL);
+            const int t = rest / GL, j = rest % GL;
+            if (t < rows) {
+                const int c = g * GL + j;
+                const long long o = (long long)g * n * GL + (p0 + t) * GL + j;
                 out[o] = (VT)tile[c][t];
                 if (out2) out2[o] = (VT2)tile[c][t];
             }
@@ -173,16 +256,17 @@ __global__ void __launch_bounds__(256) k_gather_t(const double *__restrict__ b, 
 }
 
 // RESET: the work vector is set back to the sentinel as it is read.
-template <typename VT, int K, bool RESET>
+template <typename VT, int K, bool RESET, int GL = 0>
 __global__ void __launch_bounds__(256) k_scatter_t(VT *__restrict__ xw, const int *__restrict__ ipos, int n, int k,
-                                                   double *__restrict__ x, int ld, double *const *__restrict__ cols) {
+                                                   double *__restrict__ x, int ld, double *const *__restrict__ cols,
+                                                   GroupCols grp) {
     __shared__ double tile[K][TP_ROWS + 1];
     for (long long i0 = (long long)blockIdx.x * TP_ROWS; i0 < n; i0 += (long long)gridDim.x * TP_ROWS) {
         const int rows = (int)min((long long)TP_ROWS, n - i0);
         for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
             const int t = e / K, c = e % K;
             if (t < rows) {
-                const long long o = (long long)ipos[i0 + t] * K + c;
+                const long long o = work_index<K, GL>(ipos[i0 + t], c, n);
                 tile[c][t] = (double)xw[o];
                 if (RESET) xw[o] = Sent<VT>::value();
             }
@@ -191,8 +275,15 @@ __global__ void __launch_bounds__(256) k_scatter_t(VT *__restrict__ xw, const in
         for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
             const int c = e / TP_ROWS, t = e % TP_ROWS;
             if (c < k && t < rows) {
-                if (cols) cols[c][i0 + t] = tile[c][t];
-                else x[(long long)c * ld + i0 + t] = tile[c][t];
+                if (grp.tab) {
+                    long long r;
+                    double *dst = const_cast<double *>(group_src(grp, c, i0 + t, r));
+                    if (dst) dst[r] = tile[c][t];
+                } else if (cols) {
+                    cols[c][i0 + t] = tile[c][t];
+                } else {
+                    x[(long long)c * ld + i0 + t] = tile[c][t];
+                }
             }
         }
         __syncthreads();
@@ -410,6 +501,8 @@ __global__ void __launch_bounds__(256) k_spmv_sub(const int *__restrict__ rp, co
         }
         if (K == 1) {
             VT sum = 0;
+            // unrolled: several column loads issue before their x gathers (same summation order)
+#pragma unroll 4
             for (int k = s + sl; k < e; k += g) sum += val[k] * x[col[k]];
             for (int off = g >> 1; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off, g);
             if (active && sl == 0 && e > s) b[row] -= sum;
@@ -447,6 +540,7 @@ __global__ void __launch_bounds__(256) k_spmv_rows(const int *__restrict__ rp, c
         const int i = pos[t];
         const int s = rp[i], e = rp[i + 1];
         VT sum = 0;
+#pragma unroll 4
         for (int k = s + lane; k < e; k += 32) sum += val[k] * x[col[k]];
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
@@ -575,6 +669,126 @@ __global__ void k_scatter64_cols(const double *__restrict__ x64, const int *__re
     for (; t < total; t += (long long)gridDim.x * blockDim.x) {
         const int p = (int)(t / K), c = (int)(t % K);
         if (c < k) cols[c][perm[p]] = x64[t];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Grouped work vectors (column group g of G columns: its rows contiguous, G
+// values each; groups gstride elements apart).  Pointers are those of group
+// 0 at the block's first row (or column).
+// ---------------------------------------------------------------------------
+template <typename VT, int G>
+__global__ void k_tri_diag_grp(const VT *__restrict__ inv, const VT *__restrict__ b, VT *x, int m, int ngroups,
+                               long long gstride) {
+    const long long per = (long long)m * G, total = per * ngroups;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long g = t / per, rest = t - g * per;
+        const long long o = g * gstride + rest;
+        x[o] = finalize(b[o] * inv[rest / G]);
+    }
+}
+
+// b[rows] -= S x[cols]: one thread per (row, group), consecutive threads on
+// consecutive rows of one group.
+template <typename VT, int G>
+__global__ void __launch_bounds__(256) k_spmv_sub_grp(const int *__restrict__ rp, const int *__restrict__ col,
+                                                      const VT *__restrict__ val, const int *__restrict__ rows,
+                                                      int nrows, int ngroups, long long gstride,
+                                                      const VT *__restrict__ x, VT *b) {
+    using VG = Vec<VT, G>;
+    const long long total = (long long)nrows * ngroups;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long g = t / nrows;
+        const int i = (int)(t - g * nrows);
+        const int s = rp[i], e = rp[i + 1];
+        if (e == s) continue;
+        const int row = rows ? rows[i] : i;
+        const VT *xg = x + g * gstride;
+        VT acc[G];
+#pragma unroll
+        for (int j = 0; j < G; ++j) acc[j] = 0;
+        for (int k = s; k < e; ++k) {
+            const VT v = val[k];
+            const VG xv = *reinterpret_cast<const VG *>(xg + (long long)col[k] * G);
+#pragma unroll
+            for (int j = 0; j < G; ++j) acc[j] += v * xv.v[j];
+        }
+        VG *bp = reinterpret_cast<VG *>(b + g * gstride + (long long)row * G);
+        VG bv = *bp;
+#pragma unroll
+        for (int j = 0; j < G; ++j) bv.v[j] -= acc[j];
+        *bp = bv;
+    }
+}
+
+// Mixed precision, grouped: r32 = (float)(b - A x), one thread per (row, group).
+template <int G>
+__global__ void __launch_bounds__(256) k_residual_grp(const int *__restrict__ rp, const int *__restrict__ col,
+                                                      const double *__restrict__ val, const double *__restrict__ x,
+                                                      const double *__restrict__ b, float *__restrict__ r32, int n,
+                                                      int ngroups, long long gstride) {
+    using VG = Vec<double, G>;
+    const long long total = (long long)n * ngroups;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long g = t / n;
+        const int row = (int)(t - g * n);
+        const double *xg = x + g * gstride;
+        double acc[G];
+#pragma unroll
+        for (int j = 0; j < G; ++j) acc[j] = 0;
+        for (int k = rp[row]; k < rp[row + 1]; ++k) {
+            const double v = val[k];
+            const VG xv = *reinterpret_cast<const VG *>(xg + (long long)col[k] * G);
+#pragma unroll
+            for (int j = 0; j < G; ++j) acc[j] += v * xv.v[j];
+        }
+        const long long o = g * gstride + (long long)row * G;
+        const VG bv = *reinterpret_cast<const VG *>(b + o);
+#pragma unroll
+        for (int j = 0; j < G; ++j) r32[o + j] = (float)(bv.v[j] - acc[j]);
+    }
+}
+
+// Mixed precision, grouped: x64 (+)= d32, d32 reset to the sentinel, per-column
+// sums of squares into norms[2*K].  Column c = blockIdx.y.
+template <int K, int G>
+__global__ void __launch_bounds__(256) k_update_grp(double *__restrict__ x64, float *__restrict__ d32, int n,
+                                                    int first, double *__restrict__ norms) {
+    __shared__ double red[2][8];
+    const int c = blockIdx.y;
+    const long long base = (long long)(c / G) * n * G + (c % G);
+    double dd = 0, xx = 0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const long long o = base + p * G;
+        const double d = (double)d32[o];
+        const double xn = first ? d : x64[o] + d;
+        x64[o] = xn;
+        d32[o] = __uint_as_float(RBS_SENT32);
+        dd += d * d;
+        xx += xn * xn;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        dd += __shfl_down_sync(0xffffffffu, dd, off);
+        xx += __shfl_down_sync(0xffffffffu, xx, off);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red[0][w] = dd;
+        red[1][w] = xx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, z = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+            a += red[0][q];
+            z += red[1][q];
+        }
+        atomicAdd(&norms[c], a);
+        atomicAdd(&norms[K + c], z);
     }
 }
 

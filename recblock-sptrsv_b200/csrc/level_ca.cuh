@@ -19,14 +19,16 @@
 // Dependencies within the last XW rows come from the window; older ones
 // from x in global memory (written by this CTA before an earlier barrier).
 //
-// Several right-hand sides: the work vectors are row-interleaved with a row
-// stride ld (entry (row, column c) at v[row*ld + c]); CTA y of the launch's
-// second grid dimension solves the G consecutive columns [y*G, y*G+G) on its
-// own, with no synchronisation between CTAs: every column group walks the
-// same levels with its own window (G values per slot), and the rows' columns,
-// values and inverse diagonal, which all groups share, come through L2.  One
-// dependency walk per group serves G columns; the groups run side by side
-// on separate SMs.
+// Several right-hand sides: CTA y of the launch's second grid dimension
+// solves the G consecutive columns [y*G, y*G+G) on its own, with no
+// synchronisation between CTAs: every column group walks the same levels
+// with its own window (G values per slot), and the rows' columns, values and
+// inverse diagonal, which all groups share, come through L2.  One dependency
+// walk per group serves G columns; the groups run side by side on separate
+// SMs.  The work vectors are either row-interleaved (entry (row, c) at
+// row*K + c: ld = K, groups G apart) or grouped (each group's rows
+// contiguous, G values per row: ld = G, groups n*G apart), where a thread's
+// G values sit next to its neighbours' and a warp's copies coalesce.
 #pragma once
 
 #include <type_traits>
@@ -44,10 +46,11 @@ struct CaDesc {
     const int *col;   // row-major level-ELL columns (block-local), padding -1
     const void *val;  // level-ELL values
     const void *inv;  // inverse diagonal of the block's rows
-    const void *b;    // right-hand side of the block's rows (row stride ld)
-    void *x;          // solution of the block's rows (row stride ld)
+    const void *b;    // right-hand side of the block's rows, column group 0 (row stride ld)
+    void *x;          // solution of the block's rows, column group 0 (row stride ld)
     const int *lvl;   // per level: lo, off, w, 0 (4 ints), then {m, 0, 0, 0}
     int m, nlv, ld, pad1;
+    long long gstride;  // elements from one column group to the next
 };
 
 template <typename VT, int W, int S, int G = 1>
@@ -71,6 +74,12 @@ __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+// Levels ahead at which a multi-column launch pulls a row's data into L2:
+// with many right-hand sides the work vectors outgrow L2, and the staged
+// copies (S-1 levels ahead) would wait on HBM instead.
+constexpr int CA_PF = 12;
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
@@ -102,19 +111,16 @@ __device__ __forceinline__ void cp_async_sn(unsigned dst, const void *src) {
     }
 }
 
-template <typename T, int N>
-struct alignas(sizeof(T) * N) Vec {
-    T v[N];
-};
 
 // The level loop is unrolled by the stage count S, so every stage address
 // is a compile-time offset from per-thread bases computed once.
 // WIN: the block's columns are window slots (every dependency within the
 // window; padding reads the zero slot), so a dependency is one shared-memory
 // load and an unconditional multiply-add.
-// G: right-hand sides per CTA (blockIdx.y selects the column group); for
-// G == 1 and d.ld == 1 this is the single right-hand-side solve.
-template <typename VT, int W, int S, bool WIN, int G = 1>
+// G: right-hand sides per CTA (blockIdx.y selects the column group).
+// MC: a multi-column launch; without it the row stride is 1 and there is
+// one group (the single right-hand-side solve, with no stride arithmetic).
+template <typename VT, int W, int S, bool WIN, int G = 1, bool MC = false>
 __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict__ descs) {
     using Lay = CaLayout<VT, W, S, G>;
     using VG = Vec<VT, G>;
@@ -122,8 +128,10 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
     static_assert(G == 1 || G == 2 || G == 4, "1, 2 or 4 right-hand sides per CTA");
     extern __shared__ __align__(128) unsigned char sm[];
     const CaDesc d = descs[blockIdx.x];
-    const int ld = d.ld, j0 = blockIdx.y * G;
-    VT *x = (VT *)d.x + j0;
+    static_assert(MC || G == 1, "one column per CTA without a multi-column launch");
+    const int ld = MC ? d.ld : 1;
+    const long long goff = MC ? (long long)blockIdx.y * d.gstride : 0;
+    VT *x = (VT *)d.x + goff;
     VG *xs = reinterpret_cast<VG *>(sm + Lay::xw_off);
     int *tab = reinterpret_cast<int *>(sm + Lay::tab_off);
     const int tid = threadIdx.x;
@@ -145,7 +153,7 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
     const int *colp = d.col + tid * W;
     const VT *valp = (const VT *)d.val + tid * W;
     const VT *inv_t = (const VT *)d.inv + tid;
-    const VT *b_t = (const VT *)d.b + (size_t)tid * ld + j0;
+    const VT *b_t = (const VT *)d.b + goff + (size_t)tid * ld;
     const unsigned s0 = (unsigned)__cvta_generic_to_shared(sm);
     const unsigned s_col = s0 + tid * W * 4;
     const unsigned s_val = s0 + (unsigned)Lay::col_bytes + tid * W * (unsigned)sizeof(VT);
@@ -180,6 +188,15 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
         const int4 e_stage = ent[(U + S - 1) % S];
         if (l + S <= nlv) ent[U] = lt[l + S];  // level l's own entry is no longer needed
         stage(l + S - 1, e_stage, std::integral_constant<int, (U + S - 1) % S>{});
+        if (MC && l + CA_PF < nlv) {  // several column groups: this thread's row CA_PF levels on
+            const int4 ep = lt[l + CA_PF];
+            if (tid < ep.z) {
+                prefetch_l2(b_t + (size_t)ep.x * ld);
+                prefetch_l2(colp + ep.y);
+                prefetch_l2(valp + ep.y);
+                prefetch_l2(inv_t + ep.x);
+            }
+        }
         cp_async_wait<S - 1>();
         if (tid < hi - lo) {
             const unsigned char *st = sm + (size_t)U * Lay::stage_bytes;

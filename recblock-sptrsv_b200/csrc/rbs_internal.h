@@ -252,17 +252,46 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
                      bool &is_double, std::string &err);
 int auto_lv(int m, int device_id);
 
+// The processing-order CSR that device_analyse leaves on the device for the
+// block extraction on the device (dev_pools.cu), with that step's buffers.
+// The memory comes from the per-device pool and is released, stream-ordered,
+// with the object.
+struct DevRows {
+    cudaStream_t st = nullptr;
+    cudaMemPool_t pool = nullptr;
+    int *frp = nullptr, *fcol = nullptr;
+    double *fval = nullptr;
+    int *rowcnt = nullptr, *status = nullptr;
+    long long *slot_base = nullptr;
+    int n = 0, nnz = 0, sms = 148;
+    DevRows() = default;
+    DevRows(const DevRows &) = delete;
+    DevRows &operator=(const DevRows &) = delete;
+    ~DevRows();
+};
+
 // dev_analysis.cu: validation, findlevel, reordering and the processing-order
-// CSR on the device (fills in_*, bfs_*, nlevel, label, perm, full_*, dev_reorder_*)
+// CSR on the device (fills in_*, bfs_*, nlevel, label, perm, full_*,
+// dev_reorder_*); with keep, the processing-order CSR also stays on the
+// device in *keep
 int device_analyse(Plan &P, const int *d_ptr, const int *d_idx, const double *d_val, int n, int nnz, int fmt,
-                   int substitution, std::string &err);
+                   int substitution, std::string &err, DevRows *keep = nullptr);
+// dev_pools.cu: per (block, row) entry counts (blocks in order, slot_base[b]
+// = first slot of block b), inverse diagonal and reach of every row
+int dev_block_counts(DevRows &R, int T, int s, const std::vector<long long> &slot_base, std::vector<int> &rowcnt,
+                     std::vector<double> &inv_diag, std::vector<int> &reach, std::string &err);
+// dev_pools.cu: local levels of the triangles (T > 1)
+int dev_local_levels(DevRows &R, int T, int s, long long spin_limit, std::vector<int> &level, std::string &err);
+// dev_pools.cu: the entry pools (col_pool, val_pool) from the counts
+int dev_pool_fill(DevRows &R, int T, int s, long long slots, long long entries, bulk_vector<int> &col_pool,
+                  bulk_vector<double> &val_pool, std::string &err);
 // analysis.cpp: findlevel's breadth-first search on the host (levelPtr, levelItem;
 // returns the level count or -1 when stuck)
 int host_bfs_levels(const int *cp, const int *ri, int m, std::vector<int> &levelPtr, std::vector<int> &item);
 // analysis.cpp: the layout steps after the level sets, from the fields
 // device_analyse filled
 int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, const rbs_options &opt, std::string &err,
-                         const std::vector<int> *seg_rows = nullptr);
+                         const std::vector<int> *seg_rows = nullptr, DevRows *dev_rows = nullptr);
 
 // ilu0.cu: ILU(0) of a device CSR matrix into d_lu (A's pattern)
 int device_ilu0(const int *d_rp, const int *d_ci, const double *d_val, int n, int nnz, double *d_lu,
@@ -325,8 +354,19 @@ int device_reserve(Plan &P, int k, std::string &err);
 // written).  After start, and after every next that sets *more, the caller
 // waits for the stream and calls next again while *more is set (mixed
 // refinement: one correction per call); then finish reports the status.
+// The systems of a block-diagonal plan (rbs_batch_analyse) served as one
+// unit: column c of system f reads btab[c*count + f] and writes
+// xtab[c*count + f] (device tables; NULL: no request, zeros in and nothing
+// out); seg[i] is the system of original row i and off[f] its first row
+// (device arrays).  With it, device_batch_start ignores bcols / xcols.
+struct BatchGroup {
+    const double *const *btab;
+    double *const *xtab;
+    const int *seg, *off;
+    int count;
+};
 int device_batch_start(Plan &P, const double *const *bcols, double *const *xcols, int k, int prec, int *more,
-                       std::string &err);
+                       std::string &err, const BatchGroup *grp = nullptr);
 int device_batch_next(Plan &P, int *more, std::string &err);
 int device_batch_finish(Plan &P, int *iters, double *corr, std::string &err);
 double block_bytes(const Plan &P, const ExecBlock &B);

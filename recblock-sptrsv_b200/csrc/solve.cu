@@ -101,6 +101,7 @@ struct DeviceState {
     int bat_K = 0, bat_k = 0, bat_prec = 0, bat_iters = 0;
     double bat_corr = 0;
     double *const *bat_xcols = nullptr;
+    GroupCols bat_gx{};  // the batch's solution tables when it spans the systems of a block-diagonal plan
     // captured block walks per (precision, K, profiling)
     bool use_graphs = true;
     std::map<long long, cudaGraphExec_t> graphs;
@@ -338,13 +339,13 @@ int ell_descs(Plan &P, CsfDesc *&out, std::string &err) {
     return RBS_OK;
 }
 
-template <typename VT, int W, int S, int G = 1>
+template <typename VT, int W, int S, int G = 1, bool MC = false>
 int ca_attr(std::string &err) {
     static std::atomic<unsigned long long> done{0};
     if (!attr_done(done)) {
-        CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, false, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, false, G, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)CaLayout<VT, W, S, G>::total));
-        CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, true, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, true, G, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)CaLayout<VT, W, S, G>::total));
         attr_mark(done);
     }
@@ -361,25 +362,42 @@ template <typename VT> constexpr int ca_stages(int W, int G) {
 }
 
 // Right-hand sides per CTA of a staged level triangle solved for K columns:
-// one CTA per column keeps every group's dependency walk as short as the
-// single right-hand side's; two per CTA halve the shared row data the groups
-// pull through L2 when there are many groups.  RBS_CA_GROUP (1 or 2)
-// overrides the choice.
+// the column groups all read the same row data (columns, values, inverse
+// diagonal) at about the same time, and their waits on L2 grow with their
+// number, so two columns per CTA (half the groups) measured faster than one
+// at 8 and 32 columns and the same at 128.  RBS_CA_GROUP (1 or 2) overrides
+// the choice.
 template <typename VT> int ca_group(const ExecBlock &B, int K) {
     if (K == 1) return 1;
     static const int forced = [] {
         const char *e = std::getenv("RBS_CA_GROUP");
         return e ? std::atoi(e) : 0;
     }();
-    int G = forced == 1 || forced == 2 ? forced : (K >= 64 ? 2 : 1);
+    int G = forced == 1 || forced == 2 ? forced : 2;
     if (G == 2 && ca_stages<VT>(B.ca_w, 2) == 0) G = 1;
     return G;
 }
 
+// Layout of a K-column solve's work vectors: 0 = row-interleaved (entry
+// (p, c) at p*K + c), G > 0 = grouped by column groups of G (group c/G's
+// rows contiguous, G values each), taken when every triangle is a staged
+// level triangle or diagonal-only, so that each CTA's copies coalesce; G is
+// then the plan's columns per CTA.
+template <typename VT> int plan_group(const Plan &P, int K) {
+    if (K == 1) return 0;
+    int G = 2;
+    for (const ExecBlock &B : P.blocks) {
+        if (!B.tri || B.nnz == B.m) continue;
+        if (B.kernel != RBS_K_LEVEL || !B.ca_ok) return 0;
+        G = std::min(G, ca_group<VT>(B, K));
+    }
+    return G;
+}
+
 template <typename VT>
-int ca_descs(Plan &P, CaDesc *&out, int K, std::string &err) {
+int ca_descs(Plan &P, CaDesc *&out, int K, int GL, std::string &err) {
     DeviceState &D = *P.dev;
-    const long long key = (long long)K * 2 + (sizeof(VT) == 8 ? 0 : 1);
+    const long long key = ((long long)K * 2 + (sizeof(VT) == 8 ? 0 : 1)) * 4 + GL;
     auto it = D.ca_cache.find(key);
     if (it != D.ca_cache.end()) {
         out = it->second;
@@ -392,12 +410,14 @@ int ca_descs(Plan &P, CaDesc *&out, int K, std::string &err) {
         d.col = D.ca_col + B.ca_lo;
         d.val = Pools<VT>::cav(D) + B.ca_lo;
         d.inv = Pools<VT>::inv(D) + B.r0;
-        d.b = Pools<VT>::bw(D) + (long long)B.r0 * K;
-        d.x = Pools<VT>::xw(D) + (long long)B.r0 * K;
+        const long long rowlen = GL ? GL : K;  // values per row within a column group's rows
+        d.b = Pools<VT>::bw(D) + (long long)B.r0 * rowlen;
+        d.x = Pools<VT>::xw(D) + (long long)B.r0 * rowlen;
         d.lvl = D.ca_tab + B.ca_tab_off;
         d.m = B.m;
         d.nlv = B.nlv;
-        d.ld = K;
+        d.ld = (int)rowlen;
+        d.gstride = GL ? (long long)P.n * GL : ca_group<VT>(B, K);
         h.push_back(d);
     }
     CaDesc *dd = nullptr;
@@ -408,11 +428,14 @@ int ca_descs(Plan &P, CaDesc *&out, int K, std::string &err) {
     int rc;
     if ((rc = ca_attr<VT, 1, 4>(err)) || (rc = ca_attr<VT, 2, 4>(err)) || (rc = ca_attr<VT, 4, 2>(err))) return rc;
     if (K > 1) {
+        if ((rc = ca_attr<VT, 1, 4, 1, true>(err)) || (rc = ca_attr<VT, 2, 4, 1, true>(err)) ||
+            (rc = ca_attr<VT, 4, 2, 1, true>(err)))
+            return rc;
         if constexpr (sizeof(VT) == 8) {
-            if ((rc = ca_attr<VT, 1, 2, 2>(err)) || (rc = ca_attr<VT, 2, 2, 2>(err))) return rc;
+            if ((rc = ca_attr<VT, 1, 2, 2, true>(err)) || (rc = ca_attr<VT, 2, 2, 2, true>(err))) return rc;
         } else {
-            if ((rc = ca_attr<VT, 1, 4, 2>(err)) || (rc = ca_attr<VT, 2, 4, 2>(err)) ||
-                (rc = ca_attr<VT, 4, 2, 2>(err)))
+            if ((rc = ca_attr<VT, 1, 4, 2, true>(err)) || (rc = ca_attr<VT, 2, 4, 2, true>(err)) ||
+                (rc = ca_attr<VT, 4, 2, 2, true>(err)))
                 return rc;
         }
     }
@@ -421,30 +444,33 @@ int ca_descs(Plan &P, CaDesc *&out, int K, std::string &err) {
 
 // One staged level triangle: one thread per row of the widest level, one
 // CTA per group of G right-hand sides.
-template <typename VT, int W, int S, int G>
+template <typename VT, int W, int S, int G, bool MC>
 void launch_ca(const ExecBlock &B, const CaDesc *desc, int K, cudaStream_t st) {
     const int nt = std::min(1024, std::max(32, (B.maxwidth + 31) / 32 * 32));
     const dim3 grid(1, K / G);
     if (B.ca_win)
-        k_tri_level_ca<VT, W, S, true, G><<<grid, nt, CaLayout<VT, W, S, G>::total, st>>>(desc);
+        k_tri_level_ca<VT, W, S, true, G, MC><<<grid, nt, CaLayout<VT, W, S, G>::total, st>>>(desc);
     else
-        k_tri_level_ca<VT, W, S, false, G><<<grid, nt, CaLayout<VT, W, S, G>::total, st>>>(desc);
+        k_tri_level_ca<VT, W, S, false, G, MC><<<grid, nt, CaLayout<VT, W, S, G>::total, st>>>(desc);
 }
 
 template <typename VT>
-void launch_ca_any(const ExecBlock &B, const CaDesc *desc, int K, cudaStream_t st) {
-    const int G = ca_group<VT>(B, K);
-    if (G == 1) {
-        if (B.ca_w == 1) launch_ca<VT, 1, 4, 1>(B, desc, K, st);
-        else if (B.ca_w == 2) launch_ca<VT, 2, 4, 1>(B, desc, K, st);
-        else launch_ca<VT, 4, 2, 1>(B, desc, K, st);
+void launch_ca_any(const ExecBlock &B, const CaDesc *desc, int K, int G, cudaStream_t st) {
+    if (K == 1) {
+        if (B.ca_w == 1) launch_ca<VT, 1, 4, 1, false>(B, desc, K, st);
+        else if (B.ca_w == 2) launch_ca<VT, 2, 4, 1, false>(B, desc, K, st);
+        else launch_ca<VT, 4, 2, 1, false>(B, desc, K, st);
+    } else if (G == 1) {
+        if (B.ca_w == 1) launch_ca<VT, 1, 4, 1, true>(B, desc, K, st);
+        else if (B.ca_w == 2) launch_ca<VT, 2, 4, 1, true>(B, desc, K, st);
+        else launch_ca<VT, 4, 2, 1, true>(B, desc, K, st);
     } else if constexpr (sizeof(VT) == 8) {
-        if (B.ca_w == 1) launch_ca<VT, 1, 2, 2>(B, desc, K, st);
-        else launch_ca<VT, 2, 2, 2>(B, desc, K, st);
+        if (B.ca_w == 1) launch_ca<VT, 1, 2, 2, true>(B, desc, K, st);
+        else launch_ca<VT, 2, 2, 2, true>(B, desc, K, st);
     } else {
-        if (B.ca_w == 1) launch_ca<VT, 1, 4, 2>(B, desc, K, st);
-        else if (B.ca_w == 2) launch_ca<VT, 2, 4, 2>(B, desc, K, st);
-        else launch_ca<VT, 4, 2, 2>(B, desc, K, st);
+        if (B.ca_w == 1) launch_ca<VT, 1, 4, 2, true>(B, desc, K, st);
+        else if (B.ca_w == 2) launch_ca<VT, 2, 4, 2, true>(B, desc, K, st);
+        else launch_ca<VT, 4, 2, 2, true>(B, desc, K, st);
     }
 }
 
@@ -531,7 +557,8 @@ int launch_blocks(Plan &P, std::string &err) {
     if (rc) return rc;
     CsfDesc *edescs = nullptr;
     CaDesc *cdescs = nullptr;
-    if ((rc = ca_descs<VT>(P, cdescs, K, err))) return rc;
+    const int GL = plan_group<VT>(P, K);
+    if ((rc = ca_descs<VT>(P, cdescs, K, GL, err))) return rc;
     if (K == 1 && (rc = ell_descs<VT>(P, edescs, err))) return rc;
     if (D.ntri) CK(cudaMemsetAsync(D.tickets, 0, sizeof(int) * D.ntri, st));
     if (K == 1 && D.lc_queue) {
@@ -598,6 +625,16 @@ int launch_blocks(Plan &P, std::string &err) {
             const int kernel = (K > 1 && B.kernel == RBS_K_LEVEL && !mc_ca) ? RBS_K_SYNCFREE : B.kernel;
             switch (kernel) {
             case RBS_K_DIAG:
+                if (GL) {
+                    const int grid = grid_for((long long)B.m * K, 256, D.num_sms);
+                    const long long gs = (long long)P.n * GL;
+                    if (GL == 1)
+                        k_tri_diag_grp<VT, 1><<<grid, 256, 0, st>>>(inv + B.r0, bw + B.r0, xw + B.r0, B.m, K, gs);
+                    else
+                        k_tri_diag_grp<VT, 2><<<grid, 256, 0, st>>>(inv + B.r0, bw + 2LL * B.r0, xw + 2LL * B.r0, B.m,
+                                                                    K / 2, gs);
+                    break;
+                }
                 k_tri_diag<VT, K><<<grid_for((long long)B.m * K, 256, D.num_sms), 256, 0, st>>>(inv + B.r0, bb, xx,
                                                                                                B.m);
                 break;
@@ -608,7 +645,7 @@ int launch_blocks(Plan &P, std::string &err) {
                                                                    Pools<VT>::lcrec(D), sizeof(VT) == 4 ? 1 : 0, bb,
                                                                    xx, D.lc_queue + ti, D.status, limit);
                 } else if ((K == 1 && B.lvl_var == LVL_CA && B.ca_ok) || mc_ca) {
-                    launch_ca_any<VT>(B, cdescs + cti, K, st);
+                    launch_ca_any<VT>(B, cdescs + cti, K, GL ? GL : ca_group<VT>(B, K), st);
                 } else if (K == 1 && B.lvl_var == LVL_CSF && B.ell_ok) {
                     k_tri_cta_syncfree<VT><<<1, 1024, CsfLayout<VT>::total, st>>>(edescs + eti, D.status, limit);
                 } else {
@@ -645,6 +682,16 @@ int launch_blocks(Plan &P, std::string &err) {
                 if (B.ca_ok) ++cti;
             }
             ++ti;
+        } else if (B.kernel == RBS_K_SPMV && GL) {
+            const int *rows = B.rows_off >= 0 ? D.rows + B.rows_off : nullptr;
+            const int grid = grid_for((long long)B.nrows * (K / GL), 256, D.num_sms);
+            const long long gs = (long long)P.n * GL;
+            if (GL == 1)
+                k_spmv_sub_grp<VT, 1><<<grid, 256, 0, st>>>(D.rp + B.rp_off, D.col, val, rows, B.nrows, K, gs,
+                                                            xw + B.c0, bw + B.r0);
+            else
+                k_spmv_sub_grp<VT, 2><<<grid, 256, 0, st>>>(D.rp + B.rp_off, D.col, val, rows, B.nrows, K / 2, gs,
+                                                            xw + 2LL * B.c0, bw + 2LL * B.r0);
         } else if (B.kernel == RBS_K_SPMV) {
             const int g = K == 1 ? B.group : (K < 32 ? K : 32);
             const int *rows = B.rows_off >= 0 ? D.rows + B.rows_off : nullptr;
@@ -729,10 +776,15 @@ void drop_graphs_fwd(DeviceState &D) { drop_graphs(D); }
 // transposing tile kernel, whose reads and writes are both coalesced.
 template <typename VT, typename VT2, int K>
 void gather_in(DeviceState &D, int n, const double *b, int ld, const double *const *cols, int k, VT *out,
-               VT2 *out2) {
-    if constexpr (K >= 8) {
-        const int grid = (int)std::min<long long>(((long long)n + TP_ROWS - 1) / TP_ROWS, (long long)D.num_sms * 8);
-        k_gather_t<VT, VT2, K><<<std::max(grid, 1), 256, 0, D.stream>>>(b, ld, cols, k, D.ipos, n, out, out2);
+               VT2 *out2, int GL, GroupCols grp = GroupCols{}) {
+    const int tgrid = std::max(1, (int)std::min<long long>(((long long)n + TP_ROWS - 1) / TP_ROWS, (long long)D.num_sms * 8));
+    if (GL == 1) {
+        k_gather_p<VT, VT2, K, 1><<<tgrid, 256, 0, D.stream>>>(b, ld, cols, k, D.perm, n, out, out2, grp);
+    } else if (GL == 2) {
+        if constexpr (K % 2 == 0)
+            k_gather_p<VT, VT2, K, 2><<<tgrid, 256, 0, D.stream>>>(b, ld, cols, k, D.perm, n, out, out2, grp);
+    } else if (K >= 8 || grp.tab) {
+        k_gather_t<VT, VT2, K><<<tgrid, 256, 0, D.stream>>>(b, ld, cols, k, D.ipos, n, out, out2, grp);
     } else {
         const int grid = grid_for((long long)n * K, 256, D.num_sms);
         if (cols) k_gather_cols<VT, K><<<grid, 256, 0, D.stream>>>(cols, k, D.perm, n, out);
@@ -747,10 +799,15 @@ void gather_in(DeviceState &D, int n, const double *b, int ld, const double *con
 // Solutions out of processing order into the caller's columns (x + c*ld or
 // the table cols); RESET puts the sentinel back into the work vector.
 template <typename VT, int K, bool RESET>
-void scatter_out(DeviceState &D, int n, VT *xw, int k, double *x, int ld, double *const *cols) {
-    if constexpr (K >= 8) {
-        const int grid = (int)std::min<long long>(((long long)n + TP_ROWS - 1) / TP_ROWS, (long long)D.num_sms * 8);
-        k_scatter_t<VT, K, RESET><<<std::max(grid, 1), 256, 0, D.stream>>>(xw, D.ipos, n, k, x, ld, cols);
+void scatter_out(DeviceState &D, int n, VT *xw, int k, double *x, int ld, double *const *cols, int GL,
+                 GroupCols grp = GroupCols{}) {
+    const int tgrid = std::max(1, (int)std::min<long long>(((long long)n + TP_ROWS - 1) / TP_ROWS, (long long)D.num_sms * 8));
+    if (GL == 1) {
+        k_scatter_t<VT, K, RESET, 1><<<tgrid, 256, 0, D.stream>>>(xw, D.ipos, n, k, x, ld, cols, grp);
+    } else if (GL == 2) {
+        k_scatter_t<VT, K, RESET, 2><<<tgrid, 256, 0, D.stream>>>(xw, D.ipos, n, k, x, ld, cols, grp);
+    } else if (K >= 8 || grp.tab) {
+        k_scatter_t<VT, K, RESET><<<tgrid, 256, 0, D.stream>>>(xw, D.ipos, n, k, x, ld, cols, grp);
     } else {
         const int grid = grid_for((long long)n * K, 256, D.num_sms);
         if constexpr (RESET) {
@@ -767,10 +824,11 @@ void scatter_out(DeviceState &D, int n, VT *xw, int k, double *x, int ld, double
 template <int K>
 int solve_fp64(Plan &P, const double *b, double *x, int k, int ld, std::string &err) {
     DeviceState &D = *P.dev;
-    gather_in<double, double, K>(D, P.n, b, ld, nullptr, k, D.bw64, nullptr);
+    const int GL = plan_group<double>(P, K);
+    gather_in<double, double, K>(D, P.n, b, ld, nullptr, k, D.bw64, nullptr, GL);
     int rc = run_blocks<double, K>(P, err);
     if (rc) return rc;
-    scatter_out<double, K, true>(D, P.n, D.xw64, k, x, ld, nullptr);
+    scatter_out<double, K, true>(D, P.n, D.xw64, k, x, ld, nullptr, GL);
     CK(cudaGetLastError());
     return RBS_OK;
 }
@@ -778,10 +836,11 @@ int solve_fp64(Plan &P, const double *b, double *x, int k, int ld, std::string &
 template <int K>
 int solve_fp32(Plan &P, const double *b, double *x, int k, int ld, std::string &err) {
     DeviceState &D = *P.dev;
-    gather_in<float, float, K>(D, P.n, b, ld, nullptr, k, D.bw32, nullptr);
+    const int GL = plan_group<float>(P, K);
+    gather_in<float, float, K>(D, P.n, b, ld, nullptr, k, D.bw32, nullptr, GL);
     int rc = run_blocks<float, K>(P, err);
     if (rc) return rc;
-    scatter_out<float, K, true>(D, P.n, D.xw32, k, x, ld, nullptr);
+    scatter_out<float, K, true>(D, P.n, D.xw32, k, x, ld, nullptr, GL);
     CK(cudaGetLastError());
     return RBS_OK;
 }
@@ -791,14 +850,28 @@ int solve_fp32(Plan &P, const double *b, double *x, int k, int ld, std::string &
 // until ||d||/||x|| <= ir_tol for every right-hand side.
 //
 // mixed_first: x0 = L32^-1 b (b already gathered into b64keep and bw32).
+// x64 (+)= d32 with the per-column norms, in the layout of the FP32 sweeps
+template <int K>
+void mixed_update(Plan &P, int first) {
+    DeviceState &D = *P.dev;
+    const int GL = plan_group<float>(P, K);
+    if (GL) {
+        const dim3 grid((unsigned)std::max(1, std::min((P.n + 255) / 256, 2 * D.num_sms)), K);
+        if (GL == 1) k_update_grp<K, 1><<<grid, 256, 0, D.stream>>>(D.x64acc, D.xw32, P.n, first, D.norms);
+        else k_update_grp<K, 2><<<grid, 256, 0, D.stream>>>(D.x64acc, D.xw32, P.n, first, D.norms);
+        return;
+    }
+    k_update<K><<<grid_for((long long)P.n * K, 256, D.num_sms), 256, 0, D.stream>>>(D.x64acc, D.xw32, P.n, first,
+                                                                                      D.norms);
+}
+
 template <int K>
 int mixed_first(Plan &P, std::string &err) {
     DeviceState &D = *P.dev;
     int rc = run_blocks<float, K>(P, err);
     if (rc) return rc;
     CK(cudaMemsetAsync(D.norms, 0, sizeof(double) * 2 * K, D.stream));
-    k_update<K><<<grid_for((long long)P.n * K, 256, D.num_sms), 256, 0, D.stream>>>(D.x64acc, D.xw32, P.n, 1,
-                                                                                      D.norms);
+    mixed_update<K>(P, 1);
     return RBS_OK;
 }
 
@@ -809,12 +882,20 @@ int mixed_step(Plan &P, std::string &err) {
     DeviceState &D = *P.dev;
     const int n = P.n;
     const int G = P.nnz / std::max(1, n) < 6 ? 4 : 8;
-    k_residual<K><<<grid_for((long long)n * (K == 1 ? G : std::min(K, 32)), 256, D.num_sms), 256, 0, D.stream>>>(
-        D.full_rp, D.full_col, D.full_val, D.x64acc, D.b64keep, D.bw32, n, G);
+    const int GL = plan_group<float>(P, K);
+    if (GL == 1)
+        k_residual_grp<1><<<grid_for((long long)n * K, 256, D.num_sms), 256, 0, D.stream>>>(
+            D.full_rp, D.full_col, D.full_val, D.x64acc, D.b64keep, D.bw32, n, K, (long long)n);
+    else if (GL == 2)
+        k_residual_grp<2><<<grid_for((long long)n * (K / 2), 256, D.num_sms), 256, 0, D.stream>>>(
+            D.full_rp, D.full_col, D.full_val, D.x64acc, D.b64keep, D.bw32, n, K / 2, 2LL * n);
+    else
+        k_residual<K><<<grid_for((long long)n * (K == 1 ? G : std::min(K, 32)), 256, D.num_sms), 256, 0, D.stream>>>(
+            D.full_rp, D.full_col, D.full_val, D.x64acc, D.b64keep, D.bw32, n, G);
     int rc = run_blocks<float, K>(P, err);
     if (rc) return rc;
     CK(cudaMemsetAsync(D.norms, 0, sizeof(double) * 2 * K, D.stream));
-    k_update<K><<<grid_for((long long)n * K, 256, D.num_sms), 256, 0, D.stream>>>(D.x64acc, D.xw32, n, 0, D.norms);
+    mixed_update<K>(P, 0);
     CK(cudaMemcpyAsync(D.h_norms, D.norms, sizeof(double) * 2 * K, cudaMemcpyDeviceToHost, D.stream));
     return RBS_OK;
 }
@@ -834,7 +915,8 @@ double mixed_correction(const DeviceState &D, int K, int k) {
 template <int K>
 int solve_mixed(Plan &P, const double *b, double *x, int k, int ld, int &iters, double &corr, std::string &err) {
     DeviceState &D = *P.dev;
-    gather_in<double, float, K>(D, P.n, b, ld, nullptr, k, D.b64keep, D.bw32);
+    const int GL = plan_group<float>(P, K);
+    gather_in<double, float, K>(D, P.n, b, ld, nullptr, k, D.b64keep, D.bw32, GL);
     int rc = mixed_first<K>(P, err);
     if (rc) return rc;
     iters = 0;
@@ -846,7 +928,7 @@ int solve_mixed(Plan &P, const double *b, double *x, int k, int ld, int &iters, 
         corr = mixed_correction(D, K, k);
         if (corr <= P.opt.ir_tol) break;
     }
-    scatter_out<double, K, false>(D, P.n, D.x64acc, k, x, ld, nullptr);
+    scatter_out<double, K, false>(D, P.n, D.x64acc, k, x, ld, nullptr, GL);
     CK(cudaGetLastError());
     if (!(corr <= P.opt.ir_tol)) {
         err = "mixed-precision refinement stopped at ||dx||/||x|| = " + std::to_string(corr);
@@ -875,20 +957,23 @@ int solve_mixed(Plan &P, const double *b, double *x, int k, int ld, int &iters, 
     }
 
 template <int K>
-int batch_start_k(Plan &P, const double *const *bcols, double *const *xcols, int k, int prec, std::string &err) {
+int batch_start_k(Plan &P, const double *const *bcols, double *const *xcols, int k, int prec, const GroupCols &gb,
+                  const GroupCols &gx, std::string &err) {
     DeviceState &D = *P.dev;
     const int n = P.n;
     int rc;
     if (prec == RBS_PREC_FP64) {
-        gather_in<double, double, K>(D, n, nullptr, n, bcols, k, D.bw64, nullptr);
+        const int GL = plan_group<double>(P, K);
+        gather_in<double, double, K>(D, n, nullptr, n, bcols, k, D.bw64, nullptr, GL, gb);
         if ((rc = run_blocks<double, K>(P, err))) return rc;
-        scatter_out<double, K, true>(D, n, D.xw64, k, nullptr, n, xcols);
+        scatter_out<double, K, true>(D, n, D.xw64, k, nullptr, n, xcols, GL, gx);
     } else if (prec == RBS_PREC_FP32) {
-        gather_in<float, float, K>(D, n, nullptr, n, bcols, k, D.bw32, nullptr);
+        const int GL = plan_group<float>(P, K);
+        gather_in<float, float, K>(D, n, nullptr, n, bcols, k, D.bw32, nullptr, GL, gb);
         if ((rc = run_blocks<float, K>(P, err))) return rc;
-        scatter_out<float, K, true>(D, n, D.xw32, k, nullptr, n, xcols);
+        scatter_out<float, K, true>(D, n, D.xw32, k, nullptr, n, xcols, GL, gx);
     } else {
-        gather_in<double, float, K>(D, n, nullptr, n, bcols, k, D.b64keep, D.bw32);
+        gather_in<double, float, K>(D, n, nullptr, n, bcols, k, D.b64keep, D.bw32, plan_group<float>(P, K), gb);
         if ((rc = mixed_first<K>(P, err))) return rc;
         if ((rc = mixed_step<K>(P, err))) return rc;
     }
@@ -897,9 +982,9 @@ int batch_start_k(Plan &P, const double *const *bcols, double *const *xcols, int
 }
 
 template <int K>
-int batch_end_k(Plan &P, double *const *xcols, int k, std::string &err) {
+int batch_end_k(Plan &P, double *const *xcols, int k, const GroupCols &gx, std::string &err) {
     DeviceState &D = *P.dev;
-    scatter_out<double, K, false>(D, P.n, D.x64acc, k, nullptr, P.n, xcols);
+    scatter_out<double, K, false>(D, P.n, D.x64acc, k, nullptr, P.n, xcols, plan_group<float>(P, K), gx);
     CK(cudaGetLastError());
     return RBS_OK;
 }
@@ -922,7 +1007,7 @@ int device_reserve(Plan &P, int k, std::string &err) {
 }
 
 int device_batch_start(Plan &P, const double *const *bcols, double *const *xcols, int k, int prec, int *more,
-                       std::string &err) {
+                       std::string &err, const BatchGroup *grp) {
     DeviceState &D = *P.dev;
     if (k < 1 || k > 128 || (prec != RBS_PREC_FP64 && !D.mixed)) {
         err = "batch: k must be in [1, 128]; FP32 and mixed batches need a plan with FP32 copies";
@@ -937,7 +1022,13 @@ int device_batch_start(Plan &P, const double *const *bcols, double *const *xcols
     D.bat_iters = 0;
     D.bat_corr = 0;
     D.bat_xcols = xcols;
-    RBS_FOR_K(K, rc = batch_start_k<KC>(P, bcols, xcols, k, prec, err));
+    GroupCols gb{}, gx{};
+    if (grp) {
+        gb = GroupCols{grp->btab, grp->seg, grp->off, grp->count};
+        gx = GroupCols{grp->xtab, grp->seg, grp->off, grp->count};
+    }
+    D.bat_gx = gx;
+    RBS_FOR_K(K, rc = batch_start_k<KC>(P, bcols, xcols, k, prec, gb, gx, err));
     if (rc) return rc;
     *more = prec == RBS_PREC_MIXED ? 1 : 0;
     if (!*more) CK(cudaMemcpyAsync(D.h_status, D.status, sizeof(int), cudaMemcpyDeviceToHost, D.stream));
@@ -951,7 +1042,7 @@ int device_batch_next(Plan &P, int *more, std::string &err) {
     D.bat_corr = mixed_correction(D, K, D.bat_k);
     int rc = RBS_OK;
     if (D.bat_corr <= P.opt.ir_tol || D.bat_iters >= P.opt.ir_max_iter) {
-        RBS_FOR_K(K, rc = batch_end_k<KC>(P, D.bat_xcols, D.bat_k, err));
+        RBS_FOR_K(K, rc = batch_end_k<KC>(P, D.bat_xcols, D.bat_k, D.bat_gx, err));
         if (rc) return rc;
         CK(cudaMemcpyAsync(D.h_status, D.status, sizeof(int), cudaMemcpyDeviceToHost, D.stream));
         *more = 0;

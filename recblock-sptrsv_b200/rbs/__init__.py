@@ -108,7 +108,7 @@ EXPORTS = [
     "rbs_plan_free", "rbs_last_error", "rbs_auto_lv", "recblocking_solver_cuda", "recblocking_solver",
     "rbs_gen_lower_csr", "rbs_gen_uniform", "rbs_gen_free", "rbs_plan_profile", "rbs_plan_block_times",
     "rbs_sptrsv_csr_noalloc", "rbs_batch_analyse", "rbs_server_create", "rbs_server_add_factor",
-    "rbs_server_submit", "rbs_server_submit_device", "rbs_server_wait", "rbs_server_stats_get", "rbs_server_reset_stats", "rbs_server_destroy",
+    "rbs_server_submit", "rbs_server_submit_device", "rbs_server_add_group", "rbs_server_wait", "rbs_server_stats_get", "rbs_server_reset_stats", "rbs_server_destroy",
     "rbs_plan_save", "rbs_plan_load", "rbs_ilu0_device", "rbs_mtx_read", "rbs_mtx_read_buffer", "rbs_mtx_info_get",
     "rbs_mtx_csr", "rbs_mtx_triangle", "rbs_mtx_free", "rbs_mtx_write", "rbs_ic0_device", "rbs_plan_reserve", "rbs_solve_host_async",
 ]
@@ -181,6 +181,7 @@ def _load():
                                       ctypes.POINTER(ctypes.c_longlong)]
     lib.rbs_server_submit_device.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_longlong)]
+    lib.rbs_server_add_group.argtypes = [P, P, ctypes.c_int, ip, ip]
     lib.rbs_plan_reserve.argtypes = [P, ctypes.c_int]
     lib.rbs_solve_host_async.argtypes = [P, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.rbs_server_wait.argtypes = [P, ctypes.c_longlong, dp, ip]
@@ -360,6 +361,16 @@ class Server:
         _check(lib.rbs_server_add_factor(self._h, plan.handle, ctypes.byref(fid)))
         plan._h = None  # owned by the server now
         return fid.value
+
+    def add_group(self, plan: Plan, row_offsets) -> list:
+        """A block-diagonal plan (batch_analyse) served as one unit: one factor id per system."""
+        offs = np.ascontiguousarray(row_offsets, dtype=np.int32)
+        count = len(offs) - 1
+        ids = np.zeros(count, dtype=np.int32)
+        _check(lib.rbs_server_add_group(self._h, plan.handle, count, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                        ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        plan._h = None  # owned by the server now
+        return [int(v) for v in ids]
 
     def submit_device(self, factor: int, b, x, k: int = 1, prec: int = PREC_FP64) -> int:
         """Device arrays (torch CUDA tensors, float64, n*k elements, column-major), read and

@@ -13,6 +13,27 @@
 
 using namespace rbs;
 
+// The host analysis reaches the device block extraction (dev_pools.cu) only
+// from rbs_analyse_device; this host-only build never takes that path, so
+// the device steps are stand-ins that report it.
+namespace rbs {
+DevRows::~DevRows() {}
+int dev_block_counts(DevRows &, int, int, const std::vector<long long> &, std::vector<int> &, std::vector<double> &,
+                     std::vector<int> &, std::string &err) {
+    err = "no device in this build";
+    return RBS_ERR_UNSUPPORTED;
+}
+int dev_local_levels(DevRows &, int, int, long long, std::vector<int> &, std::string &err) {
+    err = "no device in this build";
+    return RBS_ERR_UNSUPPORTED;
+}
+int dev_pool_fill(DevRows &, int, int, long long, long long, bulk_vector<int> &, bulk_vector<double> &,
+                  std::string &err) {
+    err = "no device in this build";
+    return RBS_ERR_UNSUPPORTED;
+}
+}  // namespace rbs
+
 static void band(int n, int bw, double lam, unsigned seed, std::vector<int> &rp, std::vector<int> &ci,
                  std::vector<double> &va) {
     std::mt19937_64 g(seed);

@@ -105,3 +105,61 @@ def test_reserve_then_solve_wider_and_narrower(cuda):
             got = dX.cpu().numpy().reshape(k, n)
             for c in range(k):
                 assert rel_err(got[c], oracle.sptrsv_csr(rp, ci, va, rbs.FORWARD, B[c])) <= TOL, (k, prec, c)
+
+
+def test_server_group_serves_members_in_one_launch(cuda):
+    # twelve small factors as one group (a block-diagonal plan), next to two
+    # single factors: requests of all members share launches (the server's
+    # batch count stays far below the request count), host and device
+    # arrays, FP64 and mixed; every column against the oracle and against the
+    # same factor solved alone
+    import torch
+    facs = factors(14, 53)
+    facs = [f for f in facs if len(f[0]) - 1 <= 12000][:12] + facs[:2]
+    members, singles = facs[:-2], facs[-2:]
+    srv = rbs.Server(hbm_budget_bytes=40 << 30, max_batch_rhs=16)
+    gplan, offs = rbs.batch_analyse([tuple(L) for L in members], substitution=rbs.FORWARD, fmt=rbs.FMT_CSR)
+    fids = srv.add_group(gplan, offs)
+    fids += [srv.add_factor(rbs.analyse(*L, substitution=rbs.FORWARD, lv=-1, fmt=rbs.FMT_CSR)) for L in singles]
+    alone = [rbs.analyse(*L, substitution=rbs.FORWARD, lv=-1, fmt=rbs.FMT_CSR) for L in facs]
+    rng = np.random.default_rng(91)
+    reqs = []
+    for q in range(160):
+        f = int(rng.integers(0, len(facs)))
+        k = int(rng.integers(1, 5))
+        rp, ci, va = facs[f]
+        n = len(rp) - 1
+        X = np.stack([rbs.gen_uniform(80000 + 20 * q + c, n) for c in range(k)])
+        B = np.ascontiguousarray(np.stack([oracle.spmv_csr(rp, ci, va, X[c]) for c in range(k)]))
+        prec = rbs.PREC_MIXED if q % 2 else rbs.PREC_FP64
+        r = dict(f=f, k=k, B=B, prec=prec, device=q % 3 != 0)
+        if r["device"]:
+            r["dB"] = torch.tensor(B.reshape(-1), device=cuda)
+            r["dX"] = torch.full_like(r["dB"], float("nan"))
+        else:
+            r["X"] = np.full_like(B, np.nan)
+        reqs.append(r)
+    tickets = []
+    for r in reqs:
+        if r["device"]:
+            tickets.append(srv.submit_device(fids[r["f"]], r["dB"], r["dX"], k=r["k"], prec=r["prec"]))
+        else:
+            tickets.append(srv.submit(fids[r["f"]], r["B"], r["X"], k=r["k"], prec=r["prec"]))
+    for t in tickets:
+        srv.wait(t)
+    st = srv.stats()
+    assert st.completed == len(reqs)
+    assert st.batches < len(reqs) / 2, st.batches  # members and requests shared launches
+    for r in reqs:
+        rp, ci, va = facs[r["f"]]
+        n = len(rp) - 1
+        X = r["dX"].cpu().numpy().reshape(r["k"], n) if r["device"] else r["X"]
+        dB = torch.tensor(r["B"].reshape(-1), device=cuda)
+        dXa = torch.empty_like(dB)
+        alone[r["f"]].solve(dB, dXa, k=r["k"], prec=r["prec"])
+        Xa = dXa.cpu().numpy().reshape(r["k"], n)
+        for c in range(r["k"]):
+            xo = oracle.sptrsv_csr(rp, ci, va, rbs.FORWARD, r["B"][c])
+            assert rel_err(X[c], xo) <= TOL, (r["f"], c, r["prec"])
+            assert rel_err(X[c], Xa[c]) <= TOL, (r["f"], c, r["prec"])
+    srv.close()

@@ -130,9 +130,9 @@ def test_device_analysis_entry(cuda):
 @pytest.mark.parametrize("grid", [64, 300])
 def test_multi_rhs_staged_level_triangles(cuda, grid, sub):
     # 2D-Laplacian factors: their triangles run the staged level kernel with
-    # one CTA per group of right-hand-side columns (one column per CTA below
-    # 64 columns, two from 64 on); widths 8 and up also take the transposing
-    # gather and scatter.  Every column against the oracle, FP64 and mixed
+    # one CTA per group of two right-hand-side columns; widths 8 and up also
+    # take the transposing gather and scatter (odd widths leave padding
+    # columns in the last group).  Every column against the oracle, FP64 and mixed
     # at 1e-12, FP32 at single precision.
     rp, ci, va = rbs.gen_lower_csr(rbs.GEN_LAPLACE2D, grid=grid, seed=grid + sub)
     cp, ri, cv = oracle.transpose(rp, ci, va) if sub == rbs.FORWARD else (rp, ci, va)
