@@ -660,7 +660,9 @@ def side_serving(dev, args, n_requests=1000, loads=(500, 1000, 2000, 10000, 5000
     request carries 1-16 right-hand sides in device arrays; the server
     batches within factors (one multi-RHS solve per batch, columns read in
     place) and across them (batches of all factors overlap on the device),
-    with FP32 sweeps + FP64 refinement.  Baselines, on the same arrivals and
+    once with FP32 sweeps + FP64 refinement and once in FP64 (the solves are
+    latency-bound, so the FP64 sweep, one walk instead of two or three, is
+    the faster choice here).  Baselines, on the same arrivals and
     device arrays: one plain FP64 rbs_solve of each request's k columns in
     arrival order on the caller's thread, and the plain FP64 single-RHS path
     (one rbs_solve per right-hand side, back to back)."""
@@ -728,51 +730,58 @@ def side_serving(dev, args, n_requests=1000, loads=(500, 1000, 2000, 10000, 5000
     sys.setswitchinterval(1e-4)  # the submit loop and the waiter share the interpreter
     fids = [srv.add_factor(p) for p in plans]
     plans = None
-    # warm-up: every factor once at one and at 16 columns, mixed (captures the block walks)
+    # warm-up: every factor once at one and at 16 columns, in both served
+    # precisions (captures the block walks)
     for f in range(64):
         for k in (1, 16):
-            srv.wait(srv.submit_device(fids[f], dB[f], dX[f], k=k, prec=rbs.PREC_MIXED))
+            for prec in (rbs.PREC_MIXED, rbs.PREC_FP64):
+                srv.wait(srv.submit_device(fids[f], dB[f], dX[f], k=k, prec=prec))
+
+    def serve(rate, prec):
+        arr, fid, ks = scheds[rate]
+        srv.reset_stats()
+        tickets = []
+        lats = []
+        failure = []
+
+        def waiter():
+            try:
+                for i in range(n_requests):
+                    while i >= len(tickets):
+                        time.sleep(0)
+                    lats.append(srv.wait(tickets[i])[0])
+            except Exception as e:  # handed to the main thread below
+                failure.append(e)
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        lag = []
+        t_start = time.perf_counter()
+        try:
+            for a, f, k in zip(arr, fid, ks):
+                while time.perf_counter() - t_start < a:
+                    pass
+                lag.append(1000 * (time.perf_counter() - t_start - a))
+                tickets.append(srv.submit_device(fids[f], dB[f], dX[f], k=int(k), prec=prec))
+        finally:
+            th.join()
+        if failure:
+            raise failure[0]
+        span = time.perf_counter() - t_start
+        lats = np.array(lats) + np.array(lag)  # latency from the scheduled arrival, as for the plain arm
+        st = srv.stats()
+        return {"p50_ms": float(np.percentile(lats, 50)), "p99_ms": float(np.percentile(lats, 99)),
+                "solves_per_s": float(ks.sum()) / span, "requests_per_s": n_requests / span,
+                "mean_batch_rhs": st.mean_batch_rhs, "batches": st.batches}
+
     try:
         for rate in loads:
-            arr, fid, ks = scheds[rate]
-            srv.reset_stats()
-            tickets = []
-            lats = []
-            failure = []
-
-            def waiter():
-                try:
-                    for i in range(n_requests):
-                        while i >= len(tickets):
-                            time.sleep(0)
-                        lats.append(srv.wait(tickets[i])[0])
-                except Exception as e:  # handed to the main thread below
-                    failure.append(e)
-
-            th = threading.Thread(target=waiter)
-            th.start()
-            lag = []
-            t_start = time.perf_counter()
-            try:
-                for a, f, k in zip(arr, fid, ks):
-                    while time.perf_counter() - t_start < a:
-                        pass
-                    lag.append(1000 * (time.perf_counter() - t_start - a))
-                    tickets.append(srv.submit_device(fids[f], dB[f], dX[f], k=int(k), prec=rbs.PREC_MIXED))
-            finally:
-                th.join()
-            if failure:
-                raise failure[0]
-            span = time.perf_counter() - t_start
-            lats = np.array(lats) + np.array(lag)  # latency from the scheduled arrival, as for the plain arm
-            st = srv.stats()
-            res["loads"][str(rate)] = {
-                "served_mixed": {"p50_ms": float(np.percentile(lats, 50)), "p99_ms": float(np.percentile(lats, 99)),
-                                 "solves_per_s": float(ks.sum()) / span, "requests_per_s": n_requests / span,
-                                 "mean_batch_rhs": st.mean_batch_rhs, "batches": st.batches},
-                "plain_fp64": plain[rate]}
-            res["loads"][str(rate)]["x_plain_fp64"] = float(ks.sum()) / span / plain[rate]["solves_per_s"]
-            res["loads"][str(rate)]["x_plain_fp64_single_rhs"] = float(ks.sum()) / span / single
+            row = {"served_mixed": serve(rate, rbs.PREC_MIXED), "served_fp64": serve(rate, rbs.PREC_FP64),
+                   "plain_fp64": plain[rate]}
+            for arm in ("served_mixed", "served_fp64"):
+                row[f"{arm}_x_plain_fp64"] = row[arm]["solves_per_s"] / plain[rate]["solves_per_s"]
+                row[f"{arm}_x_plain_fp64_single_rhs"] = row[arm]["solves_per_s"] / single
+            res["loads"][str(rate)] = row
         # accuracy: every factor once, b = L x_true, served mixed vs x_true
         import scipy.sparse as sp
         worst = 0.0

@@ -143,22 +143,14 @@ __global__ void k_scatter_cols(VT *__restrict__ xw, const int *__restrict__ perm
 }
 
 // Transposing forms of the gather and scatter for many right-hand sides
-// (K >= 8, or any K for the grouped layout): a CTA takes a tile of 32
-// original rows, reads it column by column (32 consecutive values of a
-// column: coalesced), and writes every row at its processing position (K
-// consecutive values: coalesced), through a shared-memory tile; the scatter
-// runs the other way.  Columns come from b + c*ld, or from the table cols[c]
-// when cols is not NULL.  ipos[i] is the processing position of original row
-// i.  GL = 0: row-interleaved work vector (entry (p, c) at p*K + c); GL > 0:
-// grouped (column group c / GL holds its rows contiguously, GL values each:
-// entry at (c / GL)*n*GL + p*GL + c % GL).
+// with the row-interleaved work vector (entry (p, c) at p*K + c): a CTA takes
+// a tile of 32 original rows, reads it column by column (32 consecutive
+// values of a column: coalesced), and writes every row at its processing
+// position (K consecutive values: coalesced), through a shared-memory tile;
+// the scatter runs the other way.  Columns come from b + c*ld, or from the
+// table cols[c] when cols is not NULL.  ipos[i] is the processing position
+// of original row i.
 constexpr int TP_ROWS = 32;
-
-template <int K, int GL>
-__device__ __forceinline__ long long work_index(long long p, int c, int n) {
-    if constexpr (GL == 0) return p * K + c;
-    else return (long long)(c / GL) * n * GL + p * GL + (c % GL);
-}
 
 // Columns of several independent systems solved as one block-diagonal plan
 // (a server group): column c of system f comes from tab[c*F + f] (NULL: no
@@ -176,7 +168,7 @@ __device__ __forceinline__ const double *group_src(const GroupCols &g, int c, lo
     return g.tab[(long long)c * g.F + f];
 }
 
-template <typename VT, typename VT2, int K, int GL = 0>
+template <typename VT, typename VT2, int K>
 __global__ void __launch_bounds__(256) k_gather_t(const double *__restrict__ b, int ld,
                                                   const double *const *__restrict__ cols, int k,
                                                   const int *__restrict__ ipos, int n, VT *__restrict__ out,
@@ -202,51 +194,7 @@ __global__ void __launch_bounds__(256) k_gather_t(const double *__restrict__ b, 
         for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
             const int t = e / K, c = e % K;
             if (t < rows) {
-                const long long o = work_index<K, GL>(ipos[i0 + t], c, n);
-                out[o] = (VT)tile[c][t];
-                if (out2) out2[o] = (VT2)tile[c][t];
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// Grouped layout (GL > 0): tiles of 32 consecutive PROCESSING positions, so
-// each column group's 32 rows are written as one contiguous run of 32*GL
-// values; the right-hand-side values are read at the rows' original
-// positions perm[p] (single values, read-only).
-template <typename VT, typename VT2, int K, int GL>
-__global__ void __launch_bounds__(256) k_gather_p(const double *__restrict__ b, int ld,
-                                                  const double *const *__restrict__ cols, int k,
-                                                  const int *__restrict__ perm, int n, VT *__restrict__ out,
-                                                  VT2 *__restrict__ out2, GroupCols grp) {
-    static_assert(GL > 0 && K % GL == 0, "grouped layout");
-    __shared__ double tile[K][TP_ROWS + 1];
-    for (long long p0 = (long long)blockIdx.x * TP_ROWS; p0 < n; p0 += (long long)gridDim.x * TP_ROWS) {
-        const int rows = (int)min((long long)TP_ROWS, n - p0);
-        for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
-            const int c = e / TP_ROWS, t = e % TP_ROWS;
-            double v = 0.0;
-            if (c < k && t < rows) {
-                const long long i = perm[p0 + t];
-                if (grp.tab) {
-                    long long r;
-                    const double *src = group_src(grp, c, i, r);
-                    if (src) v = src[r];
-                } else {
-                    v = cols ? cols[c][i] : b[(long long)c * ld + i];
-                }
-            }
-            tile[c][t] = v;
-        }
-        __syncthreads();
-        // group g's rows p0.. p0+rows-1: GL values each, contiguous
-        for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
-            const int g = e / (TP_ROWS * GL), rest = e % (TP_ROWS * GL);
-            const int t = rest / GL, j = rest % GL;
-            if (t < rows) {
-                const int c = g * GL + j;
-                const long long o = (long long)g * n * GL + (p0 + t) * GL + j;
+                const long long o = (long long)ipos[i0 + t] * K + c;
                 out[o] = (VT)tile[c][t];
                 if (out2) out2[o] = (VT2)tile[c][t];
             }
@@ -256,7 +204,7 @@ __global__ void __launch_bounds__(256) k_gather_p(const double *__restrict__ b, 
 }
 
 // RESET: the work vector is set back to the sentinel as it is read.
-template <typename VT, int K, bool RESET, int GL = 0>
+template <typename VT, int K, bool RESET>
 __global__ void __launch_bounds__(256) k_scatter_t(VT *__restrict__ xw, const int *__restrict__ ipos, int n, int k,
                                                    double *__restrict__ x, int ld, double *const *__restrict__ cols,
                                                    GroupCols grp) {
@@ -266,7 +214,7 @@ __global__ void __launch_bounds__(256) k_scatter_t(VT *__restrict__ xw, const in
         for (int e = threadIdx.x; e < K * TP_ROWS; e += blockDim.x) {
             const int t = e / K, c = e % K;
             if (t < rows) {
-                const long long o = work_index<K, GL>(ipos[i0 + t], c, n);
+                const long long o = (long long)ipos[i0 + t] * K + c;
                 tile[c][t] = (double)xw[o];
                 if (RESET) xw[o] = Sent<VT>::value();
             }
@@ -288,6 +236,185 @@ __global__ void __launch_bounds__(256) k_scatter_t(VT *__restrict__ xw, const in
         }
         __syncthreads();
     }
+}
+
+// Gather and scatter for the grouped work vector (column group g = c / GL
+// holds its rows contiguously, GL values per row: entry (p, c) at
+// g*n*GL + p*GL + c % GL).  One thread per processing position p and GT
+// column groups: the work-vector side is one GL-wide vector access per
+// group (consecutive threads, consecutive positions: coalesced), the
+// caller's side GL single values at the original row perm[p].  Grid x runs
+// over positions, grid y over chunks of GT groups, so the CTAs resident at
+// one time work on one chunk of columns and the rows they touch out of order
+// (GT*GL columns of n values) stay in L2 until every value of a sector has
+// been used.  Only positions [pa, pb) are moved (a range of triangles when
+// the moves overlap the block walk).  Columns c in [k, K), and columns whose
+// table entry cols[c] is NULL, get zeros on the way in and are not written
+// out.
+template <int K, int GL>
+struct GroupTile {
+    static_assert(GL > 0 && K % GL == 0, "grouped layout");
+    static constexpr int NG = K / GL;              // column groups
+    static constexpr int GT = NG < 4 ? NG : 4;     // groups per thread
+    static constexpr int CHUNKS = (NG + GT - 1) / GT;
+};
+
+template <typename VT, typename VT2, int K, int GL>
+__global__ void __launch_bounds__(256) k_gather_grp(const double *__restrict__ b, int ld,
+                                                    const double *const *__restrict__ cols, int k,
+                                                    const int *__restrict__ perm, int n, int pa, int pb,
+                                                    VT *__restrict__ out, VT2 *__restrict__ out2, GroupCols grp) {
+    using T = GroupTile<K, GL>;
+    const long long p = pa + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pb) return;
+    const int g0 = blockIdx.y * T::GT;
+    const long long i = perm[p];
+    long long r = i;
+    int f = 0;
+    if (grp.tab) {
+        f = grp.seg[i];
+        r = i - grp.off[f];
+    }
+    double v[T::GT][GL];
+#pragma unroll
+    for (int a = 0; a < T::GT; ++a)
+#pragma unroll
+        for (int j = 0; j < GL; ++j) {
+            const int c = (g0 + a) * GL + j;
+            double t = 0.0;
+            if (c < k) {
+                if (grp.tab) {
+                    const double *src = grp.tab[(long long)c * grp.F + f];
+                    if (src) t = src[r];
+                } else if (cols) {
+                    const double *src = cols[c];
+                    if (src) t = src[i];
+                } else {
+                    t = b[(long long)c * ld + i];
+                }
+            }
+            v[a][j] = t;
+        }
+#pragma unroll
+    for (int a = 0; a < T::GT; ++a) {
+        const int g = g0 + a;
+        if (T::NG % T::GT != 0 && g >= T::NG) break;
+        const long long o = (long long)g * n * GL + p * GL;
+        Vec<VT, GL> w;
+#pragma unroll
+        for (int j = 0; j < GL; ++j) w.v[j] = (VT)v[a][j];
+        *reinterpret_cast<Vec<VT, GL> *>(out + o) = w;
+        if (out2) {
+            Vec<VT2, GL> w2;
+#pragma unroll
+            for (int j = 0; j < GL; ++j) w2.v[j] = (VT2)v[a][j];
+            *reinterpret_cast<Vec<VT2, GL> *>(out2 + o) = w2;
+        }
+    }
+}
+
+// RESET: the work vector is set back to the sentinel as it is read (every
+// one of the K columns, as the solve expects).
+template <typename VT, int K, int GL, bool RESET>
+__global__ void __launch_bounds__(256) k_scatter_grp(VT *__restrict__ xw, const int *__restrict__ perm, int n, int k,
+                                                     int pa, int pb, double *__restrict__ x, int ld,
+                                                     double *const *__restrict__ cols, GroupCols grp) {
+    using T = GroupTile<K, GL>;
+    const long long p = pa + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pb) return;
+    const int g0 = blockIdx.y * T::GT;
+    const long long i = perm[p];
+    long long r = i;
+    int f = 0;
+    if (grp.tab) {
+        f = grp.seg[i];
+        r = i - grp.off[f];
+    }
+    Vec<VT, GL> w[T::GT];
+#pragma unroll
+    for (int a = 0; a < T::GT; ++a) {
+        const int g = g0 + a;
+        if (T::NG % T::GT != 0 && g >= T::NG) break;
+        VT *src = xw + (long long)g * n * GL + p * GL;
+        w[a] = *reinterpret_cast<const Vec<VT, GL> *>(src);
+        if (RESET) {
+            Vec<VT, GL> s;
+#pragma unroll
+            for (int j = 0; j < GL; ++j) s.v[j] = Sent<VT>::value();
+            *reinterpret_cast<Vec<VT, GL> *>(src) = s;
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < T::GT; ++a)
+#pragma unroll
+        for (int j = 0; j < GL; ++j) {
+            const int c = (g0 + a) * GL + j;
+            if (c >= k) continue;
+            const double t = (double)w[a].v[j];
+            if (grp.tab) {
+                double *dst = const_cast<double *>(grp.tab[(long long)c * grp.F + f]);
+                if (dst) dst[r] = t;
+            } else if (cols) {
+                if (cols[c]) cols[c][i] = t;
+            } else {
+                x[(long long)c * ld + i] = t;
+            }
+        }
+}
+
+// Grouped scatter of one triangle's solutions in ORIGINAL row order: rows[q]
+// for q in [qa, qb) lists the triangle's original rows ascending, so a
+// warp's writes to a caller's column fall on neighbouring rows (whole
+// sectors), while the work vector is read out of order at each row's
+// processing position ipos[i], one GL-wide vector per group (reads out of
+// order are what L2 absorbs; writes out of order of 8 bytes are not).  A CTA
+// takes TR rows and a chunk of GT column groups through a shared-memory
+// tile.  Columns whose table entry is NULL are not written.
+// The work vector keeps its values (no sentinel reset).
+template <typename VT, int K, int GL>
+__global__ void __launch_bounds__(256) k_scatter_rows(const VT *__restrict__ xw, const int *__restrict__ rows,
+                                                     const int *__restrict__ ipos, int n, int qa, int qb,
+                                                     double *const *__restrict__ cols) {
+    using T = GroupTile<K, GL>;
+    static_assert(T::NG % T::GT == 0 && 256 % T::GT == 0, "whole chunks");
+    constexpr int CC = T::GT * GL;  // columns per chunk
+    constexpr int TR = 256 / T::GT;  // rows per tile
+    __shared__ double tile[CC][TR + 1];
+    __shared__ int trow[TR];
+    const int g0 = blockIdx.y * T::GT;
+    const long long q0 = qa + (long long)blockIdx.x * TR;
+    {
+        const int t = threadIdx.x % TR, a = threadIdx.x / TR;
+        const long long q = q0 + t;
+        if (q < qb) {
+            const int i = rows[q];
+            if (a == 0) trow[t] = i;
+            const Vec<VT, GL> w =
+                *reinterpret_cast<const Vec<VT, GL> *>(xw + (long long)(g0 + a) * n * GL + (long long)ipos[i] * GL);
+#pragma unroll
+            for (int j = 0; j < GL; ++j) tile[a * GL + j][t] = (double)w.v[j];
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < CC * TR; e += blockDim.x) {
+        const int cl = e / TR, t = e % TR;
+        if (q0 + t < qb) {
+            double *dst = cols[g0 * GL + cl];
+            if (dst) dst[trow[t]] = tile[cl][t];
+        }
+    }
+}
+
+// The caller's columns as a device table for the block walk that moves them
+// itself (a graph replayed for every solve reads the columns through it):
+// tab[c] = b + c*ld and tab[RBS_IO_COLS + c] = x + c*ld for c < k, NULL
+// for the rest.
+constexpr int RBS_IO_COLS = 128;
+static __global__ void k_set_io(double **tab, const double *b, double *x, int ld, int k) {
+    const int c = threadIdx.x;
+    if (c >= RBS_IO_COLS) return;
+    tab[c] = c < k ? const_cast<double *>(b) + (long long)c * ld : nullptr;
+    tab[RBS_IO_COLS + c] = c < k ? x + (long long)c * ld : nullptr;
 }
 
 template <typename VT>
@@ -344,8 +471,23 @@ __global__ void __launch_bounds__(256) k_tri_syncfree(const int *__restrict__ rp
             const unsigned gmask = g == 32 ? 0xffffffffu : (((1u << g) - 1u) << (sub * g));
             VT sum = 0;
             if (active) {
+                // the row's entries in aligned pairs, one vector load of two
+                // values (16 bytes in FP64) and one of two columns per pair
+                // and lane; an odd first entry and an odd last one alone
                 const int s = rp[row], e = rp[row + 1];
-                for (int k = s + sl; k < e; k += g) sum += val[k] * wait_value(x + col[k], status, limit);
+                const int p0 = s + (s & 1);
+                if (sl == 0 && p0 > s && s < e) sum += val[s] * wait_value(x + col[s], status, limit);
+                using V2 = Vec<VT, 2>;
+                const int npair = (e - p0) / 2;
+                for (int q = sl; q < npair; q += g) {
+                    const int k = p0 + 2 * q;
+                    const int2 c2 = *reinterpret_cast<const int2 *>(col + k);
+                    const V2 v2 = *reinterpret_cast<const V2 *>(val + k);
+                    sum += v2.v[0] * wait_value(x + c2.x, status, limit);
+                    sum += v2.v[1] * wait_value(x + c2.y, status, limit);
+                }
+                const int last = p0 + 2 * npair;
+                if (last < e && sl == (npair % g)) sum += val[last] * wait_value(x + col[last], status, limit);
             }
             for (int off = g >> 1; off > 0; off >>= 1) sum += __shfl_down_sync(gmask, sum, off, g);
             if (active && sl == 0) st_relaxed(x + row, finalize((b[row] - sum) * inv[row]));
@@ -501,7 +643,10 @@ __global__ void __launch_bounds__(256) k_spmv_sub(const int *__restrict__ rp, co
         }
         if (K == 1) {
             VT sum = 0;
-            // unrolled: several column loads issue before their x gathers (same summation order)
+            // unrolled: several column loads issue before their x gathers
+            // (same summation order).  Aligned pairs of entries per lane (one
+            // 16-byte value load) measured no faster on the power-law factor:
+            // its short rows left half of each lane group idle.
 #pragma unroll 4
             for (int k = s + sl; k < e; k += g) sum += val[k] * x[col[k]];
             for (int off = g >> 1; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off, g);

@@ -37,6 +37,7 @@ inline void attr_mark(std::atomic<unsigned long long> &seen) {
 
 struct DeviceState {
     int device = 0, num_sms = 148;
+    int smem_sm = 233472, smem_reserved = 1024;  // shared memory per SM, reserved per CTA
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -64,8 +65,14 @@ struct DeviceState {
     LcChunk *lc_tab = nullptr;
     LcSeg *lc_segs = nullptr;
     int *lc_queue = nullptr;                              // one segment counter per triangle
-    cudaStream_t side = nullptr;                         // L2 prefetch stream
+    cudaStream_t side = nullptr;                         // L2 prefetch stream; moves of the overlapped walk
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    double **iotab = nullptr;                            // caller's columns for the overlapped walk (k_set_io)
+    int *io_rows = nullptr;                              // per triangle, its original rows ascending (n entries)
+    // x work vector left without its sentinel by an overlapped walk (which
+    // polls nothing); refilled before the next walk of that precision
+    bool xw_dirty64 = false, xw_dirty32 = false;
+    std::vector<cudaEvent_t> ov_ev;                      // per-triangle events of the overlapped walk
     int *tickets = nullptr, *status = nullptr, *h_status = nullptr;
     int ntri = 0;
     // work vectors for kcap right-hand sides
@@ -231,6 +238,7 @@ int ensure_work(Plan &P, int K, std::string &err) {
     if (D.mixed)
         k_fill<float><<<grid_for((long long)cnt, 256, D.num_sms), 256, 0, D.stream>>>(D.xw32, (long long)cnt,
                                                                                        sent32_host());
+    D.xw_dirty64 = D.xw_dirty32 = false;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         err = std::string("ensure_work: ") + cudaGetErrorString(e);
@@ -252,6 +260,8 @@ template <> struct Pools<double> {
     static const unsigned char *lcrec(const DeviceState &D) { return reinterpret_cast<const unsigned char *>(D.lc_rec64); }
     static double *bw(const DeviceState &D) { return D.bw64; }
     static double *xw(const DeviceState &D) { return D.xw64; }
+    static bool &dirty(DeviceState &D) { return D.xw_dirty64; }
+    static double sent() { return sent64_host(); }
 };
 template <> struct Pools<float> {
     static const float *val(const DeviceState &D) { return D.val32; }
@@ -263,6 +273,8 @@ template <> struct Pools<float> {
     static const unsigned char *lcrec(const DeviceState &D) { return reinterpret_cast<const unsigned char *>(D.lc_rec32); }
     static float *bw(const DeviceState &D) { return D.bw32; }
     static float *xw(const DeviceState &D) { return D.xw32; }
+    static bool &dirty(DeviceState &D) { return D.xw_dirty32; }
+    static float sent() { return sent32_host(); }
 };
 
 template <typename VT, int K>
@@ -361,19 +373,21 @@ template <typename VT> constexpr int ca_stages(int W, int G) {
     return W == 4 ? 2 : 4;
 }
 
-// Right-hand sides per CTA of a staged level triangle solved for K columns:
-// the column groups all read the same row data (columns, values, inverse
-// diagonal) at about the same time, and their waits on L2 grow with their
-// number, so two columns per CTA (half the groups) measured faster than one
-// at 8 and 32 columns and the same at 128.  RBS_CA_GROUP (1 or 2) overrides
-// the choice.
+// Right-hand sides per CTA of a staged level triangle solved for K columns.
+// One column per CTA walks a level fastest (half the shared-memory traffic
+// per row), but takes an SM per column; the overlapped walk moves the
+// columns in and out on the SMs the triangles leave free.  On the 2D
+// Laplacian (n = 1M, FP64) one column per CTA measured 20.4k solves/s
+// against 17.6k at 32 columns, two columns per CTA 49.4k against 37.7k at
+// 128 (with 128 CTAs only 20 SMs were left for the moves).  RBS_CA_GROUP
+// (1 or 2) overrides the choice.
 template <typename VT> int ca_group(const ExecBlock &B, int K) {
     if (K == 1) return 1;
     static const int forced = [] {
         const char *e = std::getenv("RBS_CA_GROUP");
         return e ? std::atoi(e) : 0;
     }();
-    int G = forced == 1 || forced == 2 ? forced : 2;
+    int G = forced == 1 || forced == 2 ? forced : K <= 64 ? 1 : 2;
     if (G == 2 && ca_stages<VT>(B.ca_w, 2) == 0) G = 1;
     return G;
 }
@@ -474,6 +488,23 @@ void launch_ca_any(const ExecBlock &B, const CaDesc *desc, int K, int G, cudaStr
     }
 }
 
+// Shared memory of the staged level kernel as launch_ca_any picks it.
+template <typename VT>
+size_t ca_smem_bytes(int W, int K, int G) {
+    if (K == 1 || G == 1) {
+        if (W == 1) return CaLayout<VT, 1, 4, 1>::total;
+        if (W == 2) return CaLayout<VT, 2, 4, 1>::total;
+        return CaLayout<VT, 4, 2, 1>::total;
+    }
+    if constexpr (sizeof(VT) == 8) {
+        return W == 1 ? CaLayout<VT, 1, 2, 2>::total : CaLayout<VT, 2, 2, 2>::total;
+    } else {
+        if (W == 1) return CaLayout<VT, 1, 4, 2>::total;
+        if (W == 2) return CaLayout<VT, 2, 4, 2>::total;
+        return CaLayout<VT, 4, 2, 2>::total;
+    }
+}
+
 template <typename VT>
 constexpr int lc_smem() {
     return LC_RING + LC_XW * (int)sizeof(VT) + LC_NB * 8;
@@ -543,9 +574,159 @@ int run_band(Plan &P, const ExecBlock &B, const VT *bb, VT *xx, int K, std::stri
     return RBS_OK;
 }
 
+// Grouped-layout moves of the processing positions [pa, pb) on stream st
+// (the whole vector, or one triangle's rows inside the overlapped walk).
+// smem: dynamic shared memory the launch reserves and does not use (0, or
+// move_reserve's choice on the overlapped walk's side stream).
+//
+// The overlapped walk's side-stream moves reserve just more shared memory
+// than an SM running one of the plan's staged triangles has left
+// (move_reserve), so they cannot share an SM with a triangle's CTA and slow
+// its level chain, as long as eight move CTAs of 256 threads still fit on an
+// idle SM.  Fewer resident move threads measured slower than the sharing
+// costs: 768 per SM took 2.5x as long per launch, 2048 in CTAs of 512 with
+// a 42 KB reservation 1.4-1.9x, and the 128-column solve lost 14% with them.
+constexpr int MOVE_SMEM_MAX = 64 << 10;
+
+template <typename F>
+void move_attr(F *kernel, std::atomic<unsigned long long> &done) {
+    if (attr_done(done)) return;
+    // a failure here surfaces as the launch error of the move itself
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MOVE_SMEM_MAX) == cudaSuccess)
+        attr_mark(done);
+}
+
+template <typename VT, typename VT2, int K, int GL>
+void launch_gather_grp(cudaStream_t st, int smem, const double *b, int ld, const double *const *cols, int k,
+                       const int *perm, int n, int pa, int pb, VT *out, VT2 *out2, GroupCols grp) {
+    static std::atomic<unsigned long long> done{0};
+    if (smem) move_attr(k_gather_grp<VT, VT2, K, GL>, done);
+    const unsigned gx = (unsigned)((pb - pa + 255) / 256);
+    k_gather_grp<VT, VT2, K, GL><<<dim3(gx, GroupTile<K, GL>::CHUNKS), 256, smem, st>>>(b, ld, cols, k, perm, n, pa,
+                                                                                       pb, out, out2, grp);
+}
+
+template <typename VT, typename VT2, int K>
+void gather_grp(const DeviceState &D, cudaStream_t st, int n, const double *b, int ld, const double *const *cols,
+                int k, VT *out, VT2 *out2, int GL, GroupCols grp, int pa, int pb, int smem = 0) {
+    if (pb <= pa) return;
+    if (GL == 1)
+        launch_gather_grp<VT, VT2, K, 1>(st, smem, b, ld, cols, k, D.perm, n, pa, pb, out, out2, grp);
+    else if constexpr (K % 2 == 0)
+        launch_gather_grp<VT, VT2, K, 2>(st, smem, b, ld, cols, k, D.perm, n, pa, pb, out, out2, grp);
+}
+
+template <typename VT, int K, bool RESET>
+void scatter_grp(const DeviceState &D, cudaStream_t st, int n, VT *xw, int k, double *x, int ld,
+                 double *const *cols, int GL, GroupCols grp, int pa, int pb) {
+    if (pb <= pa) return;
+    const unsigned gx = (unsigned)((pb - pa + 255) / 256);
+    if (GL == 1) {
+        k_scatter_grp<VT, K, 1, RESET><<<dim3(gx, GroupTile<K, 1>::CHUNKS), 256, 0, st>>>(xw, D.perm, n, k, pa, pb, x,
+                                                                                          ld, cols, grp);
+    } else if constexpr (K % 2 == 0) {
+        k_scatter_grp<VT, K, 2, RESET><<<dim3(gx, GroupTile<K, 2>::CHUNKS), 256, 0, st>>>(xw, D.perm, n, k, pa, pb, x,
+                                                                                          ld, cols, grp);
+    }
+}
+
+template <typename VT, int K, int GL>
+void launch_scatter_rows(const DeviceState &D, cudaStream_t st, int n, const VT *xw, double *const *cols, int qa,
+                         int qb, int smem) {
+    using T = GroupTile<K, GL>;
+    constexpr int TR = 256 / T::GT;
+    static std::atomic<unsigned long long> done{0};
+    if (smem) move_attr(k_scatter_rows<VT, K, GL>, done);
+    const unsigned gx = (unsigned)((qb - qa + TR - 1) / TR);
+    k_scatter_rows<VT, K, GL><<<dim3(gx, T::CHUNKS), 256, smem, st>>>(xw, D.io_rows, D.ipos, n, qa, qb, cols);
+}
+
+template <typename VT, int K>
+void scatter_rows(const DeviceState &D, cudaStream_t st, int n, const VT *xw, double *const *cols, int GL, int qa,
+                  int qb, int smem = 0) {
+    if (qb <= qa) return;
+    if (GL == 1) launch_scatter_rows<VT, K, 1>(D, st, n, xw, cols, qa, qb, smem);
+    else if constexpr (K % 2 == 0) launch_scatter_rows<VT, K, 2>(D, st, n, xw, cols, qa, qb, smem);
+}
+
+// The overlapped walk (several columns, grouped layout): the triangles, in
+// walk order, partition the rows; the right-hand sides of triangle j are
+// moved in before the first block that touches its rows (need: the last
+// triangle whose rows a block reads or updates in the b work vector) and its
+// solutions moved out after the last block that reads them (last_use).
+struct IoSchedule {
+    std::vector<int> r0, r1;      // triangle j: processing rows [r0[j], r1[j])
+    std::vector<int> need;        // per block
+    std::vector<int> last_use;    // per triangle: block index
+    bool ok = false;
+};
+
+IoSchedule io_schedule(const Plan &P) {
+    IoSchedule S;
+    const int nb = (int)P.blocks.size();
+    for (const ExecBlock &B : P.blocks)
+        if (B.tri) {
+            if (B.r0 != (S.r1.empty() ? 0 : S.r1.back())) return S;  // not a partition in walk order
+            S.r0.push_back(B.r0);
+            S.r1.push_back(B.r0 + B.m);
+        }
+    if (S.r1.empty() || S.r1.back() != P.n) return S;
+    auto tri_of = [&](int row) {
+        return (int)(std::upper_bound(S.r0.begin(), S.r0.end(), row) - S.r0.begin()) - 1;
+    };
+    S.need.assign(nb, 0);
+    S.last_use.assign(S.r0.size(), 0);
+    for (int bi = 0, j = 0; bi < nb; ++bi) {
+        const ExecBlock &B = P.blocks[bi];
+        S.need[bi] = B.m > 0 ? tri_of(B.r0 + B.m - 1) : 0;
+        if (B.tri) {
+            S.last_use[j] = std::max(S.last_use[j], bi);
+            ++j;
+        } else if (B.ncols > 0) {
+            for (int t = tri_of(B.c0); t <= tri_of(B.c0 + B.ncols - 1); ++t) S.last_use[t] = std::max(S.last_use[t], bi);
+        }
+    }
+    S.ok = true;
+    return S;
+}
+
+// The sorted row lists of the overlapped walk's scatter (k_scatter_rows),
+// built on the host once per plan, outside any stream capture.  A plan whose
+// triangles do not partition the rows in walk order gets none, and its walk
+// moves the whole vectors before and after the blocks.
+int ensure_io_rows(Plan &P, std::string &err) {
+    DeviceState &D = *P.dev;
+    if (D.io_rows || (long long)P.perm.size() != (long long)P.n) return RBS_OK;
+    const IoSchedule S = io_schedule(P);
+    if (!S.ok) return RBS_OK;
+    std::vector<int> rows(P.perm.begin(), P.perm.end());
+    for (size_t j = 0; j < S.r0.size(); ++j) std::sort(rows.begin() + S.r0[j], rows.begin() + S.r1[j]);
+    return upload(D, D.io_rows, rows, err);
+}
+
+// Dynamic shared memory of the side-stream moves next to staged triangles
+// of at least ca_min bytes: one byte more than such an SM has left, rounded
+// up to 1 KB, when eight move CTAs still fit on an idle SM; 0 otherwise (or
+// when no triangle is staged).  RBS_MOVE_SMEM (bytes, at most 64 KB)
+// overrides the choice.
+int move_reserve(const DeviceState &D, size_t ca_min) {
+    static const long long forced = [] {
+        const char *e = std::getenv("RBS_MOVE_SMEM");
+        return e ? std::atoll(e) : -1LL;
+    }();
+    if (forced >= 0) return (int)std::min<long long>(forced, MOVE_SMEM_MAX);
+    if (!ca_min) return 0;
+    const long long left = (long long)D.smem_sm - (long long)ca_min - D.smem_reserved;  // beside one triangle
+    long long need = left - D.smem_reserved + 1;  // a move CTA needs its own reservation too
+    if (need <= 0) return 0;
+    need = (need + 1023) / 1024 * 1024;
+    if (8 * (need + D.smem_reserved) > D.smem_sm) return 0;
+    return (int)need;
+}
+
 // One pass over all blocks: triangles solve into xw, squares update bw.
 template <typename VT, int K>
-int launch_blocks(Plan &P, std::string &err) {
+int launch_blocks(Plan &P, std::string &err, bool io = false) {
     DeviceState &D = *P.dev;
     cudaStream_t st = D.stream;
     const VT *val = Pools<VT>::val(D);
@@ -610,8 +791,55 @@ int launch_blocks(Plan &P, std::string &err) {
             }
         }
     }
+    // Overlapped walk (io: several columns in the grouped layout, the caller's
+    // columns in D.iotab): the first triangle's right-hand sides are moved in
+    // on the walk's stream, the other triangles' on the side stream, in walk
+    // order, each followed by an event the first block that needs it waits
+    // for; solutions go out on the side stream as blocks free them.  The moves
+    // run on the SMs the walk leaves idle.
+    io = io && K > 1 && GL > 0;
+    IoSchedule S;
+    std::vector<std::vector<int>> freed;  // per block: triangles whose solutions it is the last to read
+    int waited = 0, T = 0, move_smem = 0;
+    if (io) {
+        S = io_schedule(P);
+        if (!D.io_rows) S.ok = false;
+        T = (int)S.r0.size();
+        if (!S.ok) {
+            gather_grp<VT, VT, K>(D, st, P.n, nullptr, P.n, D.iotab, K, bw, (VT *)nullptr, GL, GroupCols{}, 0, P.n);
+        } else {
+            while ((int)D.ov_ev.size() < 2 * T) {
+                cudaEvent_t e = nullptr;
+                CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                D.ov_ev.push_back(e);
+            }
+            size_t ca_min = 0;
+            for (const ExecBlock &B : P.blocks)
+                if (B.tri && B.kernel == RBS_K_LEVEL && B.ca_ok) {
+                    const size_t v = ca_smem_bytes<VT>(B.ca_w, K, GL);
+                    ca_min = ca_min ? std::min(ca_min, v) : v;
+                }
+            move_smem = move_reserve(D, ca_min);
+            CK(cudaEventRecord(D.ev_fork, st));
+            CK(cudaStreamWaitEvent(D.side, D.ev_fork, 0));
+            gather_grp<VT, VT, K>(D, st, P.n, nullptr, P.n, D.iotab, K, bw, (VT *)nullptr, GL, GroupCols{}, S.r0[0],
+                                  S.r1[0]);
+            for (int j = 1; j < T; ++j) {
+                gather_grp<VT, VT, K>(D, D.side, P.n, nullptr, P.n, D.iotab, K, bw, (VT *)nullptr, GL, GroupCols{},
+                                      S.r0[j], S.r1[j], move_smem);
+                CK(cudaEventRecord(D.ov_ev[j], D.side));
+            }
+            freed.assign(P.blocks.size(), {});
+            for (int j = 0; j < T; ++j) freed[S.last_use[j]].push_back(j);
+        }
+    }
     int ti = 0, li = 0, eti = 0, cti = 0;
     for (const ExecBlock &B : P.blocks) {
+        const int bi = (int)(&B - P.blocks.data());
+        if (io && S.ok && S.need[bi] > waited) {
+            CK(cudaStreamWaitEvent(st, D.ov_ev[S.need[bi]], 0));
+            waited = S.need[bi];
+        }
         if (D.profile) CK(cudaEventRecord(D.bev[2 * B.index], st));
         if (B.tri) {
             const VT *bb = bw + (long long)B.r0 * K;
@@ -710,6 +938,22 @@ int launch_blocks(Plan &P, std::string &err) {
                                                                   xw + (long long)B.c0 * K, bw + (long long)B.r0 * K);
         }
         if (D.profile) CK(cudaEventRecord(D.bev[2 * B.index + 1], st));
+        if (!freed.empty())
+            for (int j : freed[bi]) CK(cudaEventRecord(D.ov_ev[T + j], st));
+    }
+    if (io) {
+        double *const *xcols = D.iotab + RBS_IO_COLS;
+        if (S.ok) {
+            for (const auto &fj : freed)
+                for (int j : fj) {
+                    CK(cudaStreamWaitEvent(D.side, D.ov_ev[T + j], 0));
+                    scatter_rows<VT, K>(D, D.side, P.n, xw, xcols, GL, S.r0[j], S.r1[j], move_smem);
+                }
+            CK(cudaEventRecord(D.ev_join, D.side));
+            CK(cudaStreamWaitEvent(st, D.ev_join, 0));
+        } else {
+            scatter_grp<VT, K, true>(D, st, P.n, xw, K, nullptr, P.n, xcols, GL, GroupCols{}, 0, P.n);
+        }
     }
     if (forked) {
         CK(cudaEventRecord(D.ev_join, D.side));
@@ -723,13 +967,32 @@ int launch_blocks(Plan &P, std::string &err) {
 // its second use (the first runs eagerly and performs the one-time set-up
 // that capture does not allow) and replayed afterwards: one launch per
 // solve pass instead of one per block.
+// Whether the block walk for K columns runs a kernel that polls the x work
+// vector for its sentinel (the sync-free kernels), with the kernel choice
+// of launch_blocks.
+bool walk_polls(const Plan &P, int K) {
+    for (const ExecBlock &B : P.blocks) {
+        if (!B.tri) continue;
+        if (B.kernel == RBS_K_SYNCFREE) return true;
+        if (B.kernel != RBS_K_LEVEL) continue;
+        if (K > 1 && !B.ca_ok) return true;  // multi-column level triangles without the staged layout
+        if (K == 1 && B.lvl_var == LVL_CSF && B.ell_ok) return true;
+    }
+    return false;
+}
+
 template <typename VT, int K>
-int run_blocks(Plan &P, std::string &err) {
+int run_blocks(Plan &P, std::string &err, bool io = false) {
     DeviceState &D = *P.dev;
+    if (!io && Pools<VT>::dirty(D) && walk_polls(P, K)) {  // the sync-free kernels poll x for the sentinel
+        const long long cnt = (long long)P.n * D.kcap;
+        k_fill<VT><<<grid_for(cnt, 256, D.num_sms), 256, 0, D.stream>>>(Pools<VT>::xw(D), cnt, Pools<VT>::sent());
+        Pools<VT>::dirty(D) = false;
+    }
     // per-block timing needs real event timestamps, which captured event
     // records are not: profiled solves launch eagerly
-    if (!D.use_graphs || D.profile) return launch_blocks<VT, K>(P, err);
-    const long long key = (long long)K * 8 + (sizeof(VT) == 8 ? 0 : 2);
+    if (!D.use_graphs || D.profile) return launch_blocks<VT, K>(P, err, io);
+    const long long key = (long long)K * 8 + (sizeof(VT) == 8 ? 0 : 2) + (io ? 4 : 0);
     auto it = D.graphs.find(key);
     if (it != D.graphs.end()) {
         CK(cudaGraphLaunch(it->second, D.stream));
@@ -737,11 +1000,11 @@ int run_blocks(Plan &P, std::string &err) {
     }
     if (!D.graph_seen.count(key)) {
         D.graph_seen.insert(key);
-        return launch_blocks<VT, K>(P, err);
+        return launch_blocks<VT, K>(P, err, io);
     }
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(D.stream, cudaStreamCaptureModeThreadLocal));
-    int rc = launch_blocks<VT, K>(P, err);
+    int rc = launch_blocks<VT, K>(P, err, io);
     cudaError_t e = cudaStreamEndCapture(D.stream, &g);
     if (rc) {
         if (g) cudaGraphDestroy(g);
@@ -752,7 +1015,8 @@ int run_blocks(Plan &P, std::string &err) {
         return RBS_ERR_CUDA;
     }
     cudaGraphExec_t ex = nullptr;
-    e = cudaGraphInstantiate(&ex, g, 0);
+    // captured kernels keep the priority of the stream they were captured on
+    e = cudaGraphInstantiate(&ex, g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
         err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
@@ -771,18 +1035,16 @@ void drop_graphs(DeviceState &D) {
 void drop_graphs_fwd(DeviceState &D) { drop_graphs(D); }
 
 // Right-hand sides into processing order: the caller's columns (b + c*ld,
-// or the device table cols) into the row-interleaved work vector out (and
-// out2 in a second precision, when given).  Many columns take the
-// transposing tile kernel, whose reads and writes are both coalesced.
+// or the device table cols) into the work vector out (and out2 in a second
+// precision, when given): grouped (GL > 0) by one thread per processing
+// position and chunk of column groups, row-interleaved with many columns by
+// the transposing tile kernel, whose reads and writes are both coalesced.
 template <typename VT, typename VT2, int K>
 void gather_in(DeviceState &D, int n, const double *b, int ld, const double *const *cols, int k, VT *out,
                VT2 *out2, int GL, GroupCols grp = GroupCols{}) {
     const int tgrid = std::max(1, (int)std::min<long long>(((long long)n + TP_ROWS - 1) / TP_ROWS, (long long)D.num_sms * 8));
-    if (GL == 1) {
-        k_gather_p<VT, VT2, K, 1><<<tgrid, 256, 0, D.stream>>>(b, ld, cols, k, D.perm, n, out, out2, grp);
-    } else if (GL == 2) {
-        if constexpr (K % 2 == 0)
-            k_gather_p<VT, VT2, K, 2><<<tgrid, 256, 0, D.stream>>>(b, ld, cols, k, D.perm, n, out, out2, grp);
+    if (GL) {
+        gather_grp<VT, VT2, K>(D, D.stream, n, b, ld, cols, k, out, out2, GL, grp, 0, n);
     } else if (K >= 8 || grp.tab) {
         k_gather_t<VT, VT2, K><<<tgrid, 256, 0, D.stream>>>(b, ld, cols, k, D.ipos, n, out, out2, grp);
     } else {
@@ -802,10 +1064,8 @@ template <typename VT, int K, bool RESET>
 void scatter_out(DeviceState &D, int n, VT *xw, int k, double *x, int ld, double *const *cols, int GL,
                  GroupCols grp = GroupCols{}) {
     const int tgrid = std::max(1, (int)std::min<long long>(((long long)n + TP_ROWS - 1) / TP_ROWS, (long long)D.num_sms * 8));
-    if (GL == 1) {
-        k_scatter_t<VT, K, RESET, 1><<<tgrid, 256, 0, D.stream>>>(xw, D.ipos, n, k, x, ld, cols, grp);
-    } else if (GL == 2) {
-        k_scatter_t<VT, K, RESET, 2><<<tgrid, 256, 0, D.stream>>>(xw, D.ipos, n, k, x, ld, cols, grp);
+    if (GL) {
+        scatter_grp<VT, K, RESET>(D, D.stream, n, xw, k, x, ld, cols, GL, grp, 0, n);
     } else if (K >= 8 || grp.tab) {
         k_scatter_t<VT, K, RESET><<<tgrid, 256, 0, D.stream>>>(xw, D.ipos, n, k, x, ld, cols, grp);
     } else {
@@ -821,10 +1081,22 @@ void scatter_out(DeviceState &D, int n, VT *xw, int k, double *x, int ld, double
     }
 }
 
+// Several columns in the grouped layout: the walk moves the columns itself,
+// overlapped with the blocks (launch_blocks), reading them through the device
+// table D.iotab set just before it on the same stream.
 template <int K>
 int solve_fp64(Plan &P, const double *b, double *x, int k, int ld, std::string &err) {
     DeviceState &D = *P.dev;
     const int GL = plan_group<double>(P, K);
+    if (K > 1 && GL) {
+        int rc = ensure_io_rows(P, err);
+        if (rc) return rc;
+        k_set_io<<<1, RBS_IO_COLS, 0, D.stream>>>(D.iotab, b, x, ld, k);
+        if ((rc = run_blocks<double, K>(P, err, true))) return rc;
+        D.xw_dirty64 = true;
+        CK(cudaGetLastError());
+        return RBS_OK;
+    }
     gather_in<double, double, K>(D, P.n, b, ld, nullptr, k, D.bw64, nullptr, GL);
     int rc = run_blocks<double, K>(P, err);
     if (rc) return rc;
@@ -837,6 +1109,15 @@ template <int K>
 int solve_fp32(Plan &P, const double *b, double *x, int k, int ld, std::string &err) {
     DeviceState &D = *P.dev;
     const int GL = plan_group<float>(P, K);
+    if (K > 1 && GL) {
+        int rc = ensure_io_rows(P, err);
+        if (rc) return rc;
+        k_set_io<<<1, RBS_IO_COLS, 0, D.stream>>>(D.iotab, b, x, ld, k);
+        if ((rc = run_blocks<float, K>(P, err, true))) return rc;
+        D.xw_dirty32 = true;
+        CK(cudaGetLastError());
+        return RBS_OK;
+    }
     gather_in<float, float, K>(D, P.n, b, ld, nullptr, k, D.bw32, nullptr, GL);
     int rc = run_blocks<float, K>(P, err);
     if (rc) return rc;
@@ -1085,7 +1366,14 @@ int device_build(Plan &P, std::string &err) {
     if (P.opt.device >= 0) CK(cudaSetDevice(P.opt.device));
     CK(cudaGetDevice(&D.device));
     CK(cudaDeviceGetAttribute(&D.num_sms, cudaDevAttrMultiProcessorCount, D.device));
-    CK(cudaStreamCreateWithFlags(&D.stream, cudaStreamNonBlocking));
+    CK(cudaDeviceGetAttribute(&D.smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, D.device));
+    CK(cudaDeviceGetAttribute(&D.smem_reserved, cudaDevAttrReservedSharedMemoryPerBlock, D.device));
+    // The walk's stream at the greatest priority, its side stream (prefetch,
+    // the overlapped walk's moves) at the lowest: when both have CTAs
+    // waiting, an SM that frees up takes the walk's.
+    int prio_low = 0, prio_high = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    CK(cudaStreamCreateWithPriority(&D.stream, cudaStreamNonBlocking, prio_high));
     D.own_stream = true;
     CK(cudaEventCreate(&D.ev0));
     CK(cudaEventCreate(&D.ev1));
@@ -1165,10 +1453,15 @@ int device_build(Plan &P, std::string &err) {
         if ((rc = upload(D, D.lc_segs, segs, err))) return rc;
         if ((rc = alloc(D, D.lc_queue, (size_t)(1 << P.lv), err))) return rc;
     }
-    CK(cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
+    {
+        int prio_low = 0, prio_high = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+        CK(cudaStreamCreateWithPriority(&D.side, cudaStreamNonBlocking, prio_low));
+    }
     CK(cudaEventCreateWithFlags(&D.ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&D.ev_join, cudaEventDisableTiming));
     D.ntri = 1 << P.lv;
+    if ((rc = alloc(D, D.iotab, 2 * RBS_IO_COLS, err))) return rc;
     if ((rc = alloc(D, D.tickets, (size_t)D.ntri, err))) return rc;
     if ((rc = alloc(D, D.status, 1, err))) return rc;
     if ((rc = alloc(D, D.norms, 2 * 128, err))) return rc;
@@ -1404,6 +1697,9 @@ void device_free(Plan &P) {
     if (D.side) cudaStreamDestroy(D.side);
     if (D.ev_fork) cudaEventDestroy(D.ev_fork);
     if (D.ev_join) cudaEventDestroy(D.ev_join);
+    for (auto &e : D.ov_ev) cudaEventDestroy(e);
+    cudaFree(D.iotab);
+    cudaFree(D.io_rows);
     cudaFree(D.ell_col);
     cudaFree(D.ell_val);
     cudaFree(D.ell_val32);
@@ -1446,7 +1742,9 @@ int device_set_stream(Plan &P, void *stream, std::string &err) {
         D.stream = (cudaStream_t)stream;
         D.own_stream = false;
     } else {
-        CK(cudaStreamCreateWithFlags(&D.stream, cudaStreamNonBlocking));
+        int prio_low = 0, prio_high = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+        CK(cudaStreamCreateWithPriority(&D.stream, cudaStreamNonBlocking, prio_high));
         D.own_stream = true;
     }
     return RBS_OK;
@@ -1467,6 +1765,7 @@ int device_sync(Plan &P, std::string &err) {
         if (D.xw32)
             k_fill<float><<<grid_for((long long)cnt, 256, D.num_sms), 256, 0, D.stream>>>(
                 D.xw32, (long long)cnt, sent32_host());
+        D.xw_dirty64 = D.xw_dirty32 = false;
         CK(cudaStreamSynchronize(D.stream));
         err = "a device wait exceeded its poll budget (dependency never produced)";
         return RBS_ERR_TIMEOUT;

@@ -147,6 +147,36 @@ def test_multi_rhs_staged_level_triangles(cuda, grid, sub):
                 assert rel_err(X[c], Xref[c]) <= tol, (k, prec, c)
 
 
+@pytest.mark.parametrize("select", [rbs.SELECT_AUTO, rbs.SELECT_TUNE])
+def test_overlapped_walk_alternating_widths(cuda, select):
+    # grouped multi-column solves move the columns inside the block walk
+    # (triangle by triangle, on a second stream) and leave the x work vector
+    # without its sentinel; a single-column walk afterwards (under TUNE it may
+    # poll for the sentinel) refills it first.  Widths, precisions and a
+    # leading dimension larger than n alternate, twice (eager, then graph
+    # replays); every column against the oracle.
+    import torch
+    rp, ci, va = rbs.gen_lower_csr(rbs.GEN_LAPLACE2D, grid=200, seed=41)
+    cp, ri, cv = oracle.transpose(rp, ci, va)
+    n = len(cp) - 1
+    plan = rbs.analyse(cp, ri, cv, substitution=rbs.FORWARD, lv=-1, opts=rbs.options(select=select))
+    seq = [(8, rbs.PREC_FP64, n), (1, rbs.PREC_FP64, n), (8, rbs.PREC_FP32, n), (8, rbs.PREC_MIXED, n),
+           (1, rbs.PREC_FP64, n), (3, rbs.PREC_FP64, n + 7), (1, rbs.PREC_FP32, n), (16, rbs.PREC_FP64, n)]
+    for rep in range(2):
+        for q, (k, prec, ld) in enumerate(seq):
+            B, Xref = system(cp, ri, cv, rbs.FORWARD, k=k, seed=1000 * rep + 50 * q)
+            hb = np.zeros((k, ld))
+            hb[:, :n] = B
+            db = torch.tensor(hb, dtype=torch.float64, device=cuda).reshape(-1)
+            dx = torch.full_like(db, float("nan"))
+            plan.solve(db, dx, k=k, ld=ld, prec=prec)
+            X = dx.cpu().numpy().reshape(k, ld)
+            assert np.isnan(X[:, n:]).all(), (rep, q)  # padding rows of the caller's columns untouched
+            tol = 1e-5 if prec == rbs.PREC_FP32 else TOL
+            for c in range(k):
+                assert rel_err(X[c, :n], Xref[c]) <= tol, (rep, q, k, prec, c)
+
+
 def test_host_async_pipelined(cuda):
     # several asynchronous host-array solves in flight on two staging slots,
     # pinned buffers, widths 1 and 3 (a wider call drains and regrows the
