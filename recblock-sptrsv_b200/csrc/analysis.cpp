@@ -1081,7 +1081,13 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
         int W = 1;
         while (W < std::max(1, B.bandwidth)) W <<= 1;
         B.band_w = W;
+        // rows per chunk: halved from 16 while the triangle has fewer chunks
+        // than two CTAs of 256 per SM of a 148-SM part would take, down to
+        // max(4, W) rows (below W the chunks' share of the scans outweighs
+        // their row steps); 125,000 rows: 4-row chunks, 123 CTAs
         B.band_c = 16;
+        while (B.band_c > std::max(4, W) && ((long long)B.m + B.band_c - 1) / B.band_c < 2LL * 148 * 256)
+            B.band_c >>= 1;
         B.band_nch = (B.m + B.band_c - 1) / B.band_c;
         B.band_off = (long long)P.band_coef.size();
         const long long slots = (long long)B.band_nch * B.band_c;

@@ -8,11 +8,20 @@
 // -a_p / l_pp and whose other rows shift the state.  Maps compose
 // associatively, so a chain of m rows is solved in three passes instead of
 // m dependent steps:
-//   1. k_band_maps   : each thread composes the maps of C consecutive rows;
-//   2. k_band_scan   : one CTA scans the chunk maps (sequential per thread,
-//                      Kogge-Stone across threads) into each chunk's
-//                      entering state;
-//   3. k_band_replay : each thread replays its rows from that state.
+//   1. k_band_maps   : each thread composes the maps of C consecutive rows
+//                      (a chunk); the CTA's BAND_T chunk maps are scanned in
+//                      shared memory (Kogge-Stone), giving each chunk the
+//                      composition of its CTA's chunks up to it, and the CTA
+//                      its total;
+//   2. k_band_scan   : one CTA scans the CTA totals (sequential per thread,
+//                      Kogge-Stone across threads) into each CTA's entering
+//                      state;
+//   3. k_band_replay : each thread applies the previous chunk's in-CTA
+//                      composition to its CTA's entering state and replays
+//                      its rows from there.
+// The first form scanned every chunk map in the one CTA of pass 2 (31
+// sequential compositions per thread for 125,000 rows, each waiting on its
+// loads): 122 us of a 155 us triangle on the banded chain.
 // Band coefficients are stored chunk-interleaved (row i of chunk j at
 // [(i*nch + j)*W]) so the threads of a warp read consecutive addresses.
 // For diagonally dominant rows every ||M_p||_inf <= 1, so composed maps stay
@@ -48,19 +57,75 @@ __device__ __forceinline__ void band_step_M(VT (&M)[W][W], VT (&c)[W], const VT 
     c[0] = c0;
 }
 
+// Chunks per CTA of the maps and replay passes (the CTA-level scan's width).
+constexpr int BAND_T = 256;
+
+__host__ __device__ constexpr int band_blocks(int nch) { return (nch + BAND_T - 1) / BAND_T; }
+
+// (M, c) <- (M, c) o (Me, ce), the earlier map Me read from memory:
+// M = M Me,  c = M ce + c
+template <typename VT, int W>
+__device__ __forceinline__ void band_compose_before(VT (&M)[W][W], VT (&c)[W], const VT *e) {
+    VT nM[W][W], nc[W];
+#pragma unroll
+    for (int r = 0; r < W; ++r) {
+        VT s = c[r];
+#pragma unroll
+        for (int k = 0; k < W; ++k) s += M[r][k] * e[W * W + k];
+        nc[r] = s;
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+            VT t = 0;
+#pragma unroll
+            for (int k = 0; k < W; ++k) t += M[r][k] * e[k * W + q];
+            nM[r][q] = t;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < W; ++r) {
+        c[r] = nc[r];
+#pragma unroll
+        for (int q = 0; q < W; ++q) M[r][q] = nM[r][q];
+    }
+}
+
+// Inclusive Kogge-Stone scan of one (M, c) per thread over the CTA, through
+// sm (blockDim.x * (W*W + W) values): thread t ends with map_t o ... o map_0.
+template <typename VT, int W>
+__device__ __forceinline__ void band_cta_scan(VT (&M)[W][W], VT (&c)[W], VT *sm) {
+    constexpr int E = W * W + W;
+    const int tid = threadIdx.x, T = blockDim.x;
+    for (int off = 1; off < T; off <<= 1) {
+        VT *mine = sm + (long long)tid * E;
+#pragma unroll
+        for (int r = 0; r < W; ++r) {
+#pragma unroll
+            for (int q = 0; q < W; ++q) mine[r * W + q] = M[r][q];
+            mine[W * W + r] = c[r];
+        }
+        __syncthreads();
+        if (tid >= off) band_compose_before<VT, W>(M, c, sm + (long long)(tid - off) * E);
+        __syncthreads();
+    }
+}
+
 // Several right-hand sides run side by side in one launch of each pass:
 // column c = blockIdx.y of the maps and replay passes (blockIdx.x of the
-// scan), with its own maps and states at c * nch * (W*W + W) and c * nch * W.
+// scan), with its own maps at c * (nch + nblk) * (W*W + W) (the chunks'
+// in-CTA prefixes, then the CTA totals) and states at c * nblk * W.
 //
-// Pass 1: maps[j] = composition of the row maps of chunk j.
+// Pass 1: maps[j] = the row maps of chunk j composed, then composed after
+// those of the chunks before it in its CTA; maps[nch + blk] = CTA blk's
+// total.  Chunks past nch are identity maps.
 template <typename VT, int W>
-__global__ void __launch_bounds__(256) k_band_maps(const VT *__restrict__ coef, const VT *__restrict__ inv,
-                                                   const VT *__restrict__ b, int K, int m, int C, int nch,
-                                                   VT *__restrict__ maps) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(BAND_T) k_band_maps(const VT *__restrict__ coef, const VT *__restrict__ inv,
+                                                      const VT *__restrict__ b, int K, int m, int C, int nch,
+                                                      VT *__restrict__ maps) {
+    extern __shared__ unsigned char smem_raw[];
+    constexpr int E = W * W + W;
+    const int j = blockIdx.x * BAND_T + threadIdx.x;
     const int colk = blockIdx.y;
-    maps += (long long)colk * nch * (W * W + W);
-    if (j >= nch) return;
+    maps += (long long)colk * (nch + band_blocks(nch)) * E;
     VT M[W][W], c[W];
 #pragma unroll
     for (int r = 0; r < W; ++r) {
@@ -68,7 +133,7 @@ __global__ void __launch_bounds__(256) k_band_maps(const VT *__restrict__ coef, 
         for (int q = 0; q < W; ++q) M[r][q] = r == q ? VT(1) : VT(0);
         c[r] = 0;
     }
-    const int rows = min(C, m - j * C);
+    const int rows = j < nch ? min(C, m - j * C) : 0;
 #pragma unroll 4
     for (int i = 0; i < rows; ++i) {
         const long long o = (long long)i * nch + j;
@@ -78,13 +143,17 @@ __global__ void __launch_bounds__(256) k_band_maps(const VT *__restrict__ coef, 
         const int p = j * C + i;
         band_step_M<VT, W>(M, c, a, inv[o], b[(long long)p * K + colk]);
     }
-    VT *out = maps + (long long)j * (W * W + W);
+    band_cta_scan<VT, W>(M, c, reinterpret_cast<VT *>(smem_raw));
+    auto put = [&](VT *out) {
 #pragma unroll
-    for (int r = 0; r < W; ++r) {
+        for (int r = 0; r < W; ++r) {
 #pragma unroll
-        for (int q = 0; q < W; ++q) out[r * W + q] = M[r][q];
-        out[W * W + r] = c[r];
-    }
+            for (int q = 0; q < W; ++q) out[r * W + q] = M[r][q];
+            out[W * W + r] = c[r];
+        }
+    };
+    if (j < nch) put(maps + (long long)j * E);
+    if (threadIdx.x == BAND_T - 1) put(maps + (long long)(nch + blockIdx.x) * E);
 }
 
 // (M, c) <- (Mo, co) o (M, c):  M = Mo M,  c = Mo c + co
@@ -113,14 +182,17 @@ __device__ __forceinline__ void band_compose_after(VT (&M)[W][W], VT (&c)[W], co
     }
 }
 
-// Pass 2: one CTA of 256 threads.  Thread t composes chunks [t*Q, t*Q+Q),
-// the CTA scans the per-thread maps, and each thread then walks its chunks
-// to write the state entering each of them (the block starts from s = 0).
+// Pass 2: one CTA of 256 threads per column over the n maps at maps (column
+// stride mstride): thread t composes maps [t*Q, t*Q+Q), the CTA scans the
+// per-thread maps, and each thread then walks its maps to write the state
+// entering each of them (states, column stride sstride; the block starts
+// from s = 0).  The maps are the CTA totals of pass 1.
 template <typename VT, int W>
-__global__ void __launch_bounds__(256) k_band_scan(const VT *__restrict__ maps, int nch, VT *__restrict__ states) {
+__global__ void __launch_bounds__(256) k_band_scan(const VT *__restrict__ maps, int nch, long long mstride,
+                                                   VT *__restrict__ states, long long sstride) {
     extern __shared__ unsigned char smem_raw[];
-    maps += (long long)blockIdx.x * nch * (W * W + W);
-    states += (long long)blockIdx.x * nch * W;
+    maps += (long long)blockIdx.x * mstride;
+    states += (long long)blockIdx.x * sstride;
     VT *sm = reinterpret_cast<VT *>(smem_raw);
     constexpr int E = W * W + W;
     const int tid = threadIdx.x, T = blockDim.x;
@@ -134,43 +206,7 @@ __global__ void __launch_bounds__(256) k_band_scan(const VT *__restrict__ maps, 
         c[r] = 0;
     }
     for (int j = j0; j < j1; ++j) band_compose_after<VT, W>(M, c, maps + (long long)j * E);
-    // inclusive Kogge-Stone over the T per-thread maps
-    for (int off = 1; off < T; off <<= 1) {
-        VT *mine = sm + (long long)tid * E;
-#pragma unroll
-        for (int r = 0; r < W; ++r) {
-#pragma unroll
-            for (int q = 0; q < W; ++q) mine[r * W + q] = M[r][q];
-            mine[W * W + r] = c[r];
-        }
-        __syncthreads();
-        if (tid >= off) {
-            // this <- this o earlier:  M = M_this M_earlier,  c = M_this c_earlier + c_this
-            const VT *e = sm + (long long)(tid - off) * E;
-            VT nM[W][W], nc[W];
-#pragma unroll
-            for (int r = 0; r < W; ++r) {
-                VT s = c[r];
-#pragma unroll
-                for (int k = 0; k < W; ++k) s += M[r][k] * e[W * W + k];
-                nc[r] = s;
-#pragma unroll
-                for (int q = 0; q < W; ++q) {
-                    VT t = 0;
-#pragma unroll
-                    for (int k = 0; k < W; ++k) t += M[r][k] * e[k * W + q];
-                    nM[r][q] = t;
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < W; ++r) {
-                c[r] = nc[r];
-#pragma unroll
-                for (int q = 0; q < W; ++q) M[r][q] = nM[r][q];
-            }
-        }
-        __syncthreads();
-    }
+    band_cta_scan<VT, W>(M, c, sm);  // inclusive over the T per-thread maps
     // state entering this thread's first chunk = exclusive prefix applied to 0
     VT *mine = sm + (long long)tid * E;
 #pragma unroll
@@ -196,18 +232,37 @@ __global__ void __launch_bounds__(256) k_band_scan(const VT *__restrict__ maps, 
     }
 }
 
-// Pass 3: replay chunk j from its entering state and write x.
+// Pass 3: the state entering chunk j (its CTA's entering state, advanced by
+// the composition of the CTA's chunks before j), then chunk j replayed from
+// it, writing x.
 template <typename VT, int W>
-__global__ void __launch_bounds__(256) k_band_replay(const VT *__restrict__ coef, const VT *__restrict__ inv,
-                                                     const VT *__restrict__ b, int K, int m, int C, int nch,
-                                                     const VT *__restrict__ states, VT *x) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(BAND_T) k_band_replay(const VT *__restrict__ coef, const VT *__restrict__ inv,
+                                                        const VT *__restrict__ b, int K, int m, int C, int nch,
+                                                        const VT *__restrict__ maps, const VT *__restrict__ states,
+                                                        VT *x) {
+    constexpr int E = W * W + W;
+    const int j = blockIdx.x * BAND_T + threadIdx.x;
     const int colk = blockIdx.y;
-    states += (long long)colk * nch * W;
+    const int nblk = band_blocks(nch);
+    maps += (long long)colk * (nch + nblk) * E;
+    states += (long long)colk * nblk * W;
     if (j >= nch) return;
-    VT s[W];
+    VT s0[W], s[W];
 #pragma unroll
-    for (int r = 0; r < W; ++r) s[r] = states[(long long)j * W + r];
+    for (int r = 0; r < W; ++r) s0[r] = states[(long long)blockIdx.x * W + r];
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int r = 0; r < W; ++r) s[r] = s0[r];
+    } else {
+        const VT *f = maps + (long long)(j - 1) * E;
+#pragma unroll
+        for (int r = 0; r < W; ++r) {
+            VT t = f[W * W + r];
+#pragma unroll
+            for (int k = 0; k < W; ++k) t += f[r * W + k] * s0[k];
+            s[r] = t;
+        }
+    }
     const int rows = min(C, m - j * C);
 #pragma unroll 4
     for (int i = 0; i < rows; ++i) {
