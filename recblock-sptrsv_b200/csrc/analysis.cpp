@@ -24,7 +24,7 @@ namespace rbs {
 namespace {
 
 constexpr int kLongRow = 2048;  // utils_spmv_cuda.h:9 LONGROW_THRESHOLD
-constexpr int kMedRow = 32;     // RBS_MEDROW (kernels.cuh)
+constexpr int kMedRow = 8;      // RBS_MEDROW (kernels.cuh)
 
 int lowbit(int t) { return t & -t; }
 

@@ -21,7 +21,7 @@ namespace rbs {
 #define RBS_SENT32 0xFFC0DEADu
 #define RBS_STATUS_TIMEOUT 1
 #define RBS_LONGROW 2048
-#define RBS_MEDROW 32  // squares, single RHS, lane group < 32: longer rows take a warp each
+#define RBS_MEDROW 8  // squares, single RHS, lane group < 32: longer rows take a warp each
 
 template <typename VT> struct Sent;
 template <> struct Sent<double> {
@@ -56,6 +56,9 @@ __device__ __forceinline__ void st_relaxed(float *p, float v) {
 
 // Wait until x[i] is produced.  Bounded: after `limit` polls the wait gives
 // up, raises RBS_STATUS_TIMEOUT and returns NaN so dependants still finish.
+// Polls back off to at most 128 ns apart: a backoff growing to 1 us added up
+// to a microsecond to every dependency hop of narrow levels (the power-law
+// factor's first triangle spent most of its 67 us asleep).
 template <typename VT>
 __device__ __forceinline__ VT wait_value(const VT *p, int *status, long long limit) {
     VT v = ld_relaxed(p);
@@ -64,7 +67,7 @@ __device__ __forceinline__ VT wait_value(const VT *p, int *status, long long lim
     for (long long it = 0; it < limit; ++it) {
         if (it > 16) {
             __nanosleep(ns);
-            if (ns < 1024) ns <<= 1;
+            if (ns < 128) ns <<= 1;
         }
         v = ld_relaxed(p);
         if (!Sent<VT>::is(v)) return v;
@@ -469,12 +472,19 @@ __global__ void __launch_bounds__(256) k_tri_syncfree(const int *__restrict__ rp
             // Reduce inside the row group only: a later group of this warp may
             // be spinning on the row this group is about to publish.
             const unsigned gmask = g == 32 ? 0xffffffffu : (((1u << g) - 1u) << (sub * g));
-            VT sum = 0;
+            VT sum = 0, bi = 0, iv = 0;
             if (active) {
                 // the row's entries in aligned pairs, one vector load of two
                 // values (16 bytes in FP64) and one of two columns per pair
-                // and lane; an odd first entry and an odd last one alone
+                // and lane; an odd first entry and an odd last one alone.
+                // b and the inverse diagonal are read with the row pointers:
+                // after the polls (whose loads order every memory access)
+                // they would add a round trip to each row
                 const int s = rp[row], e = rp[row + 1];
+                if (sl == 0) {
+                    bi = b[row];
+                    iv = inv[row];
+                }
                 const int p0 = s + (s & 1);
                 if (sl == 0 && p0 > s && s < e) sum += val[s] * wait_value(x + col[s], status, limit);
                 using V2 = Vec<VT, 2>;
@@ -490,13 +500,18 @@ __global__ void __launch_bounds__(256) k_tri_syncfree(const int *__restrict__ rp
                 if (last < e && sl == (npair % g)) sum += val[last] * wait_value(x + col[last], status, limit);
             }
             for (int off = g >> 1; off > 0; off >>= 1) sum += __shfl_down_sync(gmask, sum, off, g);
-            if (active && sl == 0) st_relaxed(x + row, finalize((b[row] - sum) * inv[row]));
+            if (active && sl == 0) st_relaxed(x + row, finalize((bi - sum) * iv));
             __syncwarp();
         } else {
             if (active) {
-                VT acc[RPL];
+                VT acc[RPL], bo[RPL];
+                const long long o = (long long)row * K + sl * RPL;
+                const VT d = inv[row];  // read ahead of the polls, as for one column
 #pragma unroll
-                for (int r = 0; r < RPL; ++r) acc[r] = 0;
+                for (int r = 0; r < RPL; ++r) {
+                    acc[r] = 0;
+                    bo[r] = b[o + r];
+                }
                 const int s = rp[row], e = rp[row + 1];
                 for (int k = s; k < e; ++k) {
                     const VT v = val[k];
@@ -504,10 +519,8 @@ __global__ void __launch_bounds__(256) k_tri_syncfree(const int *__restrict__ rp
 #pragma unroll
                     for (int r = 0; r < RPL; ++r) acc[r] += v * wait_value(xs + r, status, limit);
                 }
-                const VT d = inv[row];
-                const long long o = (long long)row * K + sl * RPL;
 #pragma unroll
-                for (int r = 0; r < RPL; ++r) st_relaxed(x + o + r, finalize((b[o + r] - acc[r]) * d));
+                for (int r = 0; r < RPL; ++r) st_relaxed(x + o + r, finalize((bo[r] - acc[r]) * d));
             }
             __syncwarp();
         }
@@ -613,24 +626,62 @@ __global__ void __launch_bounds__(32) k_tri_seq(const int *__restrict__ rp, cons
     }
 }
 
+// Medium rows of a square whose lane group is narrow (single RHS): rows of
+// more than RBS_MEDROW entries, up to RBS_LONGROW, one warp each, summed in
+// a fixed shuffle order (deterministic) -- so a few long rows no longer
+// hold a narrow group for hundreds of serial steps.  `pos` lists positions
+// in the row pointer (the row for CSR, the list index for DCSR).  Run by
+// the first `nblk` CTAs of the square's k_spmv_sub launch (block index
+// `blk`), beside the CTAs of its other rows: one launch per square, and the
+// longest rows start first.
+template <typename VT>
+__device__ __forceinline__ void spmv_rows_warps(const int *__restrict__ rp, const int *__restrict__ col,
+                                                const VT *__restrict__ val, const int *__restrict__ rows,
+                                                const int *__restrict__ pos, int npos, const VT *__restrict__ x,
+                                                VT *b, int blk, int nblk) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blk * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)nblk * blockDim.x) >> 5;
+    for (long long t = warp; t < npos; t += nwarps) {
+        const int i = pos[t];
+        const int s = rp[i], e = rp[i + 1];
+        VT sum = 0;
+        // unrolled 16 deep: a row of up to 2048 entries has its column and
+        // x loads in flight together instead of in a chain of dependent pairs
+#pragma unroll 16
+        for (int k = s + lane; k < e; k += 32) sum += val[k] * x[col[k]];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+        if (lane == 0) b[rows ? rows[i] : i] -= sum;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Square block: b[rows] -= S * x[cols]  (reference mv methods 0..3,
 // utils_spmv_cuda.h:60-203, with subKernel :205-212 fused).  `rows` lists
-// the rows for the DCSR form, NULL for plain CSR.  Rows longer than 2048 are
-// skipped here and handled by k_spmv_long (utils_spmv_cuda.h:30-58).
+// the rows for the DCSR form, NULL for plain CSR.  Rows longer than maxlen
+// are skipped by the lane groups: those of up to 2048 entries (single RHS,
+// narrow group; listed in `med`) are taken by the launch's first medctas
+// CTAs, a warp each; longer ones by k_spmv_long (utils_spmv_cuda.h:30-58).
 // ---------------------------------------------------------------------------
 template <typename VT, int K>
 __global__ void __launch_bounds__(256) k_spmv_sub(const int *__restrict__ rp, const int *__restrict__ col,
                                                   const VT *__restrict__ val, const int *__restrict__ rows,
                                                   int nrows, int G, const VT *__restrict__ x, VT *b,
-                                                  int maxlen) {
+                                                  int maxlen, const int *__restrict__ med, int nmed,
+                                                  int medctas) {
+    if (K == 1 && (int)blockIdx.x < medctas) {  // the square's medium rows, in the same launch
+        spmv_rows_warps<VT>(rp, col, val, rows, med, nmed, x, b, blockIdx.x, medctas);
+        return;
+    }
     constexpr int R = K < 32 ? K : 32;
     constexpr int RPL = K / R;
     const int g = K == 1 ? G : R;
     const int lane = threadIdx.x & 31;
     const int sl = lane % g, rpw = 32 / g;
-    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long bx = (long long)blockIdx.x - medctas, gx = (long long)gridDim.x - medctas;
+    const long long warp = (bx * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = (gx * blockDim.x) >> 5;
     for (long long base = warp * rpw; base < nrows; base += nwarps * rpw) {
         const long long i = base + lane / g;
         const bool active = i < nrows;
@@ -665,31 +716,6 @@ __global__ void __launch_bounds__(256) k_spmv_sub(const int *__restrict__ rp, co
 #pragma unroll
             for (int r = 0; r < RPL; ++r) b[o + r] -= acc[r];
         }
-    }
-}
-
-// Medium rows of a square whose lane group is narrow (single RHS): rows of
-// more than RBS_MEDROW entries, up to RBS_LONGROW, one warp each, summed in
-// a fixed shuffle order (deterministic) -- so a few long rows no longer
-// hold a narrow group for hundreds of serial steps.  `pos` lists positions
-// in the row pointer (the row for CSR, the list index for DCSR).
-template <typename VT>
-__global__ void __launch_bounds__(256) k_spmv_rows(const int *__restrict__ rp, const int *__restrict__ col,
-                                                   const VT *__restrict__ val, const int *__restrict__ rows,
-                                                   const int *__restrict__ pos, int npos,
-                                                   const VT *__restrict__ x, VT *b) {
-    const int lane = threadIdx.x & 31;
-    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long t = warp; t < npos; t += nwarps) {
-        const int i = pos[t];
-        const int s = rp[i], e = rp[i + 1];
-        VT sum = 0;
-#pragma unroll 4
-        for (int k = s + lane; k < e; k += 32) sum += val[k] * x[col[k]];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
-        if (lane == 0) b[rows ? rows[i] : i] -= sum;
     }
 }
 

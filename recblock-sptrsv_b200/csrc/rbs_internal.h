@@ -150,7 +150,7 @@ struct ExecBlock {
     int nonempty;       // squares: nonempty rows
     int longrows;       // squares: rows longer than 2048 (handled by the split kernel)
     long long long_off; // long-row list offset or -1
-    int medrows;        // squares with a lane group < 32: rows of 33..2048 entries (a warp each, single RHS)
+    int medrows;        // squares with a lane group < 32: rows of 9..2048 entries (a warp each, single RHS)
     long long med_off;  // medium-row list offset or -1
     int lenmax;
     // band-scan triangles: W = power of two >= bandwidth, chunks of C rows

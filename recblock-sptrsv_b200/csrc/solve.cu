@@ -930,13 +930,13 @@ int launch_blocks(Plan &P, std::string &err, bool io = false) {
             const int *rows = B.rows_off >= 0 ? D.rows + B.rows_off : nullptr;
             const bool med = K == 1 && B.medrows > 0;
             const int maxlen = med ? RBS_MEDROW : B.longrows > 0 ? RBS_LONGROW : 0x7fffffff;
-            k_spmv_sub<VT, K><<<grid_for((long long)B.nrows * g, 256, D.num_sms), 256, 0, st>>>(
+            // the medium rows' warps lead the launch (their CTAs first), the
+            // other rows' groups follow in the same grid
+            const int medctas = med ? grid_for((long long)B.medrows * 32, 256, D.num_sms) : 0;
+            k_spmv_sub<VT, K><<<medctas + grid_for((long long)B.nrows * g, 256, D.num_sms), 256, 0, st>>>(
                 D.rp + B.rp_off, D.col, val, rows, B.nrows, B.group, xw + (long long)B.c0 * K,
-                bw + (long long)B.r0 * K, maxlen);
-            if (med)
-                k_spmv_rows<VT><<<grid_for((long long)B.medrows * 32, 256, D.num_sms), 256, 0, st>>>(
-                    D.rp + B.rp_off, D.col, val, rows, D.rows + B.med_off, B.medrows, xw + (long long)B.c0 * K,
-                    bw + (long long)B.r0 * K);
+                bw + (long long)B.r0 * K, maxlen, med ? D.rows + B.med_off : nullptr, med ? B.medrows : 0,
+                medctas);
             if (B.longrows > 0)
                 k_spmv_long<VT, K><<<D.num_sms * 2, 256, 0, st>>>(D.rp + B.rp_off, D.col, val, rows,
                                                                   D.rows + B.long_off, B.longrows,

@@ -1,6 +1,6 @@
 """Host analysis of squares with a heavy tail of long rows: for the single-RHS
 solve, every square whose lane group is narrower than a warp lists its rows
-of 33..2048 entries for the warp-per-row pass (export "medrow"), and no other
+of 9..2048 entries for the warp-per-row pass (export "medrow"), and no other
 block lists any.  A chain keeps the level order equal to the natural order,
 so the square of lv = 1 is exactly rows [n/2, n) x columns [0, n/2)."""
 import numpy as np
@@ -31,7 +31,7 @@ def chain_with_long_rows(n, long_rows, long_len, seed):
     return rp, np.array(ci, np.int32), np.array(va)
 
 
-@pytest.mark.parametrize("long_len,expect_rows", [(40, 5), (2048, 5), (2049, 0), (32, 0)])
+@pytest.mark.parametrize("long_len,expect_rows", [(40, 5), (9, 5), (2048, 5), (2049, 0), (8, 0)])
 def test_square_medium_rows_listed(long_len, expect_rows):
     n = 6000
     long_rows = {n // 2 + 7, n // 2 + 100, n // 2 + 1500, n - 20, n - 1}
