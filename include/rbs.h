@@ -359,9 +359,8 @@ int rbs_auto_lv(int m, int device_id);
  * bytes (about 8 MB), held by every GPU that loads this library until the
  * process exits.  n > RBS_NOALLOC_MAX_ROWS is rejected with RBS_ERR_ARG.
  * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) and keeps it for the life of the process; make
- * that first call before any stream capture begins, and do not use this
- * entry point across a cudaDeviceReset.  Every call on a device shares the
+ * (cudaGetSymbolAddress) and keeps it for the life of the process; do not
+ * use this entry point across a cudaDeviceReset.  Every call on a device shares the
  * one array: calls whose work overlaps on the GPU (different streams or
  * host threads) race and corrupt each other's results; serialise them. */
 #define RBS_NOALLOC_MAX_ROWS (1 << 20)

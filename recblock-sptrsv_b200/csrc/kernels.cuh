@@ -669,7 +669,7 @@ __global__ void __launch_bounds__(256) k_spmv_sub(const int *__restrict__ rp, co
                                                   const VT *__restrict__ val, const int *__restrict__ rows,
                                                   int nrows, int G, const VT *__restrict__ x, VT *b,
                                                   int maxlen, const int *__restrict__ med, int nmed,
-                                                  int medctas) {
+                                                  int medctas, int pairs) {
     if (K == 1 && (int)blockIdx.x < medctas) {  // the square's medium rows, in the same launch
         spmv_rows_warps<VT>(rp, col, val, rows, med, nmed, x, b, blockIdx.x, medctas);
         return;
@@ -682,39 +682,91 @@ __global__ void __launch_bounds__(256) k_spmv_sub(const int *__restrict__ rp, co
     const long long bx = (long long)blockIdx.x - medctas, gx = (long long)gridDim.x - medctas;
     const long long warp = (bx * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = (gx * blockDim.x) >> 5;
-    for (long long base = warp * rpw; base < nrows; base += nwarps * rpw) {
-        const long long i = base + lane / g;
-        const bool active = i < nrows;
-        int s = 0, e = 0, row = 0;
-        if (active) {
-            s = rp[i];
-            e = rp[i + 1];
-            row = rows ? rows[i] : (int)i;
-            if (e - s > maxlen) e = s;  // a longer row is another kernel's
-        }
-        if (K == 1) {
-            VT sum = 0;
-            // unrolled: several column loads issue before their x gathers
-            // (same summation order).  Aligned pairs of entries per lane (one
-            // 16-byte value load) measured no faster on the power-law factor:
-            // its short rows left half of each lane group idle.
+    if constexpr (K == 1) {
+        if (pairs) {
+            // Two row groups per lane group and iteration (rows base + t and
+            // base + rpw + t), their loads interleaved, so the chains of row
+            // pointer, column, x and b round trips of the two rows overlap:
+            // for squares whose grid is capped, where every warp loops (the
+            // power-law factor's big square: 61 -> 46 us).  Each row keeps its
+            // summation order (lane sl: entries sl, sl+g, ...).
+            for (long long base = warp * rpw * 2; base < nrows; base += nwarps * rpw * 2) {
+                const long long i0 = base + lane / g, i1 = i0 + rpw;
+                int s0 = 0, e0 = 0, r0 = 0, s1 = 0, e1 = 0, r1 = 0;
+                if (i0 < nrows) {
+                    s0 = rp[i0];
+                    e0 = rp[i0 + 1];
+                    r0 = rows ? rows[i0] : (int)i0;
+                    if (e0 - s0 > maxlen) e0 = s0;  // a longer row is the medium or long rows' work
+                }
+                if (i1 < nrows) {
+                    s1 = rp[i1];
+                    e1 = rp[i1 + 1];
+                    r1 = rows ? rows[i1] : (int)i1;
+                    if (e1 - s1 > maxlen) e1 = s1;
+                }
+                const int n0 = e0 - s0, n1 = e1 - s1;
+                VT sum0 = 0, sum1 = 0;
 #pragma unroll 4
-            for (int k = s + sl; k < e; k += g) sum += val[k] * x[col[k]];
-            for (int off = g >> 1; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off, g);
-            if (active && sl == 0 && e > s) b[row] -= sum;
-        } else if (active && e > s) {
-            VT acc[RPL];
-#pragma unroll
-            for (int r = 0; r < RPL; ++r) acc[r] = 0;
-            for (int k = s; k < e; ++k) {
-                const VT v = val[k];
-                const VT *xs = x + (long long)col[k] * K + sl * RPL;
-#pragma unroll
-                for (int r = 0; r < RPL; ++r) acc[r] += v * xs[r];
+                for (int q = sl; q < max(n0, n1); q += g) {
+                    if (q < n0) sum0 += val[s0 + q] * x[col[s0 + q]];
+                    if (q < n1) sum1 += val[s1 + q] * x[col[s1 + q]];
+                }
+                for (int off = g >> 1; off > 0; off >>= 1) {
+                    sum0 += __shfl_down_sync(0xffffffffu, sum0, off, g);
+                    sum1 += __shfl_down_sync(0xffffffffu, sum1, off, g);
+                }
+                if (sl == 0) {
+                    if (n0 > 0) b[r0] -= sum0;
+                    if (n1 > 0) b[r1] -= sum1;
+                }
             }
-            const long long o = (long long)row * K + sl * RPL;
+        } else {
+            for (long long base = warp * rpw; base < nrows; base += nwarps * rpw) {
+                const long long i = base + lane / g;
+                int s = 0, e = 0, row = 0;
+                if (i < nrows) {
+                    s = rp[i];
+                    e = rp[i + 1];
+                    row = rows ? rows[i] : (int)i;
+                    if (e - s > maxlen) e = s;
+                }
+                VT sum = 0;
+                // unrolled: several column loads issue before their x gathers
+                // (same summation order).  Aligned pairs of entries per lane (one
+                // 16-byte value load) measured no faster on the power-law factor:
+                // its short rows left half of each lane group idle.
+#pragma unroll 4
+                for (int k = s + sl; k < e; k += g) sum += val[k] * x[col[k]];
+                for (int off = g >> 1; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off, g);
+                if (sl == 0 && e > s) b[row] -= sum;
+            }
+        }
+    } else {
+        for (long long base = warp * rpw; base < nrows; base += nwarps * rpw) {
+            const long long i = base + lane / g;
+            const bool active = i < nrows;
+            int s = 0, e = 0, row = 0;
+            if (active) {
+                s = rp[i];
+                e = rp[i + 1];
+                row = rows ? rows[i] : (int)i;
+                if (e - s > maxlen) e = s;  // a longer row is another kernel's
+            }
+            if (active && e > s) {
+                VT acc[RPL];
 #pragma unroll
-            for (int r = 0; r < RPL; ++r) b[o + r] -= acc[r];
+                for (int r = 0; r < RPL; ++r) acc[r] = 0;
+                for (int k = s; k < e; ++k) {
+                    const VT v = val[k];
+                    const VT *xs = x + (long long)col[k] * K + sl * RPL;
+#pragma unroll
+                    for (int r = 0; r < RPL; ++r) acc[r] += v * xs[r];
+                }
+                const long long o = (long long)row * K + sl * RPL;
+#pragma unroll
+                for (int r = 0; r < RPL; ++r) b[o + r] -= acc[r];
+            }
         }
     }
 }

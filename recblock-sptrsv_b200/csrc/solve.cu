@@ -933,10 +933,14 @@ int launch_blocks(Plan &P, std::string &err, bool io = false) {
             // the medium rows' warps lead the launch (their CTAs first), the
             // other rows' groups follow in the same grid
             const int medctas = med ? grid_for((long long)B.medrows * 32, 256, D.num_sms) : 0;
-            k_spmv_sub<VT, K><<<medctas + grid_for((long long)B.nrows * g, 256, D.num_sms), 256, 0, st>>>(
+            // single column, a grid at its cap (every warp loops): a lane
+            // group takes two rows per iteration
+            const long long lanes = (long long)B.nrows * g;
+            const int pairs = K == 1 && lanes > (long long)grid_for(lanes, 256, D.num_sms) * 256;
+            k_spmv_sub<VT, K><<<medctas + grid_for(pairs ? (lanes + 1) / 2 : lanes, 256, D.num_sms), 256, 0, st>>>(
                 D.rp + B.rp_off, D.col, val, rows, B.nrows, B.group, xw + (long long)B.c0 * K,
                 bw + (long long)B.r0 * K, maxlen, med ? D.rows + B.med_off : nullptr, med ? B.medrows : 0,
-                medctas);
+                medctas, pairs);
             if (B.longrows > 0)
                 k_spmv_long<VT, K><<<D.num_sms * 2, 256, 0, st>>>(D.rp + B.rp_off, D.col, val, rows,
                                                                   D.rows + B.long_off, B.longrows,

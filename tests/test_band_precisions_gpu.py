@@ -34,3 +34,29 @@ def test_band_scan_precisions(cuda, n, select, sub):
             got = dX.cpu().numpy().reshape(kk, n)
             for c in range(kk):
                 assert rel_err(got[c], Xo[c]) <= tol, (kk, prec, c)
+
+
+@pytest.mark.parametrize("bw", [1, 2, 7])
+def test_band_scan_widths_many_ctas(cuda, bw):
+    # one deep triangle (lv = 0) of 300,000 rows: band widths W = 1, 2 and 8
+    # (chunks of 4 or 8 rows, so the maps pass spans more than a hundred CTAs
+    # and the scan pass composes their totals), one and three columns, FP64
+    # and mixed against the oracle
+    import torch
+    n = 300000
+    rp, ci, va = rbs.gen_lower_csr(rbs.GEN_CHAIN, n=n, chain_bw=bw, seed=700 + bw)
+    cp, ri, cv = oracle.transpose(rp, ci, va)
+    plan = rbs.analyse(cp, ri, cv, substitution=rbs.FORWARD, lv=0, opts=rbs.options(max_rhs=4))
+    assert (plan.export("kernel") == rbs.K_BANDSCAN).all()
+    k = 3
+    X = np.stack([rbs.gen_uniform(50 + c, n) for c in range(k)])
+    B = np.stack([oracle.spmv_csr(rp, ci, va, X[c]) for c in range(k)])
+    Xo = np.stack([oracle.sptrsv_csr(rp, ci, va, rbs.FORWARD, B[c]) for c in range(k)])
+    for kk in (1, k):
+        dB = torch.tensor(B[:kk], device=cuda).reshape(-1)
+        for prec in (rbs.PREC_FP64, rbs.PREC_MIXED):
+            dX = torch.empty_like(dB)
+            plan.solve(dB, dX, k=kk, prec=prec)
+            got = dX.cpu().numpy().reshape(kk, n)
+            for c in range(kk):
+                assert rel_err(got[c], Xo[c]) <= 1e-12, (bw, kk, prec, c)
