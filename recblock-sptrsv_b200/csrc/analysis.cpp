@@ -23,8 +23,8 @@ namespace rbs {
 
 namespace {
 
-constexpr int kLongRow = 2048;  // utils_spmv_cuda.h:9 LONGROW_THRESHOLD
-constexpr int kMedRow = 8;      // RBS_MEDROW (kernels.cuh)
+constexpr int kLongRow = SQ_LONGROW;
+constexpr int kMedRow = SQ_MEDROW;
 
 int lowbit(int t) { return t & -t; }
 

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "rbs.h"
+#include "lc_layout.h"
 #include "rbs_internal.h"
 
 namespace rbs {
@@ -159,9 +160,19 @@ void fields(IO &io, Plan &P) {
     io.vec(P.full_val);
 }
 
-// layout signature: a file is read only by a build with the same record sizes
+// layout signature: a file is read only by a build with the same record
+// sizes and the same constants that give the plan's arrays their meaning
+// (the squares' row-length classes, the staged-level window, the level-chunk
+// layout and its copy distance): a plan whose lists were cut at other
+// thresholds would solve wrongly, not fail
 uint64_t layout_signature() {
-    return ((uint64_t)sizeof(ExecBlock) << 32) ^ ((uint64_t)sizeof(rbs_options) << 16) ^ (uint64_t)sizeof(Plan);
+    const uint64_t c[] = {sizeof(ExecBlock), sizeof(rbs_options), sizeof(Plan), (uint64_t)SQ_MEDROW,
+                          (uint64_t)SQ_LONGROW, (uint64_t)CA_WINDOW_ROWS, (uint64_t)LC_XW, (uint64_t)LC_NB,
+                          (uint64_t)LC_D, (uint64_t)LC_RMAX, (uint64_t)LC_T, (uint64_t)LC_RING, (uint64_t)LC_FMAX,
+                          (uint64_t)LC_HDR_INTS};
+    uint64_t h = 0;
+    for (uint64_t v : c) h = mix64(h ^ v);
+    return h;
 }
 
 }  // namespace

@@ -176,6 +176,12 @@ struct ExecBlock {
 
 // rows of the shared-memory x window of the staged level kernel (power of 2)
 constexpr int CA_WINDOW_ROWS = 4096;
+// Row-length classes of the squares (single right-hand side, narrow lane
+// group): rows of more than SQ_MEDROW entries, up to SQ_LONGROW, are listed
+// for a warp each; longer rows are split over warps (utils_spmv_cuda.h:9
+// LONGROW_THRESHOLD).  The kernels' RBS_MEDROW / RBS_LONGROW are the same.
+constexpr int SQ_MEDROW = 8;
+constexpr int SQ_LONGROW = 2048;
 
 // single-CTA level kernels of a RBS_K_LEVEL triangle
 enum { LVL_PLAIN = 0, LVL_CA = 1, LVL_CSF = 2, LVL_LC = 3 };

@@ -35,6 +35,8 @@ inline void attr_mark(std::atomic<unsigned long long> &seen) {
     seen.fetch_or(1ULL << (dev & 63));
 }
 
+static_assert(RBS_MEDROW == SQ_MEDROW && RBS_LONGROW == SQ_LONGROW, "the squares' row classes of analysis and kernels");
+
 struct DeviceState {
     int device = 0, num_sms = 148;
     int smem_sm = 233472, smem_reserved = 1024;  // shared memory per SM, reserved per CTA
