@@ -662,7 +662,9 @@ def side_serving(dev, args, n_requests=1000, loads=(500, 1000, 2000, 10000, 5000
     place) and across them (batches of all factors overlap on the device),
     once with FP32 sweeps + FP64 refinement and once in FP64 (the solves are
     latency-bound, so the FP64 sweep, one walk instead of two or three, is
-    the faster choice here).  Baselines, on the same arrivals and
+    the faster choice here), and once more in FP64 with the small factors
+    served in groups (one block-diagonal plan per group: requests of
+    different factors share a launch).  Baselines, on the same arrivals and
     device arrays: one plain FP64 rbs_solve of each request's k columns in
     arrival order on the caller's thread, and the plain FP64 single-RHS path
     (one rbs_solve per right-hand side, back to back)."""
@@ -737,7 +739,7 @@ def side_serving(dev, args, n_requests=1000, loads=(500, 1000, 2000, 10000, 5000
             for prec in (rbs.PREC_MIXED, rbs.PREC_FP64):
                 srv.wait(srv.submit_device(fids[f], dB[f], dX[f], k=k, prec=prec))
 
-    def serve(rate, prec):
+    def serve(rate, prec, srv, fids):
         arr, fid, ks = scheds[rate]
         srv.reset_stats()
         tickets = []
@@ -776,8 +778,8 @@ def side_serving(dev, args, n_requests=1000, loads=(500, 1000, 2000, 10000, 5000
 
     try:
         for rate in loads:
-            row = {"served_mixed": serve(rate, rbs.PREC_MIXED), "served_fp64": serve(rate, rbs.PREC_FP64),
-                   "plain_fp64": plain[rate]}
+            row = {"served_mixed": serve(rate, rbs.PREC_MIXED, srv, fids),
+                   "served_fp64": serve(rate, rbs.PREC_FP64, srv, fids), "plain_fp64": plain[rate]}
             for arm in ("served_mixed", "served_fp64"):
                 row[f"{arm}_x_plain_fp64"] = row[arm]["solves_per_s"] / plain[rate]["solves_per_s"]
                 row[f"{arm}_x_plain_fp64_single_rhs"] = row[arm]["solves_per_s"] / single
@@ -792,9 +794,45 @@ def side_serving(dev, args, n_requests=1000, loads=(500, 1000, 2000, 10000, 5000
             srv.wait(srv.submit_device(fids[i], b, x, k=1, prec=rbs.PREC_MIXED))
             worst = max(worst, rel(x.cpu().numpy(), xt))
         res["max_rel_err_vs_x_true"] = worst
+        srv.close()
+        srv = None
+        # Grouped: the small Laplacian and power-law factors (<= 100k rows)
+        # in groups of up to 16, each group one block-diagonal plan whose
+        # batches solve requests of all its members in one launch; chains
+        # stay alone (a group walks as deep as its deepest member).  FP64.
+        srv = rbs.Server(150 << 30, max_batch_rhs=batch_rhs)
+        small = [i for i in range(64) if ns[i] <= 100000 and i % 3 != 2]
+        gids = [None] * 64
+        for g0 in range(0, len(small), 16):
+            mem = small[g0:g0 + 16]
+            gplan, offs = rbs.batch_analyse([tuple(facs[i]) for i in mem], substitution=rbs.FORWARD, fmt=rbs.FMT_CSR)
+            for i, fid_i in zip(mem, srv.add_group(gplan, offs)):
+                gids[i] = fid_i
+        for i in range(64):
+            if gids[i] is None:
+                gids[i] = srv.add_factor(rbs.analyse(*facs[i], substitution=rbs.FORWARD, lv=-1, fmt=rbs.FMT_CSR))
+        for f in range(64):
+            for k in (1, 16):
+                srv.wait(srv.submit_device(gids[f], dB[f], dX[f], k=k, prec=rbs.PREC_FP64))
+        res["grouped"] = {"groups": (len(small) + 15) // 16, "members": len(small),
+                          "rule": "Laplacian and power-law factors of <= 100k rows, up to 16 per group"}
+        for rate in loads:
+            row = res["loads"][str(rate)]
+            row["served_fp64_grouped"] = serve(rate, rbs.PREC_FP64, srv, gids)
+            row["served_fp64_grouped_x_plain_fp64_single_rhs"] = row["served_fp64_grouped"]["solves_per_s"] / single
+        worst = 0.0
+        for i in small:
+            rp, ci, va = facs[i]
+            xt = rbs.gen_uniform(13000 + i, ns[i])
+            b = torch.tensor(sp.csr_matrix((va, ci, rp), shape=(ns[i], ns[i])) @ xt, device=dev)
+            x = torch.empty_like(b)
+            srv.wait(srv.submit_device(gids[i], b, x, k=1, prec=rbs.PREC_FP64))
+            worst = max(worst, rel(x.cpu().numpy(), xt))
+        res["grouped"]["max_rel_err_vs_x_true"] = worst
     finally:
         sys.setswitchinterval(old_si)
-        srv.close()
+        if srv is not None:
+            srv.close()
     return res
 
 
