@@ -55,6 +55,16 @@ def test_load_rejects_bad_files(tmp_path):
     (tmp_path / "long.rbs").write_bytes(raw + b"\0")
     with pytest.raises(rbs.RbsError):
         rbs.load_plan(tmp_path / "long.rbs", rbs.options(host_only=1))
+    # a file of a build with other layout constants (row-length classes of
+    # the squares, level-chunk layout): the 8-byte signature after the magic
+    # differs, and the file is refused as not of this build before its
+    # contents are read
+    other = bytearray(raw)
+    other[8] ^= 0x01
+    (tmp_path / "other.rbs").write_bytes(bytes(other))
+    with pytest.raises(rbs.RbsError) as e:
+        rbs.load_plan(tmp_path / "other.rbs", rbs.options(host_only=1))
+    assert "not a plan file of this build" in str(e.value)
 
 
 @pytest.mark.gpu
