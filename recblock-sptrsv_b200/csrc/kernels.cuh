@@ -489,12 +489,38 @@ __global__ void __launch_bounds__(256) k_tri_syncfree(const int *__restrict__ rp
                 if (sl == 0 && p0 > s && s < e) sum += val[s] * wait_value(x + col[s], status, limit);
                 using V2 = Vec<VT, 2>;
                 const int npair = (e - p0) / 2;
-                for (int q = sl; q < npair; q += g) {
+                // Two pairs per iteration: the four dependencies' first loads
+                // are issued together and only a value still carrying the
+                // sentinel is polled again, so a row's ready dependencies cost
+                // one L2 round trip instead of one each (same summation order
+                // as one pair at a time).
+                int q = sl;
+                for (; q + g < npair; q += 2 * g) {
+                    const int k0 = p0 + 2 * q, k1 = k0 + 2 * g;
+                    const int2 ca = *reinterpret_cast<const int2 *>(col + k0);
+                    const int2 cb = *reinterpret_cast<const int2 *>(col + k1);
+                    const V2 va = *reinterpret_cast<const V2 *>(val + k0);
+                    const V2 vb = *reinterpret_cast<const V2 *>(val + k1);
+                    VT xa0 = ld_relaxed(x + ca.x), xa1 = ld_relaxed(x + ca.y);
+                    VT xb0 = ld_relaxed(x + cb.x), xb1 = ld_relaxed(x + cb.y);
+                    if (Sent<VT>::is(xa0)) xa0 = wait_value(x + ca.x, status, limit);
+                    if (Sent<VT>::is(xa1)) xa1 = wait_value(x + ca.y, status, limit);
+                    if (Sent<VT>::is(xb0)) xb0 = wait_value(x + cb.x, status, limit);
+                    if (Sent<VT>::is(xb1)) xb1 = wait_value(x + cb.y, status, limit);
+                    sum += va.v[0] * xa0;
+                    sum += va.v[1] * xa1;
+                    sum += vb.v[0] * xb0;
+                    sum += vb.v[1] * xb1;
+                }
+                if (q < npair) {
                     const int k = p0 + 2 * q;
                     const int2 c2 = *reinterpret_cast<const int2 *>(col + k);
                     const V2 v2 = *reinterpret_cast<const V2 *>(val + k);
-                    sum += v2.v[0] * wait_value(x + c2.x, status, limit);
-                    sum += v2.v[1] * wait_value(x + c2.y, status, limit);
+                    VT x0 = ld_relaxed(x + c2.x), x1 = ld_relaxed(x + c2.y);
+                    if (Sent<VT>::is(x0)) x0 = wait_value(x + c2.x, status, limit);
+                    if (Sent<VT>::is(x1)) x1 = wait_value(x + c2.y, status, limit);
+                    sum += v2.v[0] * x0;
+                    sum += v2.v[1] * x1;
                 }
                 const int last = p0 + 2 * npair;
                 if (last < e && sl == (npair % g)) sum += val[last] * wait_value(x + col[last], status, limit);
