@@ -562,22 +562,20 @@ int run_band(Plan &P, const ExecBlock &B, const VT *bb, VT *xx, int K, std::stri
     const VT *binv = Pools<VT>::binv(D) + B.band_off / W;
     VT *maps = reinterpret_cast<VT *>(D.band_maps);
     VT *states = reinterpret_cast<VT *>(D.band_states);
-    const int tpb = 256;
     constexpr int E = W * W + W;
-    const size_t smem = (size_t)tpb * E * sizeof(VT);  // scan pass
-    const size_t smem_maps = (size_t)BAND_T * E * sizeof(VT);
+    const size_t smem = (size_t)BAND_T * E * sizeof(VT);
     static std::atomic<unsigned long long> attr_set{0};
     if (!attr_done(attr_set)) {
-        CK(cudaFuncSetAttribute(k_band_scan<VT, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        CK(cudaFuncSetAttribute(k_band_maps<VT, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_maps));
+        CK(cudaFuncSetAttribute(k_band_onepass<VT, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_mark(attr_set);
     }
     const int nch = B.band_nch, nblk = band_blocks(nch);
-    const dim3 grid(nblk, K);
-    k_band_maps<VT, W><<<grid, BAND_T, smem_maps, st>>>(coef, binv, bb, K, B.m, B.band_c, nch, maps);
-    k_band_scan<VT, W><<<K, tpb, smem, st>>>(maps + (long long)nch * E, nblk, (long long)(nch + nblk) * E, states,
-                                             (long long)nblk * W);
-    k_band_replay<VT, W><<<grid, BAND_T, 0, st>>>(coef, binv, bb, K, B.m, B.band_c, nch, maps, states, xx);
+    // per column: the CTA totals (nblk maps) in the maps scratch, the ticket
+    // and the CTAs' ready flags (nblk + 1 ints) in the states scratch
+    int *flags = reinterpret_cast<int *>(states);
+    CK(cudaMemsetAsync(flags, 0, sizeof(int) * (size_t)K * (nblk + 1), st));
+    k_band_onepass<VT, W><<<dim3(nblk, K), BAND_T, smem, st>>>(coef, binv, bb, K, B.m, B.band_c, nch, maps, flags, xx,
+                                                             D.status, P.opt.spin_limit);
     return RBS_OK;
 }
 
@@ -1423,9 +1421,8 @@ int device_build(Plan &P, std::string &err) {
         size_t maps = 1, states = 1;
         for (const ExecBlock &B : P.blocks)
             if (B.tri && B.band_w > 0) {
-                maps = std::max(maps, (size_t)(B.band_nch + band_blocks(B.band_nch)) *
-                                          (B.band_w * B.band_w + B.band_w));
-                states = std::max(states, (size_t)B.band_nch * B.band_w);
+                maps = std::max(maps, (size_t)band_blocks(B.band_nch) * (B.band_w * B.band_w + B.band_w));
+                states = std::max(states, ((size_t)band_blocks(B.band_nch) + 1) * sizeof(int) / sizeof(double) + 1);
             }
         D.band_maps1 = maps;  // per right-hand side; allocated with the work vectors
         D.band_states1 = states;
