@@ -59,30 +59,26 @@ constexpr int BAND_T = 256;
 
 __host__ __device__ constexpr int band_blocks(int nch) { return (nch + BAND_T - 1) / BAND_T; }
 
-// (M, c) <- (M, c) o (Me, ce), the earlier map Me read from memory:
-// M = M Me,  c = M ce + c
+// A thread's (M, c) into, and another thread's out of, shared memory laid
+// out element-major (element k of thread t at sm[k * T + t]), so a warp's
+// accesses are consecutive words.  Thread-major records (stride W*W+W)
+// put 8 threads of a warp on each bank.
 template <typename VT, int W>
-__device__ __forceinline__ void band_compose_before(VT (&M)[W][W], VT (&c)[W], const VT *e) {
-    VT nM[W][W], nc[W];
+__device__ __forceinline__ void band_put(VT *sm, int T, int t, const VT (&M)[W][W], const VT (&c)[W]) {
 #pragma unroll
     for (int r = 0; r < W; ++r) {
-        VT s = c[r];
 #pragma unroll
-        for (int k = 0; k < W; ++k) s += M[r][k] * e[W * W + k];
-        nc[r] = s;
-#pragma unroll
-        for (int q = 0; q < W; ++q) {
-            VT t = 0;
-#pragma unroll
-            for (int k = 0; k < W; ++k) t += M[r][k] * e[k * W + q];
-            nM[r][q] = t;
-        }
+        for (int q = 0; q < W; ++q) sm[(r * W + q) * T + t] = M[r][q];
+        sm[(W * W + r) * T + t] = c[r];
     }
+}
+template <typename VT, int W>
+__device__ __forceinline__ void band_get(const VT *sm, int T, int t, VT (&M)[W][W], VT (&c)[W]) {
 #pragma unroll
     for (int r = 0; r < W; ++r) {
-        c[r] = nc[r];
 #pragma unroll
-        for (int q = 0; q < W; ++q) M[r][q] = nM[r][q];
+        for (int q = 0; q < W; ++q) M[r][q] = sm[(r * W + q) * T + t];
+        c[r] = sm[(W * W + r) * T + t];
     }
 }
 
@@ -90,18 +86,36 @@ __device__ __forceinline__ void band_compose_before(VT (&M)[W][W], VT (&c)[W], c
 // sm (blockDim.x * (W*W + W) values): thread t ends with map_t o ... o map_0.
 template <typename VT, int W>
 __device__ __forceinline__ void band_cta_scan(VT (&M)[W][W], VT (&c)[W], VT *sm) {
-    constexpr int E = W * W + W;
     const int tid = threadIdx.x, T = blockDim.x;
     for (int off = 1; off < T; off <<= 1) {
-        VT *mine = sm + (long long)tid * E;
-#pragma unroll
-        for (int r = 0; r < W; ++r) {
-#pragma unroll
-            for (int q = 0; q < W; ++q) mine[r * W + q] = M[r][q];
-            mine[W * W + r] = c[r];
-        }
+        band_put<VT, W>(sm, T, tid, M, c);
         __syncthreads();
-        if (tid >= off) band_compose_before<VT, W>(M, c, sm + (long long)(tid - off) * E);
+        if (tid >= off) {
+            VT Me[W][W], ce[W];
+            band_get<VT, W>(sm, T, tid - off, Me, ce);
+            // (M, c) <- (M, c) o (Me, ce):  M = M Me,  c = M ce + c
+            VT nM[W][W], nc[W];
+#pragma unroll
+            for (int r = 0; r < W; ++r) {
+                VT v = c[r];
+#pragma unroll
+                for (int k = 0; k < W; ++k) v += M[r][k] * ce[k];
+                nc[r] = v;
+#pragma unroll
+                for (int q = 0; q < W; ++q) {
+                    VT t = 0;
+#pragma unroll
+                    for (int k = 0; k < W; ++k) t += M[r][k] * Me[k][q];
+                    nM[r][q] = t;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < W; ++r) {
+                c[r] = nc[r];
+#pragma unroll
+                for (int q = 0; q < W; ++q) M[r][q] = nM[r][q];
+            }
+        }
         __syncthreads();
     }
 }
@@ -171,25 +185,9 @@ __global__ void __launch_bounds__(BAND_T) k_band_onepass(const VT *__restrict__ 
         band_st_release(flags + 1 + o, 1);
     }
     // the composition of this CTA's chunks before this one (thread tid - 1's)
-    {
-        VT *mine = sm + (long long)tid * E;
-#pragma unroll
-        for (int r = 0; r < W; ++r) {
-#pragma unroll
-            for (int q = 0; q < W; ++q) mine[r * W + q] = M[r][q];
-            mine[W * W + r] = c[r];
-        }
-    }
+    band_put<VT, W>(sm, BAND_T, tid, M, c);
     __syncthreads();
-    if (tid > 0) {
-        const VT *prev = sm + (long long)(tid - 1) * E;
-#pragma unroll
-        for (int r = 0; r < W; ++r) {
-#pragma unroll
-            for (int q = 0; q < W; ++q) M[r][q] = prev[r * W + q];
-            c[r] = prev[W * W + r];
-        }
-    }
+    if (tid > 0) band_get<VT, W>(sm, BAND_T, tid - 1, M, c);
     __syncthreads();  // sm is reused below
 
     // 3. the state entering this CTA: predecessors' totals applied in order
