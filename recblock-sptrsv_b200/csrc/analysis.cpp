@@ -955,6 +955,25 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
             }
         }
         select_kernel(B, opt, lvl_sizes[b]);
+        // The sync-free kernel's lane group.  A deep triangle (32 levels or
+        // more) is bound by its level chain, where each level waits for its
+        // longest rows: there the group is sized for the rows' tail, the
+        // 99th percentile at about 2 entries per lane (the power-law
+        // factor's deepest backward triangle, 74 levels with a 99th
+        // percentile of 18, runs at 16 lanes in 0.21 ms against 0.35 ms at
+        // the mean's 2).  A shallow triangle is bound by its rows'
+        // throughput, and extra lanes only add warps that idle on its short
+        // rows (21 levels with a 99th percentile of 10: 57 us at 1 lane,
+        // 70 us at 4), so it keeps the group for the mean.
+        B.sf_group = B.group;
+        if (B.tri && B.nnz > B.m && B.m > 0 && B.nlv >= 32) {
+            std::vector<int> t(rowcnt[b].begin(), rowcnt[b].end());
+            const size_t k = (size_t)((double)(t.size() - 1) * 0.99);
+            std::nth_element(t.begin(), t.begin() + (long long)k, t.end());
+            int g = 1;
+            while (g < 32 && g * 2 < t[k]) g <<= 1;
+            B.sf_group = std::max(B.group, g);
+        }
     }
 
     // 6. pools.  Squares use a row list (DCSR) when more than half of their

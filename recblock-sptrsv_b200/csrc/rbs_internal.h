@@ -137,6 +137,7 @@ struct ExecBlock {
     int kernel;         // RBS_K_*
     int group;          // lanes per row for k == 1
     // triangles
+    int sf_group;       // lanes per row of the sync-free kernel for k == 1: sized for the row-length tail
     int nlv;            // local level count
     int contiguous;     // 1 if local levels are contiguous row ranges in processing order
     int bandwidth;      // max over rows of (p - smallest column) inside the triangle

@@ -900,12 +900,12 @@ int launch_blocks(Plan &P, std::string &err, bool io = false) {
                 break;
             }
             default: {
-                const int g = K == 1 ? B.group : (K < 32 ? K : 32);
+                const int gs = B.sf_group >= 1 && B.sf_group <= 32 ? B.sf_group : std::max(1, B.group);
+                const int g = K == 1 ? gs : (K < 32 ? K : 32);
                 const long long warps = ((long long)B.m * g + 31) / 32;
                 int grid = (int)std::min<long long>(syncfree_grid<VT, K>(D), (warps + 7) / 8);
                 k_tri_syncfree<VT, K><<<std::max(grid, 1), 256, 0, st>>>(D.rp + B.rp_off, D.col, val, inv + B.r0, bb,
-                                                                        xx, B.m, B.group, D.tickets + ti, D.status,
-                                                                        limit);
+                                                                        xx, B.m, gs, D.tickets + ti, D.status, limit);
                 break;
             }
             }
