@@ -18,6 +18,11 @@
 // 4-16 byte copies and the level's loads are coalesced.
 // Dependencies within the last XW rows come from the window; older ones
 // from x in global memory (written by this CTA before an earlier barrier).
+// When every dependency lies in the window (WIN) and W >= 2, the columns are
+// window slots (0..XW, XW the zero slot) held as 16-bit integers: a row's
+// columns are one 4- or 8-byte copy, and the level's column reads take half
+// the shared-memory wavefronts of 32-bit columns.  Wide levels are bound by
+// the shared-memory pipe, which carries every staged byte twice.
 //
 // Several right-hand sides: CTA y of the launch's second grid dimension
 // solves the G consecutive columns [y*G, y*G+G) on its own, with no
@@ -47,7 +52,8 @@ constexpr int CA_XW = CA_WINDOW_ROWS;    // x window (rows), plus one always-zer
 constexpr int CA_TAB = 6144;   // ints of the level table staged in shared memory (4 per level)
 
 struct CaDesc {
-    const int *col;   // row-major level-ELL columns (block-local), padding -1
+    const void *col;  // row-major level-ELL columns: block-local rows (int, padding -1), or
+                      // window slots (short, padding the zero slot) for WIN blocks with W >= 2
     const void *val;  // level-ELL values
     const void *inv;  // inverse diagonal of the block's rows
     const void *b;    // right-hand side of the block's rows, column group 0 (row stride ld)
@@ -57,9 +63,10 @@ struct CaDesc {
     long long gstride;  // elements from one column group to the next
 };
 
-template <typename VT, int W, int S, int G = 1>
+// CB: bytes per column (4, or 2 for window slots)
+template <typename VT, int W, int S, int G = 1, int CB = 4>
 struct CaLayout {
-    static constexpr size_t col_bytes = (size_t)W * CA_ROWS * 4;
+    static constexpr size_t col_bytes = (size_t)W * CA_ROWS * CB;
     static constexpr size_t val_bytes = (size_t)W * CA_ROWS * sizeof(VT);
     static constexpr size_t inv_bytes = (size_t)CA_ROWS * sizeof(VT);
     static constexpr size_t b_bytes = (size_t)G * CA_ROWS * sizeof(VT);
@@ -119,9 +126,22 @@ __device__ __forceinline__ void cp_async_sn(unsigned dst, const void *src) {
 // G: right-hand sides per CTA (blockIdx.y selects the column group).
 // MC: a multi-column launch; without it the row stride is 1 and there is
 // one group (the single right-hand-side solve, with no stride arithmetic).
+template <int W, bool WIN>
+constexpr int ca_col_bytes() {
+    return WIN && W >= 2 ? 2 : 4;
+}
+
+// Dynamic shared memory of one instance of k_tri_level_ca.
+template <typename VT, int W, int S, bool WIN, int G>
+constexpr size_t ca_smem_total() {
+    return CaLayout<VT, W, S, G, ca_col_bytes<W, WIN>()>::total;
+}
+
 template <typename VT, int W, int S, bool WIN, int G = 1, bool MC = false>
 __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict__ descs) {
-    using Lay = CaLayout<VT, W, S, G>;
+    constexpr int CB = ca_col_bytes<W, WIN>();
+    using CT = std::conditional_t<CB == 2, short, int>;
+    using Lay = CaLayout<VT, W, S, G, CB>;
     using VG = Vec<VT, G>;
     static_assert(S == 2 || S == 4, "stage count 2 or 4");
     static_assert(G == 1 || G == 2 || G == 4, "1, 2 or 4 right-hand sides per CTA");
@@ -149,12 +169,12 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
     const int4 *lt = reinterpret_cast<const int4 *>(in_smem ? tab : d.lvl);
 
     // this thread's source rows and stage-0 slots
-    const int *colp = d.col + tid * W;
+    const CT *colp = static_cast<const CT *>(d.col) + tid * W;
     const VT *valp = (const VT *)d.val + tid * W;
     const VT *inv_t = (const VT *)d.inv + tid;
     const VT *b_t = (const VT *)d.b + goff + (size_t)tid * ld;
     const unsigned s0 = (unsigned)__cvta_generic_to_shared(sm);
-    const unsigned s_col = s0 + tid * W * 4;
+    const unsigned s_col = s0 + tid * W * CB;
     const unsigned s_val = s0 + (unsigned)Lay::col_bytes + tid * W * (unsigned)sizeof(VT);
     const unsigned s_inv = s0 + (unsigned)(Lay::col_bytes + Lay::val_bytes) + tid * (unsigned)sizeof(VT);
     const unsigned s_b = s0 + (unsigned)(Lay::col_bytes + Lay::val_bytes + Lay::inv_bytes) +
@@ -166,7 +186,7 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
     auto stage = [&](int l, const int4 &e, auto slot) {
         constexpr unsigned off = decltype(slot)::value * (unsigned)Lay::stage_bytes;
         if (l < nlv && tid < e.z) {
-            cp_async_sn<4 * W>(s_col + off, colp + e.y);
+            cp_async_sn<CB * W>(s_col + off, colp + e.y);
             cp_async_sn<(int)sizeof(VT) * W>(s_val + off, valp + e.y);
             cp_async_sn<(int)sizeof(VT)>(s_inv + off, inv_t + e.x);
             cp_async_sn<(int)sizeof(VT) * G>(s_b + off, b_t + (size_t)e.x * ld);
@@ -190,7 +210,7 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
         cp_async_wait<S - 1>();
         if (tid < hi - lo) {
             const unsigned char *st = sm + (size_t)U * Lay::stage_bytes;
-            const Vec<int, W> cs = reinterpret_cast<const Vec<int, W> *>(st)[tid];
+            const Vec<CT, W> cs = reinterpret_cast<const Vec<CT, W> *>(st)[tid];
             const Vec<VT, W> vs = reinterpret_cast<const Vec<VT, W> *>(st + Lay::col_bytes)[tid];
             const VT iv = reinterpret_cast<const VT *>(st + Lay::col_bytes + Lay::val_bytes)[tid];
             const VG bv = reinterpret_cast<const VG *>(st + Lay::col_bytes + Lay::val_bytes + Lay::inv_bytes)[tid];

@@ -60,6 +60,7 @@ struct DeviceState {
     EllChunk *ell_chunks = nullptr;
     std::map<long long, CsfDesc *> ell_cache;
     int *ca_tab = nullptr, *ca_col = nullptr;
+    short *ca_col16 = nullptr;  // window-slot columns of WIN blocks with W >= 2 (16-bit copy of ca_col)
     double *ca_val = nullptr;
     float *ca_val32 = nullptr;
     std::map<long long, CaDesc *> ca_cache;
@@ -358,9 +359,9 @@ int ca_attr(std::string &err) {
     static std::atomic<unsigned long long> done{0};
     if (!attr_done(done)) {
         CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, false, G, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)CaLayout<VT, W, S, G>::total));
+                                (int)ca_smem_total<VT, W, S, false, G>()));
         CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, true, G, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)CaLayout<VT, W, S, G>::total));
+                                (int)ca_smem_total<VT, W, S, true, G>()));
         attr_mark(done);
     }
     return RBS_OK;
@@ -423,7 +424,8 @@ int ca_descs(Plan &P, CaDesc *&out, int K, int GL, std::string &err) {
     for (const ExecBlock &B : P.blocks) {
         if (!B.tri || B.kernel != RBS_K_LEVEL || !B.ca_ok) continue;
         CaDesc d{};
-        d.col = D.ca_col + B.ca_lo;
+        d.col = B.ca_win && B.ca_w >= 2 ? static_cast<const void *>(D.ca_col16 + B.ca_lo)
+                                        : static_cast<const void *>(D.ca_col + B.ca_lo);
         d.val = Pools<VT>::cav(D) + B.ca_lo;
         d.inv = Pools<VT>::inv(D) + B.r0;
         const long long rowlen = GL ? GL : K;  // values per row within a column group's rows
@@ -465,9 +467,9 @@ void launch_ca(const ExecBlock &B, const CaDesc *desc, int K, cudaStream_t st) {
     const int nt = std::min(1024, std::max(32, (B.maxwidth + 31) / 32 * 32));
     const dim3 grid(1, K / G);
     if (B.ca_win)
-        k_tri_level_ca<VT, W, S, true, G, MC><<<grid, nt, CaLayout<VT, W, S, G>::total, st>>>(desc);
+        k_tri_level_ca<VT, W, S, true, G, MC><<<grid, nt, ca_smem_total<VT, W, S, true, G>(), st>>>(desc);
     else
-        k_tri_level_ca<VT, W, S, false, G, MC><<<grid, nt, CaLayout<VT, W, S, G>::total, st>>>(desc);
+        k_tri_level_ca<VT, W, S, false, G, MC><<<grid, nt, ca_smem_total<VT, W, S, false, G>(), st>>>(desc);
 }
 
 template <typename VT>
@@ -490,20 +492,26 @@ void launch_ca_any(const ExecBlock &B, const CaDesc *desc, int K, int G, cudaStr
     }
 }
 
-// Shared memory of the staged level kernel as launch_ca_any picks it.
+// Shared memory of the staged level kernel as launch_ca_any picks it
+// (window blocks with W >= 2 stage 16-bit columns).
+template <typename VT, int W, int S, int G>
+size_t ca_total(bool win) {
+    return win ? ca_smem_total<VT, W, S, true, G>() : ca_smem_total<VT, W, S, false, G>();
+}
+
 template <typename VT>
-size_t ca_smem_bytes(int W, int K, int G) {
+size_t ca_smem_bytes(int W, bool win, int K, int G) {
     if (K == 1 || G == 1) {
-        if (W == 1) return CaLayout<VT, 1, 4, 1>::total;
-        if (W == 2) return CaLayout<VT, 2, 4, 1>::total;
-        return CaLayout<VT, 4, 2, 1>::total;
+        if (W == 1) return ca_total<VT, 1, 4, 1>(win);
+        if (W == 2) return ca_total<VT, 2, 4, 1>(win);
+        return ca_total<VT, 4, 2, 1>(win);
     }
     if constexpr (sizeof(VT) == 8) {
-        return W == 1 ? CaLayout<VT, 1, 2, 2>::total : CaLayout<VT, 2, 2, 2>::total;
+        return W == 1 ? ca_total<VT, 1, 2, 2>(win) : ca_total<VT, 2, 2, 2>(win);
     } else {
-        if (W == 1) return CaLayout<VT, 1, 4, 2>::total;
-        if (W == 2) return CaLayout<VT, 2, 4, 2>::total;
-        return CaLayout<VT, 4, 2, 2>::total;
+        if (W == 1) return ca_total<VT, 1, 4, 2>(win);
+        if (W == 2) return ca_total<VT, 2, 4, 2>(win);
+        return ca_total<VT, 4, 2, 2>(win);
     }
 }
 
@@ -781,7 +789,8 @@ int launch_blocks(Plan &P, std::string &err, bool io = false) {
             if (B.ca_ok && B.lvl_var == LVL_CA) {
                 const long long ne = B.ca_hi - B.ca_lo;
                 prefetch_range(D.side, Pools<VT>::cav(D) + B.ca_lo, ne * (long long)sizeof(VT));
-                prefetch_range(D.side, D.ca_col + B.ca_lo, ne * 4);
+                if (B.ca_win && B.ca_w >= 2) prefetch_range(D.side, D.ca_col16 + B.ca_lo, ne * 2);
+                else prefetch_range(D.side, D.ca_col + B.ca_lo, ne * 4);
                 prefetch_range(D.side, inv + B.r0, (long long)B.m * sizeof(VT));
                 budget -= ne * ((long long)sizeof(VT) + 4) + (long long)B.m * sizeof(VT);
                 continue;
@@ -821,7 +830,7 @@ int launch_blocks(Plan &P, std::string &err, bool io = false) {
             size_t ca_min = 0;
             for (const ExecBlock &B : P.blocks)
                 if (B.tri && B.kernel == RBS_K_LEVEL && B.ca_ok) {
-                    const size_t v = ca_smem_bytes<VT>(B.ca_w, K, GL);
+                    const size_t v = ca_smem_bytes<VT>(B.ca_w, B.ca_win != 0, K, GL);
                     ca_min = ca_min ? std::min(ca_min, v) : v;
                 }
             move_smem = move_reserve(D, ca_min);
@@ -1441,6 +1450,14 @@ int device_build(Plan &P, std::string &err) {
     }
     if ((rc = upload(D, D.ca_tab, P.ca_tab, err))) return rc;
     if ((rc = upload(D, D.ca_col, P.ca_col, err))) return rc;
+    {
+        // window slots (0..CA_WINDOW_ROWS) fit 16 bits; other blocks' entries stay 0
+        std::vector<short> c16(P.ca_col.size(), 0);
+        for (const ExecBlock &B : P.blocks)
+            if (B.tri && B.ca_ok && B.ca_win && B.ca_w >= 2)
+                for (long long e = B.ca_lo; e < B.ca_hi; ++e) c16[(size_t)e] = (short)P.ca_col[(size_t)e];
+        if ((rc = upload(D, D.ca_col16, c16, err))) return rc;
+    }
     if ((rc = upload(D, D.ca_val, P.ca_val, err))) return rc;
     if (D.mixed) {
         const auto c32 = to_f32(P.ca_val);
@@ -1715,6 +1732,7 @@ void device_free(Plan &P) {
     cudaFree(D.ell_chunks);
     cudaFree(D.ca_tab);
     cudaFree(D.ca_col);
+    cudaFree(D.ca_col16);
     cudaFree(D.ca_val);
     cudaFree(D.ca_val32);
     cudaFree(D.lc_rec64);
