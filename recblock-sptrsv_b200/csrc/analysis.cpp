@@ -1554,13 +1554,15 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
         dv = P.ca_val;
         return RBS_OK;
     }
-    if (name == "ca_block") {  // per block: table offset, first entry, ELL width (-1: no level-ELL layout)
-        iv.assign(3 * sum, -1);
+    if (name == "ca_block") {  // per block: table offset, first entry, ELL width, columns are window
+                               // slots (1/0) (all -1: no level-ELL layout)
+        iv.assign(4 * sum, -1);
         for (int b = 0; b < sum; ++b)
             if (P.blocks[b].ca_ok) {
-                iv[3 * b] = (int)P.blocks[b].ca_tab_off;
-                iv[3 * b + 1] = (int)P.blocks[b].ca_lo;
-                iv[3 * b + 2] = P.blocks[b].ca_w;
+                iv[4 * b] = (int)P.blocks[b].ca_tab_off;
+                iv[4 * b + 1] = (int)P.blocks[b].ca_lo;
+                iv[4 * b + 2] = P.blocks[b].ca_w;
+                iv[4 * b + 3] = P.blocks[b].ca_win;
             }
         return RBS_OK;
     }

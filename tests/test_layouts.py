@@ -25,7 +25,7 @@ def test_ell_only_where_it_can_run(name, csr):
              for sel in (rbs.SELECT_AUTO, rbs.SELECT_TUNE)}
     auto = plans[rbs.SELECT_AUTO]
     eb = auto.export("ell_block").reshape(-1, 2)
-    cb = auto.export("ca_block").reshape(-1, 3)
+    cb = auto.export("ca_block").reshape(-1, 4)
     lb = auto.export("lc_block").reshape(-1, 3)
     for b in range(len(eb)):
         if eb[b, 0] >= 0:
