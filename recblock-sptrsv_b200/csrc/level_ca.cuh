@@ -9,7 +9,9 @@
 // -- is copied by each thread for its own row of level l+S-1 with cp.async
 // while level l is being solved, into an S-stage shared-memory ring, so it
 // is on chip when the level comes up.  A thread only reads what it copied
-// itself (cp.async.wait_group), so staging needs no extra synchronisation.
+// itself (cp.async.wait_group), so staging needs no extra synchronisation,
+// and it reads the next level's row into registers before the barrier that
+// ends a level.
 //
 // Layout (host-built): per level l a table entry {lo, off, w, 0}: rows
 // [lo, lo + w) of the block; the block's ELL width W (1, 2 or 4) is fixed,
@@ -198,22 +200,46 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
     int4 ent[S];
 #pragma unroll
     for (int k = 0; k < S; ++k) ent[k] = lt[k < nlv ? k : nlv];
-    // solve level l from slot U: read the entry of level l+S a level early,
-    // stage level l+S-1 into the slot freed at the last barrier, wait for
-    // this thread's copies of level l
+    // solve level l (its staged row already in registers): read the entry of
+    // level l+S a level early.  S = 4: after the level's work, stage level
+    // l+S-1 into the slot freed at the last barrier, wait for this thread's
+    // copies of level l+1 (two groups may stay in flight) and read them into
+    // registers, all before the barrier; the copies issued at the start of
+    // the level instead queued ahead of its dependency reads (c1a 0.970 ms
+    // against 0.957).  S = 2: stage at the start and wait for level l's own
+    // copies, as a later issue would leave no level between copy and use.
+    // the staged row of the next level to solve, read into registers before
+    // the barrier that starts it (a thread reads only its own copies, so
+    // only the window reads must wait for the barrier)
+    Vec<CT, W> ncs{};
+    Vec<VT, W> nvs{};
+    VT niv{};
+    VG nbv{};
+    auto load_staged = [&](int w, auto slot) {
+        constexpr int U = decltype(slot)::value;
+        if (tid < w) {
+            const unsigned char *st = sm + (size_t)U * Lay::stage_bytes;
+            ncs = reinterpret_cast<const Vec<CT, W> *>(st)[tid];
+            nvs = reinterpret_cast<const Vec<VT, W> *>(st + Lay::col_bytes)[tid];
+            niv = reinterpret_cast<const VT *>(st + Lay::col_bytes + Lay::val_bytes)[tid];
+            nbv = reinterpret_cast<const VG *>(st + Lay::col_bytes + Lay::val_bytes + Lay::inv_bytes)[tid];
+        }
+    };
     auto level = [&](int l, int &lo, auto slot) {
         constexpr int U = decltype(slot)::value;
         const int hi = ent[(U + 1) % S].x;
         const int4 e_stage = ent[(U + S - 1) % S];
         if (l + S <= nlv) ent[U] = lt[l + S];  // level l's own entry is no longer needed
-        stage(l + S - 1, e_stage, std::integral_constant<int, (U + S - 1) % S>{});
-        cp_async_wait<S - 1>();
+        if constexpr (S == 2) {
+            stage(l + S - 1, e_stage, std::integral_constant<int, (U + S - 1) % S>{});
+            cp_async_wait<S - 1>();
+            load_staged(hi - lo, slot);
+        }
+        const Vec<CT, W> cs = ncs;
+        const Vec<VT, W> vs = nvs;
+        const VT iv = niv;
+        const VG bv = nbv;
         if (tid < hi - lo) {
-            const unsigned char *st = sm + (size_t)U * Lay::stage_bytes;
-            const Vec<CT, W> cs = reinterpret_cast<const Vec<CT, W> *>(st)[tid];
-            const Vec<VT, W> vs = reinterpret_cast<const Vec<VT, W> *>(st + Lay::col_bytes)[tid];
-            const VT iv = reinterpret_cast<const VT *>(st + Lay::col_bytes + Lay::val_bytes)[tid];
-            const VG bv = reinterpret_cast<const VG *>(st + Lay::col_bytes + Lay::val_bytes + Lay::inv_bytes)[tid];
             VT sum[G];
 #pragma unroll
             for (int g = 0; g < G; ++g) sum[g] = 0;
@@ -241,6 +267,11 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
             if constexpr (G == 1) x[(size_t)r * ld] = xv.v[0];
             else *reinterpret_cast<VG *>(x + (size_t)r * ld) = xv;
         }
+        if constexpr (S != 2) {
+            stage(l + S - 1, e_stage, std::integral_constant<int, (U + S - 1) % S>{});
+            cp_async_wait<S - 2>();
+            load_staged(ent[(U + 2) % S].x - hi, std::integral_constant<int, (U + 1) % S>{});
+        }
         lo = hi;
         __syncthreads();
     };
@@ -249,6 +280,8 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
     if constexpr (S == 4) {
         stage(1, ent[1], std::integral_constant<int, 1>{});
         stage(2, ent[2], std::integral_constant<int, 2>{});
+        cp_async_wait<S - 2>();
+        load_staged(ent[1].x, std::integral_constant<int, 0>{});
     }
     int lo = 0;
 #pragma unroll 1
