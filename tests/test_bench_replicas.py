@@ -1,7 +1,9 @@
 """The multi-GPU arm of bench.py runs independent replicas (a triangular
 solve has no data-path collective); the only cross-rank step is the max of
-the ranks' timed totals.  Checked here with world_size 2 over gloo on CPU.
-The reference arm runs on rank 0 alone and prints the contract's line."""
+the ranks' timed totals.  Checked here with world_size 2 over gloo on CPU:
+the max-over-ranks throughput, and that the ranks' host analyses of the
+same workload give identical plans.  The reference arm runs on rank 0 alone
+and prints the contract's line."""
 import os
 import sys
 
@@ -46,6 +48,54 @@ def test_replica_throughput_uses_slowest_rank():
     for rank, value, ms_per_step in out:
         assert ms_per_step == pytest.approx(15.0)          # slowest rank: 150 ms / 10 solves
         assert value == pytest.approx(2 * 10 * 1000.0 / 150.0)
+
+
+def _rank_plan(rank, world, port, q):
+    # the host side of one replica: the rank's analysis of the bench's small
+    # band workload (host-only, no device), digested and gathered over gloo
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    for p in (ROOT, os.path.join(ROOT, "recblock-sptrsv_b200")):
+        sys.path.insert(0, p)
+    import hashlib
+
+    import bench
+    import rbs
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    s = bench.make_system("c0", bench.FORWARD)
+    plan = rbs.analyse(s["cp"], s["ri"], s["cv"], substitution=bench.FORWARD, lv=-1,
+                       opts=rbs.options(host_only=1))
+    h = hashlib.sha256()
+    for key in ("kernel", "perm", "levelPtr", "recblock_Ptr", "recblock_Index", "recblock_Val", "ca_tab", "lc_tab",
+                "block_rows"):
+        h.update(key.encode())
+        h.update(plan.export(key).tobytes())
+    mine = torch.tensor(list(h.digest()), dtype=torch.int64)
+    got = [torch.zeros_like(mine) for _ in range(world)]
+    dist.all_gather(got, mine)
+    q.put((rank, [bytes(t.tolist()).hex() for t in got], int(plan.info().nlevel)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_replicas_build_identical_plans():
+    # every rank of `bench.py --gpus N` analyses the same workload for its own
+    # GPU; the host analysis is deterministic, so all ranks hold the same
+    # plan (same blocks, kernels, layouts) and time the same work
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 30000 + os.getpid() % 1000
+    procs = [ctx.Process(target=_rank_plan, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, digests, nlevel in out:
+        assert len(set(digests)) == 1, (rank, digests)
+        assert nlevel > 1
+    assert out[0][1] == out[1][1]
 
 
 def test_reference_arm_runs_on_rank0_only(monkeypatch, capsys):
