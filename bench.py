@@ -64,7 +64,7 @@ def parse():
                                                                "(short runs for profilers)")
     ap.add_argument("--side", default=None, choices=sorted(SIDE_FUNCS),
                     help="run one side measurement alone on cuda:0 and print its JSON (no benchmark line)")
-    ap.add_argument("--ks", default="1,8,32,128", help="right-hand-side counts of the multi_rhs side measurement")
+    ap.add_argument("--ks", default="1,8,32,64,128", help="right-hand-side counts of the multi_rhs side measurement")
     ap.add_argument("--precs", default="fp64,mixed", help="precisions of the multi_rhs side measurement")
     ap.add_argument("--sides", default=None,
                     help="comma-separated side measurements to run after the benchmark line's own "

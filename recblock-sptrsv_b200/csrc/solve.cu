@@ -378,11 +378,12 @@ template <typename VT> constexpr int ca_stages(int W, int G) {
 
 // Right-hand sides per CTA of a staged level triangle solved for K columns.
 // One column per CTA walks a level fastest (half the shared-memory traffic
-// per row), but takes an SM per column; the overlapped walk moves the
-// columns in and out on the SMs the triangles leave free.  On the 2D
-// Laplacian (n = 1M, FP64) one column per CTA measured 20.4k solves/s
-// against 17.6k at 32 columns, two columns per CTA 49.4k against 37.7k at
-// 128 (with 128 CTAs only 20 SMs were left for the moves).  RBS_CA_GROUP
+// per row), but every CTA reads the same level's rows at the same moment,
+// so the L2 lines holding them serve one request per CTA: past about 32
+// CTAs a solve's time grows with their number.  On the 2D Laplacian
+// (n = 1M, FP64), one column per CTA against two: k = 16 14.7k against
+// 11.1k solves/s, k = 32 25.9k against 20.6k, k = 48 23.7k against 28.4k,
+// k = 64 28.1k against 36.2k, k = 128 29.7k against 55.8k.  RBS_CA_GROUP
 // (1 or 2) overrides the choice.
 template <typename VT> int ca_group(const ExecBlock &B, int K) {
     if (K == 1) return 1;
@@ -390,7 +391,7 @@ template <typename VT> int ca_group(const ExecBlock &B, int K) {
         const char *e = std::getenv("RBS_CA_GROUP");
         return e ? std::atoi(e) : 0;
     }();
-    int G = forced == 1 || forced == 2 ? forced : K <= 64 ? 1 : 2;
+    int G = forced == 1 || forced == 2 ? forced : K <= 32 ? 1 : 2;
     if (G == 2 && ca_stages<VT>(B.ca_w, 2) == 0) G = 1;
     return G;
 }
