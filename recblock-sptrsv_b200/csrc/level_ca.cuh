@@ -9,9 +9,9 @@
 // -- is copied by each thread for its own row of level l+S-1 with cp.async
 // while level l is being solved, into an S-stage shared-memory ring, so it
 // is on chip when the level comes up.  A thread only reads what it copied
-// itself (cp.async.wait_group), so staging needs no extra synchronisation,
-// and it reads the next level's row into registers before the barrier that
-// ends a level.
+// itself (cp.async.wait_group), so staging needs no extra synchronisation;
+// in triangles of wide levels it reads the next level's row into registers
+// before the barrier that ends a level.
 //
 // Layout (host-built): per level l a table entry {lo, off, w, 0}: rows
 // [lo, lo + w) of the block; the block's ELL width W (1, 2 or 4) is fixed,
@@ -139,7 +139,9 @@ constexpr size_t ca_smem_total() {
     return CaLayout<VT, W, S, G, ca_col_bytes<W, WIN>()>::total;
 }
 
-template <typename VT, int W, int S, bool WIN, int G = 1, bool MC = false>
+// LATE (with S = 4): the late copies and register read-ahead below, for
+// triangles of wide levels.
+template <typename VT, int W, int S, bool WIN, int G = 1, bool MC = false, bool LATE = false>
 __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict__ descs) {
     constexpr int CB = ca_col_bytes<W, WIN>();
     using CT = std::conditional_t<CB == 2, short, int>;
@@ -200,17 +202,21 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
     int4 ent[S];
 #pragma unroll
     for (int k = 0; k < S; ++k) ent[k] = lt[k < nlv ? k : nlv];
-    // solve level l (its staged row already in registers): read the entry of
-    // level l+S a level early.  S = 4: after the level's work, stage level
-    // l+S-1 into the slot freed at the last barrier, wait for this thread's
-    // copies of level l+1 (two groups may stay in flight) and read them into
-    // registers, all before the barrier; the copies issued at the start of
-    // the level instead queued ahead of its dependency reads (c1a 0.970 ms
-    // against 0.957).  S = 2: stage at the start and wait for level l's own
-    // copies, as a later issue would leave no level between copy and use.
-    // the staged row of the next level to solve, read into registers before
-    // the barrier that starts it (a thread reads only its own copies, so
-    // only the window reads must wait for the barrier)
+    // solve level l: read the entry of level l+S a level early.  Late (S = 4,
+    // triangles of wide levels): after the level's work, stage level l+S-1
+    // into the slot freed at the last barrier, wait for this thread's copies
+    // of level l+1 (two groups may stay in flight) and read them into
+    // registers, all before the barrier; copies issued at the start of a
+    // wide level queue ahead of its dependency reads (c1a's wide triangles
+    // 108-111 -> 103-107 us).  Otherwise stage at the start of the level and
+    // wait for level l's own copies: a narrow level is bound by its barrier
+    // chain, which the read-ahead lengthens (c1a's narrow triangles 148-150
+    // -> 154-155 us with it); with S = 2 a later issue would leave no level
+    // between copy and use.
+    constexpr bool late = S == 4 && LATE;
+    // late: this thread's staged row of the next level, read into registers
+    // before the barrier that starts it (a thread reads only its own copies,
+    // so only the window reads must wait for the barrier)
     Vec<CT, W> ncs{};
     Vec<VT, W> nvs{};
     VT niv{};
@@ -230,16 +236,27 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
         const int hi = ent[(U + 1) % S].x;
         const int4 e_stage = ent[(U + S - 1) % S];
         if (l + S <= nlv) ent[U] = lt[l + S];  // level l's own entry is no longer needed
-        if constexpr (S == 2) {
+        if constexpr (!late) {
             stage(l + S - 1, e_stage, std::integral_constant<int, (U + S - 1) % S>{});
             cp_async_wait<S - 1>();
-            load_staged(hi - lo, slot);
         }
-        const Vec<CT, W> cs = ncs;
-        const Vec<VT, W> vs = nvs;
-        const VT iv = niv;
-        const VG bv = nbv;
         if (tid < hi - lo) {
+            Vec<CT, W> cs;
+            Vec<VT, W> vs;
+            VT iv;
+            VG bv;
+            if constexpr (late) {
+                cs = ncs;
+                vs = nvs;
+                iv = niv;
+                bv = nbv;
+            } else {
+                const unsigned char *st = sm + (size_t)U * Lay::stage_bytes;
+                cs = reinterpret_cast<const Vec<CT, W> *>(st)[tid];
+                vs = reinterpret_cast<const Vec<VT, W> *>(st + Lay::col_bytes)[tid];
+                iv = reinterpret_cast<const VT *>(st + Lay::col_bytes + Lay::val_bytes)[tid];
+                bv = reinterpret_cast<const VG *>(st + Lay::col_bytes + Lay::val_bytes + Lay::inv_bytes)[tid];
+            }
             VT sum[G];
 #pragma unroll
             for (int g = 0; g < G; ++g) sum[g] = 0;
@@ -267,7 +284,7 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
             if constexpr (G == 1) x[(size_t)r * ld] = xv.v[0];
             else *reinterpret_cast<VG *>(x + (size_t)r * ld) = xv;
         }
-        if constexpr (S != 2) {
+        if constexpr (late) {
             stage(l + S - 1, e_stage, std::integral_constant<int, (U + S - 1) % S>{});
             cp_async_wait<S - 2>();
             load_staged(ent[(U + 2) % S].x - hi, std::integral_constant<int, (U + 1) % S>{});
@@ -280,6 +297,8 @@ __global__ void __launch_bounds__(1024) k_tri_level_ca(const CaDesc *__restrict_
     if constexpr (S == 4) {
         stage(1, ent[1], std::integral_constant<int, 1>{});
         stage(2, ent[2], std::integral_constant<int, 2>{});
+    }
+    if constexpr (late) {
         cp_async_wait<S - 2>();
         load_staged(ent[1].x, std::integral_constant<int, 0>{});
     }

@@ -362,6 +362,12 @@ int ca_attr(std::string &err) {
                                 (int)ca_smem_total<VT, W, S, false, G>()));
         CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, true, G, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)ca_smem_total<VT, W, S, true, G>()));
+        if constexpr (S == 4) {
+            CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, false, G, MC, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ca_smem_total<VT, W, S, false, G>()));
+            CK(cudaFuncSetAttribute(k_tri_level_ca<VT, W, S, true, G, MC, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ca_smem_total<VT, W, S, true, G>()));
+        }
         attr_mark(done);
     }
     return RBS_OK;
@@ -467,6 +473,18 @@ template <typename VT, int W, int S, int G, bool MC>
 void launch_ca(const ExecBlock &B, const CaDesc *desc, int K, cudaStream_t st) {
     const int nt = std::min(1024, std::max(32, (B.maxwidth + 31) / 32 * 32));
     const dim3 grid(1, K / G);
+    if constexpr (S == 4) {
+        // triangles of wide levels (a mean of 384 rows or more) take the late
+        // copies and the register read-ahead
+        if (B.m >= 384LL * std::max(1, B.nlv)) {
+            if (B.ca_win)
+                k_tri_level_ca<VT, W, S, true, G, MC, true><<<grid, nt, ca_smem_total<VT, W, S, true, G>(), st>>>(desc);
+            else
+                k_tri_level_ca<VT, W, S, false, G, MC, true><<<grid, nt, ca_smem_total<VT, W, S, false, G>(), st>>>(
+                    desc);
+            return;
+        }
+    }
     if (B.ca_win)
         k_tri_level_ca<VT, W, S, true, G, MC><<<grid, nt, ca_smem_total<VT, W, S, true, G>(), st>>>(desc);
     else
