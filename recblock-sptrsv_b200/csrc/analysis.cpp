@@ -897,9 +897,11 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
         ExecBlock &TB = P.blocks[2 * tri_of(p)];
         TB.bandwidth = std::max(TB.bandwidth, reach[p]);
     }
-    // block statistics and the reference's method codes
+    // block statistics, the reference's method codes and the kernel choice:
+    // blocks are independent, done on host threads
     std::vector<std::vector<int>> lvl_sizes((size_t)P.sum_block);
-    for (int b = 0; b < P.sum_block; ++b) {
+    parallel_for((size_t)P.sum_block, [&](size_t bi) {
+        const int b = (int)bi;
         ExecBlock &B = P.blocks[b];
         long long tot = 0;
         int nonempty = 0, longrows = 0, lenmax = B.m > 0 ? rowcnt[b][0] : 0;
@@ -974,7 +976,7 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
             while (g < 32 && g * 2 < t[k]) g <<= 1;
             B.sf_group = std::max(B.group, g);
         }
-    }
+    });
 
     // 6. pools.  Squares use a row list (DCSR) when more than half of their
     //    rows are empty; rows longer than 2048 go to the split kernel.
@@ -988,71 +990,128 @@ int analyse_after_levels(Plan &P, int n, int nnz, int substitution, int lv, cons
     for (int b = 0; b < P.sum_block; ++b) total_entries += P.blocks[b].tri ? P.blocks[b].nnz - P.blocks[b].m : P.blocks[b].nnz;
     P.col_pool.reserve((size_t)total_entries);
     P.val_pool.reserve((size_t)total_entries);
-    // entry offset of every (block, local row) so the fill is one pass over rows
+    // entry offset of every (block, local row) so the fill is one pass over
+    // rows.  Blocks are independent: their sizes on host threads, then the
+    // pools' offsets in block order, then every block fills its own parts
+    // (row pointer, row lists, level pointer and map) on host threads.
     std::vector<std::vector<int>> rowstart((size_t)P.sum_block);
-    long long ent = 0;
+    struct PoolSizes {
+        long long ent = 0;
+        int nrows = 0, nlong = 0, nmed = 0;
+        bool dcsr = false, med = false, lvl = false, map = false;
+    };
+    std::vector<PoolSizes> ps((size_t)P.sum_block);
+    parallel_for((size_t)P.sum_block, [&](size_t bi) {
+        const ExecBlock &B = P.blocks[bi];
+        PoolSizes &z = ps[bi];
+        const std::vector<int> &rc = rowcnt[bi];
+        z.dcsr = !B.tri && B.kernel == RBS_K_SPMV &&
+                 (opt.select == RBS_SELECT_REFERENCE ? (B.ref_method == 1 || B.ref_method == 3) : 2 * B.nonempty < B.m);
+        z.med = !B.tri && B.kernel == RBS_K_SPMV && B.group < 32 && B.lenmax > kMedRow;
+        int nonempty = 0;
+        for (int r = 0; r < B.m; ++r) {
+            const int c = rc[r];
+            z.ent += c;
+            nonempty += c != 0;
+            z.nlong += c > kLongRow;
+            z.nmed += c > kMedRow && c <= kLongRow;
+        }
+        z.nrows = z.dcsr ? nonempty : B.m;
+        z.lvl = wants_level(B, opt);
+        z.map = z.lvl && !B.contiguous;
+    });
+    long long ent = 0, rp_n = 0, rows_n = 0, lvl_n = 0, map_n = 0;
+    std::vector<long long> ent0((size_t)P.sum_block), rows_dcsr0((size_t)P.sum_block);
     for (int b = 0; b < P.sum_block; ++b) {
         ExecBlock &B = P.blocks[b];
-        rowstart[b].resize((size_t)B.m + 1);
-        rowstart[b][0] = (int)ent;
-        for (int r = 0; r < B.m; ++r) rowstart[b][r + 1] = rowstart[b][r] + rowcnt[b][r];
-        ent = rowstart[b][B.m];
-        bool dcsr = !B.tri && B.kernel == RBS_K_SPMV &&
-                    (opt.select == RBS_SELECT_REFERENCE ? (B.ref_method == 1 || B.ref_method == 3)
-                                                        : 2 * B.nonempty < B.m);
-        B.rp_off = (long long)P.rp_pool.size();
-        if (dcsr) {
-            B.rows_off = (long long)P.rows_pool.size();
-            int cnt = 0;
-            for (int r = 0; r < B.m; ++r)
-                if (rowcnt[b][r]) {
-                    P.rows_pool.push_back(r);
-                    P.rp_pool.push_back(rowstart[b][r]);
-                    ++cnt;
-                }
-            P.rp_pool.push_back(rowstart[b][B.m]);
-            B.nrows = cnt;
-        } else {
-            for (int r = 0; r <= B.m; ++r) P.rp_pool.push_back(rowstart[b][r]);
-            B.nrows = B.m;
+        const PoolSizes &z = ps[(size_t)b];
+        ent0[(size_t)b] = ent;
+        ent += z.ent;
+        B.rp_off = rp_n;
+        rp_n += (long long)z.nrows + 1;
+        B.nrows = z.nrows;
+        rows_dcsr0[(size_t)b] = rows_n;
+        if (z.dcsr) {
+            B.rows_off = rows_n;
+            rows_n += z.nrows;
         }
         if (!B.tri && B.longrows) {
             // positions in the row pointer: the row for CSR, the list index for DCSR
-            B.long_off = (long long)P.rows_pool.size();
-            int pos = 0;
-            for (int r = 0; r < B.m; ++r) {
-                if (dcsr && rowcnt[b][r] == 0) continue;
-                if (rowcnt[b][r] > kLongRow) P.rows_pool.push_back(pos);
-                ++pos;
-            }
+            B.long_off = rows_n;
+            rows_n += z.nlong;
         }
-        if (!B.tri && B.kernel == RBS_K_SPMV && B.group < 32 && B.lenmax > kMedRow) {
+        if (z.med) {
             // single RHS: rows of kMedRow+1..kLongRow entries take a warp each
-            B.med_off = (long long)P.rows_pool.size();
-            int pos = 0;
-            for (int r = 0; r < B.m; ++r) {
-                if (dcsr && rowcnt[b][r] == 0) continue;
-                if (rowcnt[b][r] > kMedRow && rowcnt[b][r] <= kLongRow) P.rows_pool.push_back(pos);
-                ++pos;
-            }
-            B.medrows = (int)((long long)P.rows_pool.size() - B.med_off);
-            if (!B.medrows) B.med_off = -1;
+            B.med_off = z.nmed ? rows_n : -1;
+            B.medrows = z.nmed;
+            rows_n += z.nmed;
         }
-        if (wants_level(B, opt)) {
-            B.lvl_off = (long long)P.lvl_pool.size();
-            P.lvl_pool.push_back(0);
-            for (int L = 0; L < B.nlv; ++L) P.lvl_pool.push_back(P.lvl_pool.back() + lvl_sizes[b][L]);
-            if (!B.contiguous) {
-                B.map_off = (long long)P.map_pool.size();
-                std::vector<int> fillL(P.lvl_pool.begin() + B.lvl_off, P.lvl_pool.begin() + B.lvl_off + B.nlv);
-                P.map_pool.resize(P.map_pool.size() + (size_t)B.m);
-                for (int r = 0; r < B.m; ++r) {
-                    int L = B.nnz == B.m ? 0 : level[B.r0 + r];
-                    P.map_pool[(size_t)B.map_off + fillL[L]++] = r;
-                }
+        if (z.lvl) {
+            B.lvl_off = lvl_n;
+            lvl_n += (long long)B.nlv + 1;
+            if (z.map) {
+                B.map_off = map_n;
+                map_n += B.m;
             }
         }
     }
+    P.rp_pool.resize((size_t)rp_n);
+    P.rows_pool.resize((size_t)rows_n);
+    P.lvl_pool.resize((size_t)lvl_n);
+    P.map_pool.resize((size_t)map_n);
+    parallel_for((size_t)P.sum_block, [&](size_t bi) {
+        const int b = (int)bi;
+        const ExecBlock &B = P.blocks[bi];
+        const PoolSizes &z = ps[bi];
+        const std::vector<int> &rc = rowcnt[bi];
+        std::vector<int> &rs = rowstart[bi];
+        rs.resize((size_t)B.m + 1);
+        rs[0] = (int)ent0[bi];
+        for (int r = 0; r < B.m; ++r) rs[(size_t)r + 1] = rs[(size_t)r] + rc[r];
+        int *rp = P.rp_pool.data() + B.rp_off;
+        if (z.dcsr) {
+            int *rows = P.rows_pool.data() + rows_dcsr0[bi];
+            int cnt = 0;
+            for (int r = 0; r < B.m; ++r)
+                if (rc[r]) {
+                    rows[cnt] = r;
+                    rp[cnt++] = rs[(size_t)r];
+                }
+            rp[cnt] = rs[(size_t)B.m];
+        } else {
+            for (int r = 0; r <= B.m; ++r) rp[r] = rs[(size_t)r];
+        }
+        if (!B.tri && B.longrows) {
+            int *out = P.rows_pool.data() + B.long_off, pos = 0, k = 0;
+            for (int r = 0; r < B.m; ++r) {
+                if (z.dcsr && rc[r] == 0) continue;
+                if (rc[r] > kLongRow) out[k++] = pos;
+                ++pos;
+            }
+        }
+        if (z.med && z.nmed) {
+            int *out = P.rows_pool.data() + B.med_off, pos = 0, k = 0;
+            for (int r = 0; r < B.m; ++r) {
+                if (z.dcsr && rc[r] == 0) continue;
+                if (rc[r] > kMedRow && rc[r] <= kLongRow) out[k++] = pos;
+                ++pos;
+            }
+        }
+        if (z.lvl) {
+            int *lp = P.lvl_pool.data() + B.lvl_off;
+            lp[0] = 0;
+            for (int L = 0; L < B.nlv; ++L) lp[L + 1] = lp[L] + lvl_sizes[bi][L];
+            if (z.map) {
+                std::vector<int> fillL(lp, lp + B.nlv);
+                int *mp = P.map_pool.data() + B.map_off;
+                for (int r = 0; r < B.m; ++r) {
+                    const int L = B.nnz == B.m ? 0 : level[B.r0 + r];
+                    mp[fillL[L]++] = r;
+                }
+            }
+        }
+        (void)b;
+    });
     if (dev_rows) {  // the entry pools filled on the device
         int rc = dev_pool_fill(*dev_rows, T, s, slot_base[(size_t)P.sum_block], ent, P.col_pool, P.val_pool, err);
         if (rc) return rc;
@@ -1547,6 +1606,12 @@ int export_reference(const Plan &P, const std::string &name, std::vector<int> &i
         iv = {LC_XW, LC_NB, LC_D, LC_RMAX, LC_T, LC_RING, LC_FMAX, LC_HDR_INTS};
         return RBS_OK;
     }
+    // the execution pools' index arrays (row pointers, row lists, level
+    // pointers and level maps of all blocks), for inspection
+    if (name == "rp_pool") return put(P.rp_pool);
+    if (name == "rows_pool") return put(P.rows_pool);
+    if (name == "lvl_pool") return put(P.lvl_pool);
+    if (name == "map_pool") return put(P.map_pool);
     if (name == "ca_tab") return put(P.ca_tab);
     if (name == "ca_col") return put(P.ca_col);
     if (name == "ca_val") {
